@@ -1,0 +1,263 @@
+/* reyn_b200 — a B200 (sm_100a) SPH step engine behind the reference's
+ * (reyn) interfaces. This is the C ABI: plain pointers, sizes and POD
+ * structs; every entry point returns an int status (REYN_OK = 0, negative on
+ * error) and never throws; reyn_last_error() describes the last failure of
+ * the calling thread. Device pointers are CUDA device pointers; `stream` is a
+ * cudaStream_t (NULL = legacy default stream). All work is enqueued on
+ * `stream`; functions that must return a host value (iteration counts, dt)
+ * synchronise that stream.
+ *
+ * Reference interfaces replaced (paths relative to the reference project):
+ *   smoothing kernels   src/kernels.cuh:19-165 (Kernel<D>, C2, B3, W6, COS)
+ *   particle state      src/particles.cuh:25-75 (Particles, SoA xx..m)
+ *   uniform grid        src/datastructure/uniformgrid.cuh:200-489
+ *                       (UniformGridBuilder, construct, construct_and_reorder)
+ *   grid query POD      src/datastructure/uniformgrid.cuh:84-179 (UniformGrid)
+ *   boundary            src/scene/scene.cuh:14-46 (Boundary, BoundarySamples),
+ *                       src/scene/sample_boundary.cu:267-297 (masses)
+ *   solvers             src/solvers/SESPH.cuh:37-53, PCISPH.cuh:80-103,
+ *                       IISPH.cuh:51-85 (constructors and step)
+ *   time step           src/timestep/cfl.cuh:13-32
+ *   bounds              src/scene/scene.cu:485-491 (Scene::hard_enforce_bounds)
+ */
+#ifndef REYN_B200_H_
+#define REYN_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define REYN_ABI_VERSION 1
+
+/* ---- status ------------------------------------------------------------ */
+enum reyn_status {
+    REYN_OK = 0,
+    REYN_ERR_INVALID = -1,       /* bad argument (null, size, enum, ...) */
+    REYN_ERR_OUT_OF_BOUNDS = -2, /* a particle lay outside its grid */
+    REYN_ERR_NONFINITE = -3,     /* NaN/Inf input where finite is required */
+    REYN_ERR_ITER_LIMIT = -4,    /* solver hit max_iter before converging */
+    REYN_ERR_CUDA = -5,          /* CUDA runtime error */
+    REYN_ERR_ALLOC = -6,         /* device allocation failed */
+    REYN_ERR_NOT_READY = -7      /* state used out of order */
+};
+
+/* message for the last failing call on this thread ("" if none) */
+const char* reyn_last_error(void);
+int reyn_abi_version(void);
+
+/* ---- smoothing kernels (src/kernels.cuh:19-174, FOREACH_KERNEL) ---------- */
+typedef enum reyn_kernel {
+    REYN_KERNEL_C2 = 0, /* Wendland C2, alpha = 21/(2 pi)       kernels.cuh:78 */
+    REYN_KERNEL_B3 = 1, /* cubic B-spline, alpha = 16/pi         kernels.cuh:101 */
+    REYN_KERNEL_W6 = 2, /* Wendland C6, alpha = 1365/(64 pi)     kernels.cuh:121 */
+    REYN_KERNEL_COS = 3 /* double cosine, alpha = pi/(4pi^2-30)  kernels.cuh:148 */
+} reyn_kernel;
+
+/* W(dx) and grad W(dx) at support h_bar for n offsets (device SoA arrays),
+ * Kernel::operator() and Kernel::nabla (kernels.cuh:40-64). */
+int reyn_kernel_eval(reyn_kernel kernel, float h_bar, const float* dx,
+    const float* dy, const float* dz, uint32_t n, float* w, float* gx,
+    float* gy, float* gz, void* stream);
+
+/* ---- particle state (src/particles.cuh:25-75) ---------------------------- */
+typedef struct reyn_particles reyn_particles;
+
+/* current device pointers of the SoA arrays; they CHANGE after a reorder,
+ * exactly as Particles' DeviceBuffers swap with `tmp` (buffer.cuh:205-207) */
+typedef struct reyn_soa {
+    float *xx, *xy, *xz, *vx, *vy, *vz, *m;
+    uint32_t n;
+    float rho0;
+} reyn_soa;
+
+/* Particles(N, rho0) (particles.cu:22): allocates 7 zeroed device arrays */
+int reyn_particles_create(uint32_t n, float rho0, reyn_particles** out);
+int reyn_particles_destroy(reyn_particles* p);
+/* pointers for direct device access; marks the engine's packed copy stale */
+int reyn_particles_soa(reyn_particles* p, reyn_soa* out);
+/* host <-> device copies of the 7 arrays (any host pointer may be NULL) */
+int reyn_particles_upload(reyn_particles* p, const float* xx, const float* xy,
+    const float* xz, const float* vx, const float* vy, const float* vz,
+    const float* m, void* stream);
+int reyn_particles_download(reyn_particles* p, float* xx, float* xy,
+    float* xz, float* vx, float* vy, float* vz, float* m, void* stream);
+
+/* ---- uniform grid (src/datastructure/uniformgrid.cuh:200-489) ----------- */
+typedef struct reyn_grid reyn_grid;
+
+typedef enum reyn_cell_order {
+    REYN_ORDER_XYZ = 0 /* z*nx*ny + y*nx + x, uniformgrid.cuh:33-40 */
+} reyn_cell_order;
+
+/* Device-usable description of a built grid: UniformGrid<R>
+ * (uniformgrid.cuh:84-179). `sorted` is NULL after construct_and_reorder
+ * (Resort::yes: particle arrays are in grid order). prefix has
+ * nx*ny*nz + 1 entries (the last equals n). */
+typedef struct reyn_grid_info {
+    float bound_min[3]; /* lower bound INCLUDING the 2r safety margin */
+    float cell_size;
+    float r_c_2;        /* squared search radius */
+    int32_t nx, ny, nz, nxny;
+    int32_t range;      /* cells searched per side: 2 at r/2, 1 at r */
+    uint32_t n;         /* particles indexed by the last construct */
+    const uint32_t* prefix;
+    const uint32_t* sorted;
+} reyn_grid_info;
+
+/* UniformGridBuilder(bound_min, bound_max, search_radius) (uniformgrid.cu:
+ * 65-96). cell_ratio = cell size / search radius: 0.5 is the reference
+ * geometry (5x5 strips of 5 cells), 1.0 gives 3x3 strips of 3 cells. */
+int reyn_grid_create(const float bound_min[3], const float bound_max[3],
+    float search_radius, float cell_ratio, reyn_cell_order order,
+    reyn_grid** out);
+int reyn_grid_destroy(reyn_grid* g);
+/* construct (uniformgrid.cu:145-156): builds prefix + sorted for n
+ * positions (device arrays), particles are not moved. Within a cell the
+ * indices are ascending (a stable counting sort), which is the canonical
+ * form of the reference's order. */
+int reyn_grid_construct(reyn_grid* g, float search_radius, const float* xx,
+    const float* xy, const float* xz, uint32_t n, void* stream);
+/* construct_and_reorder (uniformgrid.cuh:477-483): builds the grid over
+ * the particle positions, then permutes the 7 state arrays and the n_extra
+ * caller arrays (device, n floats each, permuted in place) into grid order. */
+int reyn_grid_construct_and_reorder(reyn_grid* g, float search_radius,
+    reyn_particles* state, float* const* extra, uint32_t n_extra,
+    void* stream);
+int reyn_grid_info_get(const reyn_grid* g, reyn_grid_info* out);
+/* after a construct_and_reorder: the permutation applied (new[i] =
+ * old[perm[i]]), device array of n entries */
+int reyn_grid_permutation(const reyn_grid* g, const uint32_t** perm);
+
+/* neighbour statistics over a built grid (the reference grid test's
+ * quantities, uniformgrid.cu:185-207): count of neighbours within r (self
+ * excluded), sum of |x_ij|^2, and, if m != NULL, density sum m_j W(x_ij)
+ * with `kernel` at support r. Positions/masses are the arrays the grid was
+ * built over (in grid order after a reorder). Any output may be NULL. */
+int reyn_grid_neighbour_stats(const reyn_grid* g, const float* xx,
+    const float* xy, const float* xz, const float* m, reyn_kernel kernel,
+    uint32_t* count, float* len2, float* rho, void* stream);
+
+/* ---- boundary (src/scene/scene.cuh:14-46) -------------------------------- */
+typedef struct reyn_boundary reyn_boundary;
+
+/* Boundary samples at positions bx,by,bz (DEVICE arrays, nb entries) with
+ * masses bm (device) or, if bm == NULL, Akinci masses computed as
+ * calculate_boundary_masses does (sample_boundary.cu:267-297: B3 at 2h,
+ * m = 1 then `mass_iters` refinements; double-buffered here). The samples
+ * are copied and reordered into their own grid at support 2h over their own
+ * bounds (sample_boundary.cu:413-428). nb == 0 is an empty boundary. */
+int reyn_boundary_create(const float* bx, const float* by, const float* bz,
+    const float* bm, uint32_t nb, float h, float rho0, uint32_t mass_iters,
+    void* stream, reyn_boundary** out);
+int reyn_boundary_destroy(reyn_boundary* b);
+/* device pointers of the reordered samples and masses */
+int reyn_boundary_arrays(const reyn_boundary* b, const float** bx,
+    const float** by, const float** bz, const float** bm, uint32_t* nb);
+
+/* ---- solvers (src/solvers/*) --------------------------------------------- */
+typedef enum reyn_scheme {
+    REYN_SESPH = 0, /* SESPH.cu:68-95   */
+    REYN_PCISPH = 1, /* PCISPH.cu:59-111 */
+    REYN_IISPH = 2 /* IISPH.cu:165-262 */
+} reyn_scheme;
+
+typedef enum reyn_convergence {
+    /* the reference's own criteria: PCISPH avg(rho) <= (1+eta) rho0
+     * (PCISPH.cu:101); IISPH "no particle's predicted error above eta rho0"
+     * (IISPH.cu:246-250) */
+    REYN_CONV_REFERENCE = 0,
+    /* IISPH: average of max(0, predicted density error) <= eta rho0,
+     * reduced in FP64 */
+    REYN_CONV_AVERAGE = 1
+} reyn_convergence;
+
+typedef struct reyn_params {
+    reyn_kernel kernel;     /* support radius = 2h (main.cu:51) */
+    float h;                /* particle spacing */
+    float rho0;             /* rest density */
+    float nu;               /* viscosity */
+    float g[3];             /* gravity */
+    float k_sesph;          /* SESPH stiffness (SESPH.cuh:50: 500) */
+    float eta;              /* tolerance (PCISPH 0.001, IISPH 0.005) */
+    uint32_t min_iter;      /* 3 (PCISPH.cuh:38, IISPH.cuh:43) */
+    uint32_t max_iter;      /* 0 = unbounded, as the reference */
+    float omega;            /* IISPH Jacobi weight (0.5, IISPH.cuh:45) */
+    int32_t warmstart;      /* IISPH p *= 0.5 (IISPH.cuh:48) */
+    reyn_convergence convergence;
+} reyn_params;
+
+/* the reference's constants for `scheme` (gravity (0,-9.81,0)) */
+int reyn_params_reference(reyn_scheme scheme, reyn_kernel kernel, float h,
+    float rho0, float nu, reyn_params* out);
+
+typedef struct reyn_solver reyn_solver;
+
+/* SESPH/PCISPH/IISPH(W, N, nu, h, rho0, buffers...): the solver owns its
+ * per-particle buffers (rho, a, p, a_ii, s_i). */
+int reyn_solver_create(reyn_scheme scheme, const reyn_params* params,
+    uint32_t n, reyn_solver** out);
+int reyn_solver_destroy(reyn_solver* s);
+
+/* Solver::step(state, grid, bdy, dt) on a grid built by
+ * construct_and_reorder over `state`. IISPH's pressure is carried across
+ * steps and re-permuted with the grid's permutation automatically (the
+ * reference passes it as an extra reorder buffer, main.cu:68). iters (may
+ * be NULL) receives the iteration count (1 for SESPH); it synchronises the
+ * stream for PCISPH/IISPH. */
+int reyn_solver_step(reyn_solver* s, reyn_particles* state,
+    const reyn_grid* grid, const reyn_boundary* bdy, float dt,
+    uint32_t* iters, void* stream);
+
+/* per-particle solver buffers (device, grid order of the last step) */
+typedef struct reyn_solver_buffers {
+    const float *rho, *p, *aii, *sii, *ax, *ay, *az;
+    uint32_t n;
+} reyn_solver_buffers;
+int reyn_solver_buffers_get(const reyn_solver* s, reyn_solver_buffers* out);
+
+/* statistics of the last step: iterations and the last sweep's average
+ * (max(0, .)) and maximum predicted density error, in units of rho0 */
+typedef struct reyn_step_stats {
+    uint32_t iters;
+    double avg_density_error;
+    double max_density_error;
+} reyn_step_stats;
+int reyn_solver_stats(const reyn_solver* s, reyn_step_stats* out);
+
+/* ---- time step (src/timestep/cfl.cu) -------------------------------------- */
+/* cfl_time_step (cfl.cu:5-37); synchronises the stream */
+int reyn_cfl_time_step(reyn_particles* state, float lambda, float h,
+    const float g[3], float* dt_out, void* stream);
+/* simple_dt_controller (cfl.cu:39-52); synchronises the stream */
+int reyn_dt_controller(reyn_particles* state, uint32_t iter_last,
+    float dt_last, float lambda, float h, const float g[3],
+    uint32_t iter_target, float change_factor, float* dt_out, void* stream);
+
+/* ---- bounds (src/scene/scene.cu:466-491) ---------------------------------- */
+int reyn_enforce_bounds(reyn_particles* state, const float bound_min[3],
+    const float bound_max[3], void* stream);
+
+/* ---- launch accounting (no counterpart in the reference, which has no
+ * tracing): per-kernel launch counts and CUDA-event device time ----------- */
+typedef struct reyn_profile_entry {
+    char name[48];     /* kernel name */
+    uint64_t launches; /* launches since the last reset */
+    double total_ms;   /* summed device time while timing was enabled */
+} reyn_profile_entry;
+
+/* on != 0: bracket every engine kernel launch with CUDA events on its
+ * stream (launches are always counted) */
+int reyn_profile_enable(int on);
+int reyn_profile_reset(void);
+/* per-kernel totals; synchronises on the recorded events. Writes at most
+ * cap entries to out (may be NULL) and the number of kernels to *count. */
+int reyn_profile_read(reyn_profile_entry* out, uint32_t cap, uint32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* REYN_B200_H_ */

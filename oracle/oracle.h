@@ -1,0 +1,121 @@
+/* CPU ORACLE — test infrastructure only.
+ *
+ * A host C++/OpenMP restatement of the reference's (reyn) SPH hot path, used
+ * as the checker for the CUDA engine in tests/, by __graft_entry__.smoke() and
+ * as bench.py's CPU baseline. It is never linked into, loaded by or called
+ * from the product (reyn_b200/). Every function cites the reference file:line
+ * it restates. Parity of this oracle is pinned against the reference itself:
+ * kernel values against the reference's own kernel classes compiled for the
+ * host (oracle/ref/ref_kernels_host.cpp), grid and solver outputs against the
+ * reference's CUDA code run on a B200 (fixtures in tests/golden/).
+ *
+ * Conventions: all arrays are host SoA arrays; status 0 = ok, < 0 = error.
+ * The sort inside each grid cell is STABLE (ascending particle index), i.e.
+ * the canonical form of the reference's atomicSub order (uniformgrid.cu:59).
+ */
+#ifndef REYN_ORACLE_H_
+#define REYN_ORACLE_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* grid geometry, restating UniformGridBuilder's initializer list
+ * (uniformgrid.cu:65-96); cell_ratio 0.5 is the reference geometry. */
+typedef struct orc_geom {
+    float bmin[3]; /* lower bound minus the 2r safety margin */
+    float cell;    /* cell size */
+    float r2;      /* squared search radius */
+    int32_t nx, ny, nz;
+    int32_t range; /* cells searched on each side: 2 at cell r/2, 1 at r */
+} orc_geom;
+
+int orc_geometry(const float bmin[3], const float bmax[3], float r,
+    float cell_ratio, orc_geom* g);
+
+/* W(dx) and ∇W(dx) of kernel `kind` (0 C2, 1 B3, 2 W6, 3 COS) with support
+ * h_bar, kernels.cuh:19-165 (host flavour: norm = sqrt(dot)). */
+int orc_kernel_eval(int kind, float h_bar, uint32_t n, const float* dx,
+    const float* dy, const float* dz, float* w, float* gx, float* gy,
+    float* gz);
+
+/* counting-sort grid build (uniformgrid.cu:20-63, 98-143), stable within a
+ * cell. prefix: nx*ny*nz + 1 entries (exclusive scan, last = N);
+ * sorted: N particle indices; keys (optional): N cell keys. */
+int orc_grid_build(const orc_geom* g, uint32_t n, const float* x,
+    const float* y, const float* z, uint32_t* prefix, uint32_t* sorted,
+    uint32_t* keys);
+
+/* the grid test's neighbour count (self excluded) and Σ|x_ij|² over the
+ * `ff_nbrs` traversal (uniformgrid.cu:185-207, uniformgrid.cuh:113-178),
+ * plus the fluid density Σ m_j W(x_ij) (solver.cuh:31-33) when m != NULL. */
+int orc_neighbours(const orc_geom* g, uint32_t n, const float* x,
+    const float* y, const float* z, const uint32_t* prefix,
+    const uint32_t* sorted, uint32_t* count, float* len2, int kind,
+    const float* m, float* rho);
+
+/* brute-force O(N^2) neighbour count (uniformgrid.cu:209-229) */
+int orc_brute_count(uint32_t n, const float* x, const float* y,
+    const float* z, float r, uint32_t* count, float* len2);
+
+/* Akinci boundary masses (sample_boundary.cu:250-297): B3 at support 2h,
+ * m0 = 1, `iters` refinements m_i <- rho0 m_i / Σ_j m_j W_ij. The reference
+ * updates m in place while neighbours read it (a data race); this oracle uses
+ * a double-buffered (Jacobi) update. Positions are given in any order. */
+int orc_boundary_masses(uint32_t nb, const float* bx, const float* by,
+    const float* bz, float h, float rho0, uint32_t iters, float* m);
+
+/* cfl_time_step (cfl.cu:5-37) */
+float orc_cfl(uint32_t n, const float* vx, const float* vy, const float* vz,
+    float lambda, float h, const float g[3]);
+
+/* simple_dt_controller (cfl.cu:39-52) */
+float orc_dt_controller(uint32_t iter_last, float dt_last, float lambda,
+    float h, uint32_t n, const float* vx, const float* vy, const float* vz,
+    const float g[3], uint32_t iter_target, float change_factor);
+
+/* solver parameters; orc_params_reference() gives the reference's hard-coded
+ * constants (SESPH.cuh:50, PCISPH.cuh:27-38, IISPH.cuh:37-48). */
+typedef struct orc_params {
+    int scheme;         /* 0 SESPH, 1 PCISPH, 2 IISPH */
+    int kind;           /* smoothing kernel, support 2h */
+    float h, rho0, nu;
+    float g[3];
+    float k_sesph;      /* SESPH stiffness */
+    float eta;          /* PCISPH: avg rho tolerance; IISPH: per-particle */
+    uint32_t min_iter;
+    uint32_t max_iter;  /* 0 = unbounded (reference) */
+    float omega;        /* IISPH Jacobi weight */
+    int warmstart;      /* IISPH: p *= 0.5 at step start */
+    int iisph_avg;      /* IISPH: stop on average error <= eta instead of
+                           "no particle above eta" (reference) */
+    float cell_ratio;   /* 0.5 = reference */
+} orc_params;
+
+void orc_params_reference(int scheme, int kind, float h, float rho0,
+    float nu, orc_params* p);
+
+/* `steps` iterations of the reference main loop (main.cu:60-78): grid build
+ * + reorder of the state, id and (IISPH) pressure at 2h (scene.cuh:149-156),
+ * solver step, hard_enforce_bounds (scene.cu:466-491), with a fixed dt.
+ * State arrays are updated in place and left in the last grid order; solver
+ * buffers after the last step go to rho/p/aii/sii/ax/ay/az (may be NULL);
+ * iters[k] receives the iteration count of step k; p must hold the pressure
+ * to warm-start from (zeros on the first step, like the reference). */
+int orc_run(const orc_params* prm, uint32_t n, float* x, float* y, float* z,
+    float* vx, float* vy, float* vz, float* m, float* id, float* p,
+    uint32_t nb, const float* bx, const float* by, const float* bz,
+    const float* bm, const float scene_min[3], const float scene_max[3],
+    float dt, uint32_t steps, float* rho, float* aii, float* sii, float* ax,
+    float* ay, float* az, uint32_t* iters);
+
+/* number of OpenMP threads the oracle uses */
+int orc_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

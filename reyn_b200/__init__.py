@@ -1,0 +1,400 @@
+"""reyn_b200 — Python binding of the B200 SPH step engine's C ABI
+(include/reyn_b200.h) through ctypes.
+
+The engine itself is CUDA C++ (reyn_b200/csrc, built in-tree into
+libreyn_b200.so by ``python -m reyn_b200.build``). This module only marshals
+arguments; device memory for inputs/outputs is owned by torch tensors or by
+the engine's own handles. There is no CPU fallback: every call fails loudly if
+the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libreyn_b200.so")
+
+C2, B3, W6, COS = 0, 1, 2, 3
+KERNELS = {"C2": C2, "B3": B3, "W6": W6, "COS": COS}
+SESPH, PCISPH, IISPH = 0, 1, 2
+CONV_REFERENCE, CONV_AVERAGE = 0, 1
+
+OK = 0
+ERR_INVALID, ERR_OUT_OF_BOUNDS, ERR_NONFINITE, ERR_ITER_LIMIT = -1, -2, -3, -4
+ERR_CUDA, ERR_ALLOC, ERR_NOT_READY = -5, -6, -7
+
+_vp = ctypes.c_void_p
+_f = ctypes.c_float
+_u32 = ctypes.c_uint32
+
+
+class ReynError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"reyn_b200 error {code}: {msg}")
+        self.code = code
+
+
+class Soa(ctypes.Structure):
+    _fields_ = [("xx", _vp), ("xy", _vp), ("xz", _vp), ("vx", _vp), ("vy", _vp), ("vz", _vp),
+                ("m", _vp), ("n", _u32), ("rho0", _f)]
+
+
+class GridInfo(ctypes.Structure):
+    _fields_ = [("bound_min", _f * 3), ("cell_size", _f), ("r_c_2", _f), ("nx", ctypes.c_int32),
+                ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("nxny", ctypes.c_int32),
+                ("range", ctypes.c_int32), ("n", _u32), ("prefix", _vp), ("sorted", _vp)]
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int), ("h", _f), ("rho0", _f), ("nu", _f), ("g", _f * 3),
+                ("k_sesph", _f), ("eta", _f), ("min_iter", _u32), ("max_iter", _u32),
+                ("omega", _f), ("warmstart", ctypes.c_int32), ("convergence", ctypes.c_int)]
+
+
+class SolverBuffers(ctypes.Structure):
+    _fields_ = [("rho", _vp), ("p", _vp), ("aii", _vp), ("sii", _vp), ("ax", _vp), ("ay", _vp),
+                ("az", _vp), ("n", _u32)]
+
+
+class ProfileEntry(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 48), ("launches", ctypes.c_uint64),
+                ("total_ms", ctypes.c_double)]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [("iters", _u32), ("avg_density_error", ctypes.c_double),
+                ("max_density_error", ctypes.c_double)]
+
+
+_lib = None
+
+# (name, argtypes) of every entry point in include/reyn_b200.h
+_SIGNATURES = {
+    "reyn_last_error": [],
+    "reyn_abi_version": [],
+    "reyn_kernel_eval": [ctypes.c_int, _f, _vp, _vp, _vp, _u32, _vp, _vp, _vp, _vp, _vp],
+    "reyn_particles_create": [_u32, _f, ctypes.POINTER(_vp)],
+    "reyn_particles_destroy": [_vp],
+    "reyn_particles_soa": [_vp, ctypes.POINTER(Soa)],
+    "reyn_particles_upload": [_vp] + [_vp] * 7 + [_vp],
+    "reyn_particles_download": [_vp] + [_vp] * 7 + [_vp],
+    "reyn_grid_create": [_f * 3, _f * 3, _f, _f, ctypes.c_int, ctypes.POINTER(_vp)],
+    "reyn_grid_destroy": [_vp],
+    "reyn_grid_construct": [_vp, _f, _vp, _vp, _vp, _u32, _vp],
+    "reyn_grid_construct_and_reorder": [_vp, _f, _vp, ctypes.POINTER(_vp), _u32, _vp],
+    "reyn_grid_info_get": [_vp, ctypes.POINTER(GridInfo)],
+    "reyn_grid_permutation": [_vp, ctypes.POINTER(_vp)],
+    "reyn_grid_neighbour_stats": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp],
+    "reyn_boundary_create": [_vp, _vp, _vp, _vp, _u32, _f, _f, _u32, _vp, ctypes.POINTER(_vp)],
+    "reyn_boundary_destroy": [_vp],
+    "reyn_boundary_arrays": [_vp] + [ctypes.POINTER(_vp)] * 4 + [ctypes.POINTER(_u32)],
+    "reyn_params_reference": [ctypes.c_int, ctypes.c_int, _f, _f, _f, ctypes.POINTER(Params)],
+    "reyn_solver_create": [ctypes.c_int, ctypes.POINTER(Params), _u32, ctypes.POINTER(_vp)],
+    "reyn_solver_destroy": [_vp],
+    "reyn_solver_step": [_vp, _vp, _vp, _vp, _f, ctypes.POINTER(_u32), _vp],
+    "reyn_solver_buffers_get": [_vp, ctypes.POINTER(SolverBuffers)],
+    "reyn_solver_stats": [_vp, ctypes.POINTER(StepStats)],
+    "reyn_cfl_time_step": [_vp, _f, _f, _f * 3, ctypes.POINTER(_f), _vp],
+    "reyn_dt_controller": [_vp, _u32, _f, _f, _f, _f * 3, _u32, _f, ctypes.POINTER(_f), _vp],
+    "reyn_enforce_bounds": [_vp, _f * 3, _f * 3, _vp],
+    "reyn_profile_enable": [ctypes.c_int],
+    "reyn_profile_reset": [],
+    "reyn_profile_read": [ctypes.POINTER(ProfileEntry), _u32, ctypes.POINTER(_u32)],
+}
+
+
+def declared_symbols() -> list[str]:
+    """Entry points declared in include/reyn_b200.h."""
+    return list(_SIGNATURES)
+
+
+def lib():
+    """The loaded engine library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m reyn_b200.build` "
+                              "(the engine has no fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in _SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.reyn_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise ReynError(rc, lib().reyn_last_error().decode())
+
+
+def _f3(v) -> ctypes.Array:
+    return (_f * 3)(*[float(x) for x in v])
+
+
+def _ptr(t) -> Optional[int]:
+    """Device pointer of a torch tensor (or None)."""
+    if t is None:
+        return None
+    assert t.is_cuda and t.is_contiguous(), "expected a contiguous CUDA tensor"
+    return t.data_ptr()
+
+
+def _stream(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return int(stream)
+
+
+def kernel_eval(kernel: int, h_bar: float, dx, dy, dz, stream=None):
+    """W and grad W (device tensors in, device tensors out)."""
+    import torch
+    n = dx.numel()
+    w, gx, gy, gz = (torch.empty(n, device=dx.device, dtype=torch.float32) for _ in range(4))
+    check(lib().reyn_kernel_eval(kernel, h_bar, _ptr(dx), _ptr(dy), _ptr(dz), n, _ptr(w),
+                                 _ptr(gx), _ptr(gy), _ptr(gz), _stream(stream)))
+    return w, gx, gy, gz
+
+
+class Particles:
+    """Particles(N, rho0) (reference particles.cuh:25-75): 7 device SoA arrays."""
+
+    FIELDS = ("xx", "xy", "xz", "vx", "vy", "vz", "m")
+
+    def __init__(self, n: int, rho0: float):
+        h = _vp()
+        check(lib().reyn_particles_create(n, rho0, ctypes.byref(h)))
+        self.h = h
+        self.n = n
+        self.rho0 = rho0
+
+    def close(self):
+        # at interpreter shutdown the module globals may already be gone
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.reyn_particles_destroy(self.h)
+        self.h = None
+
+    __del__ = close
+
+    def soa(self) -> Soa:
+        s = Soa()
+        check(lib().reyn_particles_soa(self.h, ctypes.byref(s)))
+        return s
+
+    def upload(self, host: dict, stream=None):
+        arrs = [np.ascontiguousarray(host[k], np.float32) if k in host else None
+                for k in ("x", "y", "z", "vx", "vy", "vz", "m")]
+        ptrs = [a.ctypes.data if a is not None else None for a in arrs]
+        check(lib().reyn_particles_upload(self.h, *ptrs, _stream(stream)))
+        import torch
+        torch.cuda.synchronize()
+
+    def download(self, stream=None) -> dict:
+        out = {k: np.empty(self.n, np.float32) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        check(lib().reyn_particles_download(self.h, *[out[k].ctypes.data for k in
+                                                      ("x", "y", "z", "vx", "vy", "vz", "m")],
+                                            _stream(stream)))
+        return out
+
+
+class Grid:
+    """UniformGridBuilder (reference uniformgrid.cuh:200-489)."""
+
+    def __init__(self, bmin, bmax, search_radius: float, cell_ratio: float = 0.5):
+        h = _vp()
+        check(lib().reyn_grid_create(_f3(bmin), _f3(bmax), search_radius, cell_ratio, 0,
+                                     ctypes.byref(h)))
+        self.h = h
+        self.r = search_radius
+
+    def close(self):
+        # at interpreter shutdown the module globals may already be gone
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.reyn_grid_destroy(self.h)
+        self.h = None
+
+    __del__ = close
+
+    def construct(self, x, y, z, stream=None):
+        check(lib().reyn_grid_construct(self.h, self.r, _ptr(x), _ptr(y), _ptr(z), x.numel(),
+                                        _stream(stream)))
+
+    def construct_and_reorder(self, state: Particles, extra: Sequence = (), stream=None):
+        ptrs = (_vp * max(len(extra), 1))(*[_ptr(t) for t in extra])
+        check(lib().reyn_grid_construct_and_reorder(self.h, self.r, state.h, ptrs, len(extra),
+                                                    _stream(stream)))
+
+    def info(self) -> GridInfo:
+        g = GridInfo()
+        check(lib().reyn_grid_info_get(self.h, ctypes.byref(g)))
+        return g
+
+    def permutation_ptr(self) -> int:
+        p = _vp()
+        check(lib().reyn_grid_permutation(self.h, ctypes.byref(p)))
+        return p.value
+
+    def neighbour_stats(self, x, y, z, m=None, kernel: int = C2, stream=None):
+        import torch
+        n = x.numel()
+        count = torch.empty(n, device=x.device, dtype=torch.int32)
+        len2 = torch.empty(n, device=x.device, dtype=torch.float32)
+        rho = torch.empty(n, device=x.device, dtype=torch.float32) if m is not None else None
+        check(lib().reyn_grid_neighbour_stats(self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(m), kernel,
+                                              _ptr(count), _ptr(len2), _ptr(rho),
+                                              _stream(stream)))
+        return count, len2, rho
+
+
+class Boundary:
+    """BoundarySamples (reference scene.cuh:14-46) with Akinci masses."""
+
+    def __init__(self, bx, by, bz, bm=None, h: float = 1.0, rho0: float = 1.0,
+                 mass_iters: int = 5, stream=None):
+        hdl = _vp()
+        nb = 0 if bx is None else bx.numel()
+        check(lib().reyn_boundary_create(_ptr(bx), _ptr(by), _ptr(bz), _ptr(bm), nb, h, rho0,
+                                         mass_iters, _stream(stream), ctypes.byref(hdl)))
+        self.h = hdl
+        self.nb = nb
+
+    def close(self):
+        # at interpreter shutdown the module globals may already be gone
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.reyn_boundary_destroy(self.h)
+        self.h = None
+
+    __del__ = close
+
+    def arrays(self):
+        """(x, y, z, m) device pointers of the reordered samples."""
+        ps = [_vp() for _ in range(4)]
+        nb = _u32()
+        check(lib().reyn_boundary_arrays(self.h, *[ctypes.byref(p) for p in ps],
+                                         ctypes.byref(nb)))
+        return [p.value for p in ps], nb.value
+
+
+def reference_params(scheme: int, kernel: int, h: float, rho0: float, nu: float) -> Params:
+    p = Params()
+    check(lib().reyn_params_reference(scheme, kernel, h, rho0, nu, ctypes.byref(p)))
+    return p
+
+
+class Solver:
+    """SESPH / PCISPH / IISPH (reference solvers/*.cuh)."""
+
+    def __init__(self, scheme: int, params: Params, n: int):
+        h = _vp()
+        check(lib().reyn_solver_create(scheme, ctypes.byref(params), n, ctypes.byref(h)))
+        self.h = h
+        self.n = n
+        self.scheme = scheme
+
+    def close(self):
+        # at interpreter shutdown the module globals may already be gone
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.reyn_solver_destroy(self.h)
+        self.h = None
+
+    __del__ = close
+
+    def step(self, state: Particles, grid: Grid, bdy: Optional[Boundary], dt: float,
+             stream=None) -> int:
+        it = _u32()
+        check(lib().reyn_solver_step(self.h, state.h, grid.h, bdy.h if bdy else None, dt,
+                                     ctypes.byref(it), _stream(stream)))
+        return it.value
+
+    def buffers(self) -> SolverBuffers:
+        b = SolverBuffers()
+        check(lib().reyn_solver_buffers_get(self.h, ctypes.byref(b)))
+        return b
+
+    def stats(self) -> StepStats:
+        s = StepStats()
+        check(lib().reyn_solver_stats(self.h, ctypes.byref(s)))
+        return s
+
+
+def cfl_time_step(state: Particles, lam: float, h: float, g, stream=None) -> float:
+    dt = _f()
+    check(lib().reyn_cfl_time_step(state.h, lam, h, _f3(g), ctypes.byref(dt), _stream(stream)))
+    return dt.value
+
+
+def dt_controller(state: Particles, iter_last: int, dt_last: float, lam: float, h: float, g,
+                  iter_target: int = 5, change: float = 0.01, stream=None) -> float:
+    dt = _f()
+    check(lib().reyn_dt_controller(state.h, iter_last, dt_last, lam, h, _f3(g), iter_target,
+                                   change, ctypes.byref(dt), _stream(stream)))
+    return dt.value
+
+
+def enforce_bounds(state: Particles, bmin, bmax, stream=None) -> None:
+    check(lib().reyn_enforce_bounds(state.h, _f3(bmin), _f3(bmax), _stream(stream)))
+
+
+def profile_enable(on: bool = True) -> None:
+    """Bracket every engine kernel launch with CUDA events (launches are
+    always counted)."""
+    check(lib().reyn_profile_enable(1 if on else 0))
+
+
+def profile_reset() -> None:
+    check(lib().reyn_profile_reset())
+
+
+def profile_read() -> dict:
+    """{kernel name: (launches, total device ms)} since the last reset."""
+    cnt = _u32()
+    check(lib().reyn_profile_read(None, 0, ctypes.byref(cnt)))
+    arr = (ProfileEntry * max(cnt.value, 1))()
+    check(lib().reyn_profile_read(arr, cnt.value, ctypes.byref(cnt)))
+    return {arr[i].name.decode(): (int(arr[i].launches), float(arr[i].total_ms))
+            for i in range(cnt.value)}
+
+
+class _DeviceView:
+    """__cuda_array_interface__ over an engine-owned device array."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (ptr, False), "version": 3}
+
+
+def device_tensor(ptr: int, n: int, dtype=np.float32):
+    """A torch view (no copy) of n elements at an engine device pointer."""
+    import torch
+    typestr = {np.float32: "<f4", np.uint32: "<u4", np.int32: "<i4"}[dtype]
+    if n == 0:
+        return torch.empty(0, dtype=torch.float32 if dtype == np.float32 else torch.int32,
+                           device="cuda")
+    t = torch.as_tensor(_DeviceView(ptr, n, typestr), device="cuda")
+    return t
+
+
+def device_to_numpy(ptr: int, n: int, dtype=np.float32) -> np.ndarray:
+    """Copies n elements at an engine device pointer into a numpy array."""
+    import torch
+    torch.cuda.synchronize()
+    return device_tensor(ptr, n, dtype).cpu().numpy().astype(dtype, copy=False)
+
+
+@dataclass
+class StepOutputs:
+    state: dict
+    rho: np.ndarray
+    p: np.ndarray
+    aii: np.ndarray
+    sii: np.ndarray
+    a: np.ndarray
+    iters: list

@@ -1,0 +1,244 @@
+// Device-side building blocks of the reyn_b200 engine: smoothing kernels,
+// the uniform-grid view and the fixed-radius neighbour traversal.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+
+namespace reyn {
+
+// ---- smoothing kernels ----------------------------------------------------
+// Kernel<D> (reference kernels.cuh:19-65) precomputes 1/h, alpha/h^3 and
+// alpha/h^4; the four shape functions w(q), dw(q) follow kernels.cuh:78-165.
+
+enum KernelKind : int { K_C2 = 0, K_B3 = 1, K_W6 = 2, K_COS = 3 };
+
+struct KernelConst {
+    float h_inv;    // 1 / h_bar
+    float w_scale;  // alpha / h_bar^3
+    float dw_scale; // alpha / h_bar^4
+};
+
+// normalisation alpha of each kernel, rounded to float exactly as the
+// reference's constructors do (kernels.cuh:81, 104, 124, 151)
+inline float kernel_alpha(int kind)
+{
+    switch (kind) {
+    case K_C2: return (float)(21.f / 2.f * M_1_PI);
+    case K_B3: return (float)(16.f * M_1_PI);
+    case K_W6: return (float)(1365.f / 64.f * M_1_PI);
+    case K_COS: return (float)(M_PI / (4.f * M_PI * M_PI - 30.f));
+    default: return 0.f;
+    }
+}
+
+inline KernelConst make_kernel(int kind, float h_bar)
+{
+    const float a = kernel_alpha(kind);
+    return KernelConst { 1.0f / h_bar, a / (h_bar * h_bar * h_bar),
+        a / (h_bar * h_bar * h_bar * h_bar) };
+}
+
+// clamp to [0, 1]: __saturatef on the device, fmin/fmax on the host (the
+// same split as the reference's `sat`, vector.cuh:236-243)
+__host__ __device__ __forceinline__ float sat01(float a)
+{
+#ifdef __CUDA_ARCH__
+    return __saturatef(a);
+#else
+    return fminf(fmaxf(a, 0.f), 1.f);
+#endif
+}
+
+template <int KIND> struct Shape;
+
+template <> struct Shape<K_C2> { // w = (1-q)_+^4 (4q+1)
+    __host__ __device__ static float w(float q)
+    {
+        const float t = fmaxf(0.f, 1.f - q);
+        const float t2 = t * t;
+        return t2 * t2 * (4.f * q + 1.f);
+    }
+    __host__ __device__ static float dw(float q)
+    {
+        const float t = fmaxf(0.f, 1.f - q);
+        return t * t * t * (-20.f * q);
+    }
+};
+
+template <> struct Shape<K_B3> { // w = (1-q)_+^3 - 4 (1/2-q)_+^3
+    __host__ __device__ static float w(float q)
+    {
+        const float t = fmaxf(0.f, 1.f - q);
+        const float u = sat01(0.5f - q);
+        return t * t * t - 4.f * u * u * u;
+    }
+    __host__ __device__ static float dw(float q)
+    {
+        const float t = fmaxf(0.f, 1.f - q);
+        const float u = sat01(0.5f - q);
+        return -3.f * t * t + 12.f * u * u;
+    }
+};
+
+template <> struct Shape<K_W6> { // w = (1-q)_+^8 (32q^3 + 25q^2 + 8q + 1)
+    __host__ __device__ static float w(float q)
+    {
+        const float t = fmaxf(0.f, 1.f - q);
+        const float t2 = t * t;
+        const float t4 = t2 * t2;
+        const float q2 = q * q;
+        return (t4 * t4) * (32.f * q2 * q + 25.f * q2 + 8.f * q + 1.f);
+    }
+    __host__ __device__ static float dw(float q)
+    {
+        const float t = fmaxf(0.f, 1.f - q);
+        const float t2 = t * t;
+        const float t7 = t2 * t2 * t2 * t;
+        return t7 * ((16.f * q * q + 7.f * q + 1.f) * (-22.f * q));
+    }
+};
+
+template <> struct Shape<K_COS> { // w = 4 cos(pi q) + cos(2 pi q) + 3
+    __host__ __device__ static float w(float q)
+    {
+        const float s = (float)M_PI * fminf(1.f, q);
+        return 4.f * cosf(s) + cosf(2.f * s) + 3.f;
+    }
+    __host__ __device__ static float dw(float q)
+    {
+        const float s = (float)M_PI * fminf(1.f, q);
+        const float tp = (float)(2.0 * M_PI);
+        return -2.f * tp * sinf(s) - sinf(2.f * s) * tp;
+    }
+};
+
+// W and the gradient factor g (grad W = g * x_ij) for a neighbour pair with
+// squared distance 0 <= l2 <= r^2 (the traversal guarantees the range).
+// len = l2 * rsqrt(l2) replaces the reference's norm3df; the self pair
+// (l2 = 0) has W = W(0) and a zero gradient, as kernels.cuh:60-63 defines.
+template <int KIND>
+__device__ __forceinline__ float pair_w(const KernelConst& k, float l2)
+{
+    const float len = l2 > 0.f ? l2 * rsqrtf(l2) : 0.f;
+    return k.w_scale * Shape<KIND>::w(__saturatef(len * k.h_inv));
+}
+
+template <int KIND>
+__device__ __forceinline__ float pair_g(const KernelConst& k, float l2)
+{
+    const float inv = rsqrtf(l2);
+    const float len = l2 * inv;
+    const float g = k.dw_scale * Shape<KIND>::dw(len * k.h_inv) * inv;
+    return (l2 > 0.f && isfinite(g)) ? g : 0.f;
+}
+
+template <int KIND>
+__device__ __forceinline__ void pair_wg(
+    const KernelConst& k, float l2, float& w, float& g)
+{
+    const float inv = rsqrtf(l2);
+    const float len = l2 > 0.f ? l2 * inv : 0.f;
+    const float q = len * k.h_inv;
+    w = k.w_scale * Shape<KIND>::w(__saturatef(q));
+    const float gg = k.dw_scale * Shape<KIND>::dw(q) * inv;
+    g = (l2 > 0.f && isfinite(gg)) ? gg : 0.f;
+}
+
+// ---- uniform grid view ----------------------------------------------------
+// The device POD of a built grid, UniformGrid<Resort::yes>
+// (uniformgrid.cuh:84-97): lower bound (with margin), cell size, r^2, cell
+// counts and the prefix over all cells (C + 1 entries).
+struct GridView {
+    float lox, loy, loz;
+    float cell;
+    float r2;
+    int nx, ny, nz, nxny;
+    const uint32_t* __restrict__ prefix;
+};
+
+// _index3 (uniformgrid.cuh:17-22): floor((x - min) / cell), IEEE division so
+// that keys agree with the reference bit for bit
+__device__ __forceinline__ int3 cell_of(const GridView& g, float x, float y, float z)
+{
+    return make_int3((int)floorf((x - g.lox) / g.cell),
+        (int)floorf((y - g.loy) / g.cell), (int)floorf((z - g.loz) / g.cell));
+}
+
+__device__ __forceinline__ bool cell_inside(const GridView& g, int3 c, int R)
+{
+    return c.x >= R && c.y >= R && c.z >= R && c.x < g.nx - R && c.y < g.ny - R
+        && c.z < g.nz - R;
+}
+
+__device__ __forceinline__ int3 clamp_cell(const GridView& g, int3 c, int R)
+{
+    return make_int3(min(max(c.x, R), g.nx - 1 - R), min(max(c.y, R), g.ny - 1 - R),
+        min(max(c.z, R), g.nz - 1 - R));
+}
+
+// Fixed-radius neighbour traversal (the role of UniformGrid::ff_nbrs,
+// uniformgrid.cuh:113-178): (2R+1)^2 rows of cells, each a contiguous run of
+// 2R+1 x-cells in the sorted arrays bounded by two prefix entries. `pts` are
+// packed (x, y, z, mass) in grid order; f(j, pts[j], dx, dy, dz, l2) is
+// called for every candidate with l2 <= r^2 (self included, as the
+// reference's accumulation does).
+template <int R, class F>
+__device__ __forceinline__ void for_each_neighbour(const GridView& g, int3 c,
+    float xi, float yi, float zi, const float4* __restrict__ pts, F&& f)
+{
+    constexpr int ROW = 2 * R + 1;
+    int plane = (c.z - R) * g.nxny + (c.y - R) * g.nx + (c.x - R);
+#pragma unroll 1
+    for (int dz = 0; dz < ROW; ++dz, plane += g.nxny) {
+        int cid = plane;
+#pragma unroll 1
+        for (int dy = 0; dy < ROW; ++dy, cid += g.nx) {
+            const uint32_t s = __ldg(g.prefix + cid);
+            const uint32_t e = __ldg(g.prefix + cid + ROW);
+            for (uint32_t j = s; j < e; ++j) {
+                const float4 q = __ldg(pts + j);
+                const float dx = xi - q.x, dy_ = yi - q.y, dz_ = zi - q.z;
+                const float l2 = fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_));
+                if (l2 <= g.r2)
+                    f(j, q, dx, dy_, dz_, l2);
+            }
+        }
+    }
+}
+
+// ---- reductions -------------------------------------------------------------
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ unsigned warp_sum(unsigned v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// atomic max on non-negative floats through their ordered bit patterns
+__device__ __forceinline__ void atomic_max_nonneg(float* addr, float v)
+{
+    if (v > 0.f)
+        atomicMax(reinterpret_cast<unsigned*>(addr), __float_as_uint(v));
+}
+
+} // namespace reyn

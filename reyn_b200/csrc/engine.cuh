@@ -1,0 +1,148 @@
+// Host-side engine objects behind the C ABI handles: particle state, uniform
+// grid, boundary and solver. Kernels live in grid.cu and solver.cu.
+#pragma once
+
+#include "common.cuh"
+#include "device.cuh"
+
+#include <array>
+#include <memory>
+#include <vector>
+
+// C-ABI handle types are the engine classes themselves
+struct reyn_particles;
+struct reyn_grid;
+struct reyn_boundary;
+struct reyn_solver;
+
+namespace reyn {
+
+enum Field : int { FX = 0, FY, FZ, FVX, FVY, FVZ, FM, NFIELDS };
+
+// Geometry of UniformGridBuilder (uniformgrid.cu:65-96): cell = r * ratio,
+// lower bound with a 2r margin, cell counts by ceil. All float arithmetic
+// mirrors the reference so that cell keys match bit for bit.
+struct GridGeom {
+    float lo[3];
+    float cell;
+    float r;
+    int n[3];
+    int range; // 2 at ratio 0.5, 1 at ratio 1.0
+    int64_t cells() const { return int64_t(n[0]) * n[1] * n[2]; }
+};
+
+GridGeom make_geom(const float bmin[3], const float bmax[3], float r, float ratio);
+
+// The uniform grid over one set of positions.
+struct Grid {
+    GridGeom geom;
+    float ratio = 0.5f;
+    DevArray<uint32_t> counts; // C, all zero between builds
+    DevArray<uint32_t> prefix; // C + 1
+    DevArray<uint32_t> keys;   // n
+    DevArray<uint32_t> slots;  // n, unordered counting-sort output
+    DevArray<uint32_t> sorted; // n, canonical order (the permutation)
+    DevArray<uint32_t> scan_part;
+    DevArray<uint32_t> status; // 1 word of StatusBits
+    DevArray<float> extra_tmp; // reorder staging of caller arrays
+    mutable DevArray<float4> pts_tmp; // packed positions for statistics
+    uint32_t n = 0;
+    bool counts_dirty = false; // a build stopped between histogram and scatter
+    bool reordered = false;    // last build was construct_and_reorder
+    const reyn_particles* reordered_state = nullptr;
+    uint64_t reorder_epoch = 0; // state epoch produced by that reorder
+
+    GridView view(float search_radius) const;
+    // counting-sort build over positions: keys, counts, prefix, canonical
+    // `sorted`; flags particles outside the grid in `status`
+    void build(const float* x, const float* y, const float* z, uint32_t n,
+        cudaStream_t s);
+    // host check of the status word (synchronises)
+    void check_status(cudaStream_t s, const char* what);
+};
+
+} // namespace reyn
+
+// particle state: the reference's SoA arrays (current + spare for the
+// reorder swap) and the packed copies the neighbour loops read
+struct reyn_particles {
+    uint32_t n = 0;
+    float rho0 = 1.f;
+    std::array<reyn::DevArray<float>, reyn::NFIELDS> cur, alt;
+    reyn::DevArray<float4> pm;  // (x, y, z, m) in grid order
+    reyn::DevArray<float4> vel; // (vx, vy, vz, rho)
+    bool packed_valid = false;
+    uint64_t epoch = 0; // number of reorders applied
+};
+
+struct reyn_grid : reyn::Grid { };
+
+struct reyn_boundary {
+    uint32_t nb = 0;
+    float h = 0.f;
+    reyn::Grid grid;
+    reyn::DevArray<float> x, y, z, m;
+    reyn::DevArray<float4> pm;
+    reyn::GridView view() const;
+};
+
+struct reyn_solver {
+    reyn_scheme scheme;
+    reyn_params prm;
+    uint32_t n = 0;
+    reyn::DevArray<float> rho, p, aii, sii, ax, ay, az;
+    reyn::DevArray<float4> acc, vel2, bterm;
+    reyn::DevArray<float> p_tmp;
+    reyn::DevArray<unsigned char> sweep_stats; // per-sweep reductions
+    std::unique_ptr<reyn::PinnedArray<unsigned char>> readback;
+    uint64_t p_epoch = 0;      // particle epoch p is ordered for
+    const reyn_particles* p_state = nullptr;
+    reyn_step_stats stats {};
+    double pcisph_delta = 0.0; // k_c_pcisph template stiffness
+};
+
+namespace reyn {
+
+// gather of up to MAX_GATHER arrays by a permutation, plus optional packing
+constexpr int MAX_GATHER = 16;
+struct GatherArgs {
+    const float* src[MAX_GATHER];
+    float* dst[MAX_GATHER];
+    int count;
+    float4* pm;  // (x, y, z, m) from dst[FX..FZ], dst[FM]; may be null
+    float4* vel; // (vx, vy, vz, 0) from dst[FVX..FVZ]; may be null
+};
+void launch_gather(uint32_t n, const uint32_t* perm, const GatherArgs& a,
+    cudaStream_t s);
+
+// packs the particle arrays into pm/vel (after a direct SoA write)
+void pack_state(reyn_particles& st, cudaStream_t s);
+
+void reorder_state(reyn_particles& st, Grid& g, float* const* extra,
+    uint32_t n_extra, cudaStream_t s);
+
+void kernel_eval(int kind, float h_bar, const float* dx, const float* dy,
+    const float* dz, uint32_t n, float* w, float* gx, float* gy, float* gz,
+    cudaStream_t s);
+
+void neighbour_stats(const Grid& g, const float* x, const float* y,
+    const float* z, const float* m, int kind, uint32_t* count, float* len2,
+    float* rho, cudaStream_t s);
+
+void boundary_build(reyn_boundary& b, const float* bx, const float* by,
+    const float* bz, const float* bm, uint32_t nb, float h, float rho0,
+    uint32_t mass_iters, cudaStream_t s);
+
+void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& g,
+    const reyn_boundary* bdy, float dt, cudaStream_t s);
+
+float cfl_time_step(reyn_particles& st, float lambda, float h,
+    const float g[3], cudaStream_t s);
+
+void enforce_bounds(reyn_particles& st, const float lo[3], const float hi[3],
+    cudaStream_t s);
+
+// host evaluation of k_c_pcisph's template stiffness (PCISPH.cuh:49-77)
+double pcisph_template_delta(int kind, float h);
+
+} // namespace reyn

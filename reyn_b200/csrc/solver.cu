@@ -1,0 +1,772 @@
+// SESPH / PCISPH / IISPH steps on the B200. Each pass is one fixed-radius
+// neighbour kernel over the packed (x, y, z, m) copy in grid order; work the
+// reference spreads over separate kernels is fused where no neighbour reads
+// the value being written:
+//   * density also caches, per particle, the boundary sums rho_b = sum m_b W
+//     and g_b = sum m_b grad W (positions are fixed within a step, so every
+//     later boundary term of the step is a multiply by g_b);
+//   * the non-pressure pass writes v* = v + dt a into a second velocity
+//     buffer (integrate_a_v_only fused);
+//   * PCISPH's pressure pass applies v += dt a in place (it reads no
+//     neighbour velocity), so the next prediction and the final integrate
+//     see the same velocities as the reference's separate kernels;
+//   * IISPH's diagonal pass also applies the warm start; the final pressure
+//     pass integrates (v, x) and writes the SoA state.
+// Reference: solver.cuh:18-105, solver.cu, SESPH.cu:6-95, PCISPH.cuh:49-77,
+// PCISPH.cu:15-111, IISPH.cu:11-262.
+#include "engine.cuh"
+
+#include <cmath>
+#include <type_traits>
+
+namespace reyn {
+
+namespace {
+
+struct Fluid {
+    GridView g;
+    KernelConst kc;
+    const float4* __restrict__ pm; // (x, y, z, m), grid order
+    uint32_t* status;
+};
+
+struct Bdy {
+    GridView g;
+    const float4* __restrict__ pm;
+    uint32_t n;
+};
+
+// the cell of particle i in the fluid grid; positions outside it are
+// clamped (results are then meaningless) and reported through `status`
+template <int R>
+__device__ __forceinline__ int3 fluid_cell(const Fluid& f, const float4& me)
+{
+    int3 c = cell_of(f.g, me.x, me.y, me.z);
+    if (!cell_inside(f.g, c, R) || !(isfinite(me.x) && isfinite(me.y) && isfinite(me.z))) {
+        atomicOr(f.status, STATUS_OUT_OF_GRID);
+        c = clamp_cell(f.g, c, R);
+    }
+    return c;
+}
+
+// boundary neighbours of a point; a point whose cell is outside the
+// boundary grid's searchable range is farther than r from every sample
+template <class F>
+__device__ __forceinline__ void for_each_boundary(const Bdy& b, float x, float y, float z, F&& f)
+{
+    if (b.n == 0)
+        return;
+    const int3 c = cell_of(b.g, x, y, z);
+    if (!cell_inside(b.g, c, 2))
+        return;
+    for_each_neighbour<2>(b.g, c, x, y, z, b.pm, f);
+}
+
+// jacobi_update (IISPH.cu:108-117)
+__device__ __forceinline__ float jacobi_update(float omega, float a_ii, float Ap, float s)
+{
+    return ((double)a_ii < 1e-6 && (double)a_ii > -1e-6) ? 0.f
+                                                          : fmaxf(0.f, omega * (s - Ap) / a_ii);
+}
+
+// per-sweep reductions (one slot per sweep, zeroed before use)
+struct SweepStats {
+    unsigned long long over; // particles with predicted error above eta rho0
+    double err_sum;          // sum of max(0, predicted error)
+    double rho_sum;          // PCISPH: sum of predicted densities
+    float err_max;
+    float pad;
+};
+
+__device__ __forceinline__ void block_accumulate(SweepStats* st, unsigned over, double err,
+    double rho, float emax)
+{
+    __shared__ unsigned s_over[NBR_THREADS / 32];
+    __shared__ double s_err[NBR_THREADS / 32], s_rho[NBR_THREADS / 32];
+    __shared__ float s_max[NBR_THREADS / 32];
+    over = warp_sum(over);
+    err = warp_sum(err);
+    rho = warp_sum(rho);
+    emax = warp_max(emax);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        s_over[w] = over;
+        s_err[w] = err;
+        s_rho[w] = rho;
+        s_max[w] = emax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < NBR_THREADS / 32; ++k) {
+            over += s_over[k];
+            err += s_err[k];
+            rho += s_rho[k];
+            emax = fmaxf(emax, s_max[k]);
+        }
+        if (over)
+            atomicAdd(&st->over, (unsigned long long)over);
+        if (err != 0.0)
+            atomicAdd(&st->err_sum, err);
+        if (rho != 0.0)
+            atomicAdd(&st->rho_sum, rho);
+        atomic_max_nonneg(&st->err_max, emax);
+    }
+}
+
+// ---- passes ----------------------------------------------------------------
+
+// compute_densities (solver.cuh:18-38) + cached boundary sums
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bdy b,
+    float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 me = f.pm[i];
+    const int3 c = fluid_cell<R>(f, me);
+    float rf = 0.f;
+    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        [&](uint32_t, const float4& q, float, float, float, float l2) {
+            rf += q.w * pair_w<KIND>(f.kc, l2);
+        });
+    float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    for_each_boundary(b, me.x, me.y, me.z,
+        [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
+            float w, g;
+            pair_wg<KIND>(f.kc, l2, w, g);
+            rb += q.w * w;
+            const float mg = q.w * g;
+            gx += mg * dx;
+            gy += mg * dy;
+            gz += mg * dz;
+        });
+    const float r = rf + rb;
+    rho[i] = r;
+    vel[i].w = r;
+    bterm[i] = make_float4(gx, gy, gz, rb);
+}
+
+// write_non_prs_acc_ff (solver.cuh:40-69): gravity + artificial viscosity;
+// optionally fused with integrate_a_v_only (solver.cu:3-13) into vel_out
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_nonpressure(uint32_t n, Fluid f,
+    const float4* __restrict__ vel, float nu10, float eps, float3 grav, float dt,
+    float4* __restrict__ acc, float4* __restrict__ vel_out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 me = f.pm[i];
+    const float4 vi = vel[i];
+    const int3 c = fluid_cell<R>(f, me);
+    float ax = grav.x, ay = grav.y, az = grav.z;
+    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+            const float4 vj = __ldg(vel + j);
+            const float vdx = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
+            const float s = (nu10 * q.w / vj.w * vdx) / (l2 + eps) * pair_g<KIND>(f.kc, l2);
+            ax += s * dx;
+            ay += s * dy;
+            az += s * dz;
+        });
+    acc[i] = make_float4(ax, ay, az, 0.f);
+    if (vel_out)
+        vel_out[i] = make_float4(vi.x + dt * ax, vi.y + dt * ay, vi.z + dt * az, vi.w);
+}
+
+__device__ __forceinline__ float eos_sesph(float rho, float k, float rho0)
+{
+    return fmaxf(0.f, k * (rho / rho0 - 1.f)); // SESPH.cu:6-12
+}
+
+// _compute_accelerations (SESPH.cu:15-65) fused with integrate (solver.cu:
+// 15-32): writes the new SoA state
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_sesph(uint32_t n, Fluid f,
+    const float4* __restrict__ vel, const float4* __restrict__ bterm, float k, float rho0,
+    float nu10, float eps, float3 grav, float dt, float4* __restrict__ acc,
+    float* __restrict__ x, float* __restrict__ y, float* __restrict__ z,
+    float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 me = f.pm[i];
+    const float4 vi = vel[i];
+    const int3 c = fluid_cell<R>(f, me);
+    const float pi = eos_sesph(vi.w, k, rho0);
+    const float pri = pi / (vi.w * vi.w);
+    float ax = grav.x, ay = grav.y, az = grav.z;
+    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+            const float4 vj = __ldg(vel + j);
+            const float pj = eos_sesph(vj.w, k, rho0);
+            const float vdx = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
+            const float visc = (nu10 * q.w / vj.w * vdx) / (l2 + eps);
+            const float prs = q.w * (pri + pj / (vj.w * vj.w));
+            const float s = (visc - prs) * pair_g<KIND>(f.kc, l2);
+            ax += s * dx;
+            ay += s * dy;
+            az += s * dz;
+        });
+    const float4 bt = bterm[i];
+    ax -= pri * bt.x;
+    ay -= pri * bt.y;
+    az -= pri * bt.z;
+    acc[i] = make_float4(ax, ay, az, 0.f);
+    const float nvx = vi.x + dt * ax, nvy = vi.y + dt * ay, nvz = vi.z + dt * az;
+    vx[i] = nvx;
+    vy[i] = nvy;
+    vz[i] = nvz;
+    x[i] = me.x + dt * nvx;
+    y[i] = me.y + dt * nvy;
+    z[i] = me.z + dt * nvz;
+}
+
+// predict_rho (solver.cuh:71-105); the boundary part uses the cached sums:
+// sum_b m_b (W + dt grad W . v_i) = rho_b + dt g_b . v_i
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_pcisph_predict(uint32_t n, Fluid f,
+    const float4* __restrict__ vel, const float4* __restrict__ bterm, float dt,
+    float* __restrict__ rho, SweepStats* stats)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    double contrib = 0.0;
+    if (i < n) {
+        const float4 me = f.pm[i];
+        const float4 vi = vel[i];
+        const int3 c = fluid_cell<R>(f, me);
+        float r = 0.f;
+        for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+            [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+                const float4 vj = __ldg(vel + j);
+                float w, g;
+                pair_wg<KIND>(f.kc, l2, w, g);
+                const float vdx = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
+                r += q.w * (w + dt * (g * vdx));
+            });
+        const float4 bt = bterm[i];
+        r += bt.w + dt * fmaf(bt.x, vi.x, fmaf(bt.y, vi.y, bt.z * vi.z));
+        rho[i] = r;
+        contrib = r;
+    }
+    block_accumulate(stats, 0u, 0.0, contrib, 0.f);
+}
+
+// _write_pcisph_prs_acc (PCISPH.cu:21-56) + v += dt a in place
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_pcisph_pressure(uint32_t n, Fluid f,
+    const float* __restrict__ rho, const float4* __restrict__ bterm, float k, float rho0,
+    float r0i, float dt, float4* __restrict__ acc, float4* __restrict__ vel)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 me = f.pm[i];
+    const int3 c = fluid_cell<R>(f, me);
+    const float ri = rho[i];
+    const float pi = fmaxf(0.f, k * (ri - rho0));
+    const float pri = pi / (ri * ri);
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+            const float rj = __ldg(rho + j);
+            const float pj = fmaxf(0.f, k * (rj - rho0));
+            const float s = q.w * (pri + pj / (rj * rj)) * pair_g<KIND>(f.kc, l2);
+            ax += s * dx;
+            ay += s * dy;
+            az += s * dz;
+        });
+    const float4 bt = bterm[i];
+    const float cb = 0.5f * (pri + pi * r0i);
+    ax = -ax - cb * bt.x;
+    ay = -ay - cb * bt.y;
+    az = -az - cb * bt.z;
+    acc[i] = make_float4(ax, ay, az, 0.f);
+    float4 v = vel[i];
+    v.x += dt * ax;
+    v.y += dt * ay;
+    v.z += dt * az;
+    vel[i] = v;
+}
+
+// the final position update of integrate (solver.cu:15-32) when v already
+// holds v + dt a
+__global__ void k_advect(uint32_t n, const float4* __restrict__ pm,
+    const float4* __restrict__ vel, float dt, float* __restrict__ x, float* __restrict__ y,
+    float* __restrict__ z, float* __restrict__ vx, float* __restrict__ vy,
+    float* __restrict__ vz)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 p = pm[i];
+    const float4 v = vel[i];
+    vx[i] = v.x;
+    vy[i] = v.y;
+    vz[i] = v.z;
+    x[i] = p.x + dt * v.x;
+    y[i] = p.y + dt * v.y;
+    z[i] = p.z + dt * v.z;
+}
+
+// _compute_diagonal_elem_and_source_term (IISPH.cu:11-66) + warm start
+// (IISPH.cu:193-209)
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
+    const float4* __restrict__ vel, const float4* __restrict__ bterm, float rho0, float dt,
+    float omega, int warmstart, float* __restrict__ aii, float* __restrict__ sii,
+    float* __restrict__ p)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 me = f.pm[i];
+    const float4 vi = vel[i];
+    const int3 c = fluid_cell<R>(f, me);
+    float gx = 0.f, gy = 0.f, gz = 0.f, vdiv = 0.f, gsq = 0.f;
+    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+            const float4 vj = __ldg(vel + j);
+            const float g = pair_g<KIND>(f.kc, l2);
+            const float mg = q.w * g;
+            gx += mg * dx;
+            gy += mg * dy;
+            gz += mg * dz;
+            vdiv += mg * fmaf(dx, vi.x - vj.x, fmaf(dy, vi.y - vj.y, dz * (vi.z - vj.z)));
+            gsq += mg * g * l2;
+        });
+    const float4 bt = bterm[i];
+    gx += bt.x;
+    gy += bt.y;
+    gz += bt.z;
+    const float gss = fmaf(gx, gx, fmaf(gy, gy, gz * gz));
+    const float a = -dt * (gss + me.w * gsq) / (rho0 * rho0);
+    const float s = (rho0 - vi.w) / dt - (vdiv + fmaf(vi.x, bt.x, fmaf(vi.y, bt.y, vi.z * bt.z)));
+    aii[i] = a;
+    sii[i] = s;
+    p[i] = warmstart ? p[i] * 0.5f : jacobi_update(omega, a, 0.f, s);
+}
+
+// _set_pressure_accelerations (IISPH.cu:68-98)
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
+    const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
+    float4* __restrict__ acc)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 me = f.pm[i];
+    const int3 c = fluid_cell<R>(f, me);
+    const float pi = p[i];
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+            const float s = q.w * (pi + __ldg(p + j)) * pair_g<KIND>(f.kc, l2);
+            ax += s * dx;
+            ay += s * dy;
+            az += s * dz;
+        });
+    const float4 bt = bterm[i];
+    acc[i] = make_float4(-r0i * (ax + pi * bt.x), -r0i * (ay + pi * bt.y),
+        -r0i * (az + pi * bt.z), 0.f);
+}
+
+// _jacobi_update_pressures (IISPH.cu:119-162); the convergence bitmask of the
+// reference becomes a count of particles above the threshold, reduced per
+// block together with the FP64 sum of max(0, error)
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid f,
+    const float4* __restrict__ acc, const float4* __restrict__ bterm,
+    const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
+    float dt, float omega, float thr, SweepStats* stats)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned over = 0;
+    double epos = 0.0;
+    float emax = 0.f;
+    if (i < n) {
+        const float4 me = f.pm[i];
+        const int3 c = fluid_cell<R>(f, me);
+        const float4 ai = acc[i];
+        float sum = 0.f;
+        for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+            [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+                const float4 aj = __ldg(acc + j);
+                const float d = fmaf(ai.x - aj.x, dx, fmaf(ai.y - aj.y, dy, (ai.z - aj.z) * dz));
+                sum += q.w * (pair_g<KIND>(f.kc, l2) * d);
+            });
+        const float4 bt = bterm[i];
+        const float Ap = dt * (sum + fmaf(ai.x, bt.x, fmaf(ai.y, bt.y, ai.z * bt.z)));
+        const float s = sii[i];
+        p[i] = p[i] + jacobi_update(omega, aii[i], Ap, s);
+        const float err = (Ap - s) * dt;
+        over = err > thr ? 1u : 0u;
+        epos = err > 0.f ? (double)err : 0.0;
+        emax = fmaxf(err, 0.f);
+    }
+    block_accumulate(stats, over, epos, 0.0, emax);
+}
+
+// final _set_pressure_accelerations + integrate (IISPH.cu:248-257)
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f,
+    const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
+    const float4* __restrict__ vel, float dt, float4* __restrict__ acc,
+    float* __restrict__ x, float* __restrict__ y, float* __restrict__ z,
+    float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 me = f.pm[i];
+    const int3 c = fluid_cell<R>(f, me);
+    const float pi = p[i];
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+            const float s = q.w * (pi + __ldg(p + j)) * pair_g<KIND>(f.kc, l2);
+            ax += s * dx;
+            ay += s * dy;
+            az += s * dz;
+        });
+    const float4 bt = bterm[i];
+    ax = -r0i * (ax + pi * bt.x);
+    ay = -r0i * (ay + pi * bt.y);
+    az = -r0i * (az + pi * bt.z);
+    acc[i] = make_float4(ax, ay, az, 0.f);
+    const float4 v = vel[i];
+    const float nvx = v.x + dt * ax, nvy = v.y + dt * ay, nvz = v.z + dt * az;
+    vx[i] = nvx;
+    vy[i] = nvy;
+    vz[i] = nvz;
+    x[i] = me.x + dt * nvx;
+    y[i] = me.y + dt * nvy;
+    z[i] = me.z + dt * nvz;
+}
+
+__global__ void k_unpack_acc(uint32_t n, const float4* __restrict__ acc, float* __restrict__ ax,
+    float* __restrict__ ay, float* __restrict__ az)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 a = acc[i];
+    ax[i] = a.x;
+    ay[i] = a.y;
+    az[i] = a.z;
+}
+
+__global__ void k_gather_p(uint32_t n, const uint32_t* __restrict__ perm,
+    const float* __restrict__ src, float* __restrict__ dst)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        dst[i] = src[perm[i]];
+}
+
+template <class F> void dispatch(int kind, int range, F&& f)
+{
+    auto go = [&](auto K) {
+        if (range == 2)
+            f(K, std::integral_constant<int, 2> {});
+        else
+            f(K, std::integral_constant<int, 1> {});
+    };
+    switch (kind) {
+    case K_C2: go(std::integral_constant<int, K_C2> {}); break;
+    case K_B3: go(std::integral_constant<int, K_B3> {}); break;
+    case K_W6: go(std::integral_constant<int, K_W6> {}); break;
+    case K_COS: go(std::integral_constant<int, K_COS> {}); break;
+    default: fail(REYN_ERR_INVALID, "unknown kernel");
+    }
+}
+
+} // namespace
+
+// k_c_pcisph (PCISPH.cuh:49-77): host evaluation of grad W on a 5^3 lattice
+// template particle at spacing h, support 2h; returns delta*dt^2 (rounded to
+// float, as the reference's return type does)
+double pcisph_template_delta(int kind, float h)
+{
+    const KernelConst kc = make_kernel(kind, 2.f * h);
+    auto dw = [&](float q) {
+        switch (kind) {
+        case K_C2: return Shape<K_C2>::dw(q);
+        case K_B3: return Shape<K_B3>::dw(q);
+        case K_W6: return Shape<K_W6>::dw(q);
+        default: return Shape<K_COS>::dw(q);
+        }
+    };
+    const double hd = h;
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    double sum_of_sq = 0.0;
+    for (int a = -2; a <= 2; ++a)
+        for (int b = -2; b <= 2; ++b)
+            for (int c = -2; c <= 2; ++c) {
+                const float x = -((float)a * h), y = -((float)b * h), z = -((float)c * h);
+                const float l2 = std::fmaf(x, x, std::fmaf(y, y, z * z));
+                const float len = (float)std::sqrt((double)l2);
+                const float sc = kc.dw_scale * dw(len * kc.h_inv) * (1.f / len);
+                const float s = std::isfinite(sc) ? sc : 0.f;
+                const float gx = x * s, gy = y * s, gz = z * s;
+                sx += gx;
+                sy += gy;
+                sz += gz;
+                sum_of_sq += (double)std::fmaf(gx, gx, std::fmaf(gy, gy, gz * gz));
+            }
+    const double sq_of_sum = (double)std::fmaf(sx, sx, std::fmaf(sy, sy, sz * sz));
+    const double V0 = hd * hd * hd;
+    const double beta = 2. * V0 * V0;
+    return (double)(float)(1. / (beta * (sq_of_sum + sum_of_sq)));
+}
+
+static void ensure_buffers(reyn_solver& sv, uint32_t n)
+{
+    sv.rho.resize(n);
+    sv.aii.resize(n);
+    sv.sii.resize(n);
+    sv.ax.resize(n);
+    sv.ay.resize(n);
+    sv.az.resize(n);
+    sv.acc.resize(n);
+    sv.vel2.resize(n);
+    sv.bterm.resize(n);
+    if (sv.p.size() != n) {
+        sv.p.resize(n);
+        REYN_CUDA(cudaMemset(sv.p.get(), 0, size_t(n) * sizeof(float)));
+    }
+    sv.p_tmp.resize(n);
+    constexpr size_t SLOTS = 64;
+    if (sv.sweep_stats.size() == 0) {
+        sv.sweep_stats.resize(SLOTS * sizeof(SweepStats));
+        sv.readback = std::make_unique<PinnedArray<unsigned char>>(sizeof(SweepStats));
+    }
+}
+
+void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
+    const reyn_boundary* bdy, float dt, cudaStream_t s)
+{
+    const reyn_params& P = sv.prm;
+    const uint32_t n = st.n;
+    require(n == sv.n, "particle count differs from the solver's");
+    require(dt > 0.f && std::isfinite(dt), "dt must be positive and finite");
+    if (!(grid.reordered && grid.reordered_state == &st && grid.reorder_epoch == st.epoch
+            && grid.n == n))
+        fail(REYN_ERR_NOT_READY,
+            "the grid must come from construct_and_reorder over this particle state");
+    ensure_buffers(sv, n);
+    if (!st.packed_valid)
+        pack_state(st, s);
+    // IISPH carries p across steps in particle order: follow the permutation
+    if (sv.scheme == REYN_IISPH && n) {
+        if (sv.p_state == &st && sv.p_epoch + 1 == st.epoch) {
+            REYN_KERNEL("k_gather_p", s,
+                k_gather_p<<<blocks_for(n, THREADS), THREADS, 0, s>>>(
+                n, grid.sorted.get(), sv.p.get(), sv.p_tmp.get()));
+            sv.p.swap(sv.p_tmp);
+        } else if (!(sv.p_state == &st && sv.p_epoch == st.epoch)) {
+            sv.p.zero(s); // no step on this ordering yet: cold start
+        }
+        sv.p_state = &st;
+        sv.p_epoch = st.epoch;
+    }
+    sv.stats = reyn_step_stats {};
+    if (n == 0)
+        return;
+
+    Fluid f;
+    f.g = grid.view(2.f * P.h);
+    f.kc = make_kernel(P.kernel, 2.f * P.h);
+    f.pm = st.pm.get();
+    f.status = const_cast<uint32_t*>(grid.status.get());
+    Bdy b {};
+    if (bdy && bdy->nb) {
+        b.g = bdy->view();
+        b.g.r2 = f.g.r2;
+        b.pm = bdy->pm.get();
+        b.n = bdy->nb;
+    }
+    const unsigned nb = blocks_for(n, NBR_THREADS);
+    const float rho0 = P.rho0;
+    const float r0i = 1.f / (rho0 * rho0);
+    const float nu10 = 10.f * P.nu;
+    const float eps = (float)(0.01 * (double)P.h * (double)P.h);
+    const float3 grav = make_float3(P.g[0], P.g[1], P.g[2]);
+    float* X = st.cur[FX].get();
+    float* Y = st.cur[FY].get();
+    float* Z = st.cur[FZ].get();
+    float* VX = st.cur[FVX].get();
+    float* VY = st.cur[FVY].get();
+    float* VZ = st.cur[FVZ].get();
+    SweepStats* slots = reinterpret_cast<SweepStats*>(sv.sweep_stats.get());
+    SweepStats& host = *reinterpret_cast<SweepStats*>(sv.readback->get());
+    auto readback = [&](SweepStats* slot) {
+        REYN_CUDA(cudaMemcpyAsync(&host, slot, sizeof(SweepStats), cudaMemcpyDeviceToHost, s));
+        REYN_CUDA(cudaStreamSynchronize(s));
+    };
+    uint32_t iters = 0;
+    bool converged = true;
+
+    dispatch(P.kernel, grid.geom.range, [&](auto KC, auto RC) {
+        constexpr int K = decltype(KC)::value;
+        constexpr int R = decltype(RC)::value;
+        REYN_KERNEL("k_density", s,
+            k_density<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, b, sv.rho.get(), st.vel.get(),
+            sv.bterm.get()));
+        if (sv.scheme == REYN_SESPH) {
+            REYN_KERNEL("k_sesph", s,
+                k_sesph<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), sv.bterm.get(),
+                P.k_sesph, rho0, nu10, eps, grav, dt, sv.acc.get(), X, Y, Z, VX, VY, VZ));
+            iters = 1;
+        } else if (sv.scheme == REYN_PCISPH) {
+            const float kp = (float)((sv.pcisph_delta / dt) / dt); // PCISPH.cu:65
+            REYN_KERNEL("k_nonpressure", s,
+                k_nonpressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), nu10, eps, grav,
+                dt, sv.acc.get(), sv.vel2.get()));
+            float4* v = sv.vel2.get();
+            for (;;) {
+                SweepStats* slot = slots + (iters % 64);
+                REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats), s));
+                REYN_KERNEL("k_pcisph_predict", s,
+                    k_pcisph_predict<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, v, sv.bterm.get(), dt,
+                    sv.rho.get(), slot));
+                REYN_KERNEL("k_pcisph_pressure", s,
+                    k_pcisph_pressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.rho.get(),
+                    sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
+                iters += 1;
+                if (P.max_iter && iters >= P.max_iter) {
+                    if (iters >= P.min_iter) {
+                        readback(slot);
+                        converged = (float)(host.rho_sum / n) <= (P.eta + 1.f) * rho0;
+                    }
+                    break;
+                }
+                if (iters < P.min_iter)
+                    continue;
+                readback(slot);
+                const float avg = (float)(host.rho_sum / n);
+                sv.stats.avg_density_error = std::max(0.0, host.rho_sum / n / rho0 - 1.0);
+                if (!(avg > (P.eta + 1.f) * rho0)) // PCISPH.cu:101
+                    break;
+            }
+            REYN_KERNEL("k_advect", s,
+                k_advect<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, st.pm.get(), v, dt, X, Y, Z,
+                VX, VY, VZ));
+        } else { // IISPH
+            REYN_KERNEL("k_nonpressure", s,
+                k_nonpressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), nu10, eps, grav,
+                dt, sv.acc.get(), sv.vel2.get()));
+            REYN_KERNEL("k_iisph_diag", s,
+                k_iisph_diag<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(), sv.bterm.get(),
+                rho0, dt, P.omega, P.warmstart, sv.aii.get(), sv.sii.get(), sv.p.get()));
+            const float thr = P.eta * rho0;
+            for (;;) {
+                SweepStats* slot = slots + (iters % 64);
+                REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats), s));
+                REYN_KERNEL("k_iisph_pacc", s,
+                    k_iisph_pacc<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
+                    r0i, sv.acc.get()));
+                REYN_KERNEL("k_iisph_jacobi", s,
+                    k_iisph_jacobi<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.acc.get(),
+                    sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, thr,
+                    slot));
+                iters += 1;
+                const bool last = P.max_iter && iters >= P.max_iter;
+                if (iters < P.min_iter && !last)
+                    continue;
+                readback(slot);
+                sv.stats.avg_density_error = host.err_sum / n / rho0;
+                sv.stats.max_density_error = host.err_max / rho0;
+                const bool more = P.convergence == REYN_CONV_AVERAGE
+                    ? host.err_sum / n > (double)P.eta * rho0
+                    : host.over > 0; // IISPH.cu:246
+                if (!more)
+                    break;
+                if (last) {
+                    converged = false;
+                    break;
+                }
+            }
+            REYN_KERNEL("k_iisph_final", s,
+                k_iisph_final<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
+                r0i, sv.vel2.get(), dt, sv.acc.get(), X, Y, Z, VX, VY, VZ));
+        }
+    });
+    REYN_KERNEL("k_unpack_acc", s,
+        k_unpack_acc<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, sv.acc.get(), sv.ax.get(),
+        sv.ay.get(), sv.az.get()));
+    st.packed_valid = false; // positions moved: the packed copy is stale
+    sv.stats.iters = iters;
+    if (!converged)
+        fail(REYN_ERR_ITER_LIMIT, "solver reached max_iter before converging (step completed)");
+}
+
+// ---- time step and bounds ------------------------------------------------------
+
+__global__ void k_vmax(uint32_t n, const float* __restrict__ vx, const float* __restrict__ vy,
+    const float* __restrict__ vz, float* out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float v = 0.f;
+    if (i < n)
+        v = norm3df(vx[i], vy[i], vz[i]); // cfl.cu:13-18
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0)
+        atomic_max_nonneg(out, v);
+}
+
+float cfl_time_step(reyn_particles& st, float lambda, float h, const float g[3], cudaStream_t s)
+{
+    DevArray<float> d(1);
+    d.zero(s);
+    if (st.n) {
+        REYN_KERNEL("k_vmax", s,
+            k_vmax<<<blocks_for(st.n, THREADS), THREADS, 0, s>>>(st.n, st.cur[FVX].get(),
+            st.cur[FVY].get(), st.cur[FVZ].get(), d.get()));
+    }
+    float vmax = 0.f;
+    REYN_CUDA(cudaMemcpyAsync(&vmax, d.get(), sizeof(float), cudaMemcpyDeviceToHost, s));
+    REYN_CUDA(cudaStreamSynchronize(s));
+    // cfl.cu:22-36
+    const float dt_vel = lambda * h / vmax;
+    const float gn = (float)std::sqrt((double)std::fmaf(g[0], g[0], std::fmaf(g[1], g[1], g[2] * g[2])));
+    const float dt_g = std::sqrt((float)(2. * lambda * h / (double)gn));
+    return std::fmin(dt_vel, dt_g);
+}
+
+// _hard_enforce_bounds (scene.cu:466-483)
+__global__ void k_bounds_enforce(uint32_t n, float3 lo, float3 hi, float* __restrict__ x,
+    float* __restrict__ y, float* __restrict__ z, float* __restrict__ vx,
+    float* __restrict__ vy, float* __restrict__ vz)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float px = x[i], py = y[i], pz = z[i];
+    if (px <= lo.x || py <= lo.y || pz <= lo.z || hi.x <= px || hi.y <= py || hi.z <= pz) {
+        const float d = (float)-0.1;
+        vx[i] = vx[i] * d;
+        vy[i] = vy[i] * d;
+        vz[i] = vz[i] * d;
+    }
+    x[i] = fmaxf(fminf(px, hi.x), lo.x);
+    y[i] = fmaxf(fminf(py, hi.y), lo.y);
+    z[i] = fmaxf(fminf(pz, hi.z), lo.z);
+}
+
+void enforce_bounds(reyn_particles& st, const float lo[3], const float hi[3], cudaStream_t s)
+{
+    if (!st.n)
+        return;
+    REYN_KERNEL("k_bounds_enforce", s,
+        k_bounds_enforce<<<blocks_for(st.n, THREADS), THREADS, 0, s>>>(st.n,
+        make_float3(lo[0], lo[1], lo[2]), make_float3(hi[0], hi[1], hi[2]), st.cur[FX].get(),
+        st.cur[FY].get(), st.cur[FZ].get(), st.cur[FVX].get(), st.cur[FVY].get(),
+        st.cur[FVZ].get()));
+    st.packed_valid = false;
+}
+
+} // namespace reyn

@@ -1,0 +1,156 @@
+"""Seeded synthetic scenes for the workloads the engine is measured on.
+
+Each scene is a fluid block on a cubic lattice with seeded uniform jitter,
+standing in the lower corner of a closed box whose six walls are sampled with
+one layer of boundary particles on a square lattice. "Up" is +y: gravity is
+(0, -9.81, 0), the reference solvers' hard-coded axis (PCISPH.cuh:27,
+IISPH.cuh:37). Fluid masses are rho0 h^3 (the reference's _init_box_kernel,
+scene.cu:14-37). Boundary masses are left to the Akinci refinement
+(calculate_boundary_masses, sample_boundary.cu:267-297).
+
+The generator is numpy with a PCG64 seed, so every machine builds the same
+scene bit for bit.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Scene:
+    name: str
+    h: float                 # particle spacing
+    rho0: float
+    fluid: dict              # x, y, z, vx, vy, vz, m, id (float32)
+    bdy: dict                # x, y, z (float32)
+    box_min: np.ndarray
+    box_max: np.ndarray
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return int(self.fluid["x"].size)
+
+    @property
+    def nb(self) -> int:
+        return int(self.bdy["x"].size)
+
+
+def box_walls(box_min, box_max, spacing: float) -> dict:
+    """One layer of samples on the six faces of an axis-aligned box, on a
+    square lattice of the given spacing (no duplicates at edges/corners)."""
+    lo = np.asarray(box_min, np.float64)
+    hi = np.asarray(box_max, np.float64)
+    n = np.rint((hi - lo) / spacing).astype(np.int64)
+    axes = [np.arange(k + 1) for k in n]
+    pts = []
+    # x faces (full), y faces (x interior), z faces (x, y interior)
+    for ix in (0, n[0]):
+        j, k = np.meshgrid(axes[1], axes[2], indexing="ij")
+        pts.append(np.stack([np.full(j.size, ix), j.ravel(), k.ravel()], 1))
+    for iy in (0, n[1]):
+        i, k = np.meshgrid(axes[0][1:-1], axes[2], indexing="ij")
+        pts.append(np.stack([i.ravel(), np.full(i.size, iy), k.ravel()], 1))
+    for iz in (0, n[2]):
+        i, j = np.meshgrid(axes[0][1:-1], axes[1][1:-1], indexing="ij")
+        pts.append(np.stack([i.ravel(), j.ravel(), np.full(i.size, iz)], 1))
+    p = np.concatenate(pts, 0).astype(np.float64)
+    xyz = lo + p * ((hi - lo) / n)
+    return {"x": xyz[:, 0].astype(np.float32), "y": xyz[:, 1].astype(np.float32),
+            "z": xyz[:, 2].astype(np.float32)}
+
+
+_ALPHA = {"C2": 21.0 / (2.0 * np.pi), "B3": 16.0 / np.pi, "W6": 1365.0 / (64.0 * np.pi),
+          "COS": np.pi / (4.0 * np.pi ** 2 - 30.0)}
+
+
+def _shape(kernel: str, q: np.ndarray) -> np.ndarray:
+    """Kernel shape functions w(q) of the four smoothing kernels."""
+    t = np.maximum(0.0, 1.0 - q)
+    if kernel == "C2":
+        return t ** 4 * (4 * q + 1)
+    if kernel == "B3":
+        return t ** 3 - 4 * np.clip(0.5 - q, 0, 1) ** 3
+    if kernel == "W6":
+        return t ** 8 * (32 * q ** 3 + 25 * q ** 2 + 8 * q + 1)
+    qq = np.minimum(1.0, q)
+    return 4 * np.cos(np.pi * qq) + np.cos(2 * np.pi * qq) + 3
+
+
+def lattice_density_factor(kernel: str) -> float:
+    """sum_j h^3 W(x_ij) over a cubic lattice of spacing h at support 2h: the
+    SPH density of a perfect lattice of masses rho0 h^3, in units of rho0
+    (C2 1.034, B3 1.000, W6 1.169, COS 0.988)."""
+    r = np.arange(-2, 3, dtype=np.float64)
+    X, Y, Z = np.meshgrid(r, r, r, indexing="ij")
+    q = np.sqrt(X ** 2 + Y ** 2 + Z ** 2).ravel() / 2.0
+    return float((_ALPHA[kernel] / 8.0 * _shape(kernel, np.minimum(q, 1.0))).sum())
+
+
+def fluid_block(counts, h: float, origin, rho0: float, jitter: float, seed: int,
+                velocity_noise: float = 0.0, mass_kernel: str | None = None) -> dict:
+    """counts[0] x counts[1] x counts[2] lattice at spacing h from `origin`
+    with uniform jitter in [-jitter, jitter] * h; x varies fastest."""
+    nx, ny, nz = counts
+    rng = np.random.Generator(np.random.PCG64(seed))
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    base = np.stack([i.ravel(), j.ravel(), k.ravel()], 1).astype(np.float64) * h
+    base += np.asarray(origin, np.float64)
+    n = base.shape[0]
+    if jitter:
+        base += rng.uniform(-jitter, jitter, size=(n, 3)) * h
+    v = np.zeros((n, 3))
+    if velocity_noise:
+        v = rng.uniform(-velocity_noise, velocity_noise, size=(n, 3))
+    m = np.float32(np.float32(np.float32(rho0) * np.float32(h)) * np.float32(h)) * np.float32(h)
+    if mass_kernel:
+        # calibrated so that the unjittered lattice sits exactly at rho0
+        m = np.float32(float(m) / lattice_density_factor(mass_kernel))
+    return {"x": base[:, 0].astype(np.float32), "y": base[:, 1].astype(np.float32),
+            "z": base[:, 2].astype(np.float32), "vx": v[:, 0].astype(np.float32),
+            "vy": v[:, 1].astype(np.float32), "vz": v[:, 2].astype(np.float32),
+            "m": np.full(n, m, np.float32), "id": np.arange(n, dtype=np.float32)}
+
+
+def dam_break(counts, h: float, box, rho0: float = 1000.0, jitter: float = 0.1,
+              seed: int = 1, velocity_noise: float = 0.0, name: str = "dam_break",
+              mass_kernel: str | None = None) -> Scene:
+    """A fluid block one spacing away from the lower corner of box [0, box].
+    Fluid masses are rho0 h^3 (the reference's), or calibrated to the lattice
+    density of `mass_kernel` when given."""
+    box_max = np.asarray(box, np.float32)
+    box_min = np.zeros(3, np.float32)
+    fl = fluid_block(counts, h, (h, h, h), rho0, jitter, seed, velocity_noise, mass_kernel)
+    bd = box_walls(box_min, box_max, h)
+    return Scene(name, h, rho0, fl, bd, box_min, box_max,
+                 {"counts": list(counts), "box": list(map(float, box)), "jitter": jitter,
+                  "seed": seed})
+
+
+def sesph_small(seed: int = 1) -> Scene:
+    """SESPH dam break: 32^3 fluid particles at spacing 0.02, jitter +-0.1 h,
+    unit box with Akinci walls at spacing 0.02."""
+    return dam_break((32, 32, 32), 0.02, (1.0, 1.0, 1.0), 1000.0, 0.1, seed,
+                     name="sesph_32k")
+
+
+def iisph_4m(seed: int = 3) -> Scene:
+    """IISPH dam break: 256 x 128 x 128 = 4,194,304 fluid particles at spacing
+    0.005, jitter +-0.05 h, in a 2 x 1 x 1 box with Akinci walls; masses
+    calibrated to the Wendland C2 lattice density."""
+    return dam_break((256, 128, 128), 0.005, (2.0, 1.0, 1.0), 1000.0, 0.05, seed,
+                     name="iisph_4m", mass_kernel="C2")
+
+
+def uniform_cloud(n: int = 1 << 20, seed: int = 2):
+    """Neighbour-search microbenchmark: n uniform-random points in [0,1)^3."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    p = rng.random((n, 3), dtype=np.float32)
+    return p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy()
+
+
+def scaled(counts, h: float, box, **kw) -> Scene:
+    """A smaller dam break with the same structure (for parity tests)."""
+    return dam_break(counts, h, box, **kw)
