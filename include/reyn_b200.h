@@ -157,7 +157,7 @@ int reyn_boundary_destroy(reyn_boundary* b);
 int reyn_boundary_arrays(const reyn_boundary* b, const float** bx,
     const float** by, const float** bz, const float** bm, uint32_t* nb);
 
-/* ---- solvers (src/solvers/*) --------------------------------------------- */
+/* ---- solvers (src/solvers/SESPH, PCISPH, IISPH) ------------------------- */
 typedef enum reyn_scheme {
     REYN_SESPH = 0, /* SESPH.cu:68-95   */
     REYN_PCISPH = 1, /* PCISPH.cu:59-111 */

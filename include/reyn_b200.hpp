@@ -1,0 +1,325 @@
+// reyn_b200 C++ adapters: header-only wrappers over the C ABI (reyn_b200.h)
+// that reproduce the reference's (reyn) C++ surface, so that a loop written
+// against the reference —
+//
+//     Particles state(N, rho0);
+//     UniformGridBuilder builder(bmin, bmax, 2.f * h);
+//     IISPH<B3, Resort::yes> solver(W, N, nu, h, rho0);
+//     dt = simple_dt_controller(iters, dt, 1.0, h, state, g, 10, 0.001f);
+//     const auto grid { builder.construct_and_reorder(2.f * h, state) };
+//     iters = solver.step(state, grid, bdy, dt);
+//     hard_enforce_bounds(state, bmin, bmax);
+//
+// (main.cu:60-78) — compiles against this header with the reyn:: namespace.
+// Differences from the reference, by design of the C ABI: the solvers own
+// their per-particle buffers (the reference takes caller DeviceBuffers,
+// SESPH.cuh:37-41 etc.), the IISPH pressure follows reorders automatically
+// (main.cu:68 passes it as an extra buffer), errors are exceptions carrying
+// the C status code instead of exit() (common.h:24-36), and every call takes
+// an optional cudaStream_t.
+#ifndef REYN_B200_HPP_
+#define REYN_B200_HPP_
+
+#include "reyn_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace reyn {
+
+class Error : public std::runtime_error {
+public:
+    Error(int code, const std::string& msg)
+        : std::runtime_error("reyn_b200 error " + std::to_string(code) + ": " + msg)
+        , code_(code)
+    {
+    }
+    int code() const { return code_; }
+
+private:
+    int code_;
+};
+
+inline void check(int rc)
+{
+    if (rc != REYN_OK)
+        throw Error(rc, reyn_last_error());
+}
+
+// uniformgrid.cuh:70
+enum class Resort : bool { no = false, yes = true };
+
+// ---- smoothing kernels (kernels.cuh:78-165): tags carrying h_bar ----------
+template <reyn_kernel KIND> struct KernelTag {
+    static constexpr reyn_kernel kind = KIND;
+    float h_bar;
+    explicit KernelTag(float h) : h_bar(h) { }
+};
+using C2 = KernelTag<REYN_KERNEL_C2>;
+using B3 = KernelTag<REYN_KERNEL_B3>;
+using W6 = KernelTag<REYN_KERNEL_W6>;
+using COS = KernelTag<REYN_KERNEL_COS>;
+
+// ---- Particles (particles.cuh:25-75) ----------------------------------------
+class Particles {
+public:
+    Particles(uint32_t n, float rho0) { check(reyn_particles_create(n, rho0, &h_)); }
+    ~Particles() { reyn_particles_destroy(h_); }
+    Particles(const Particles&) = delete;
+    Particles& operator=(const Particles&) = delete;
+
+    // SoA device pointers (DeviceBuffer::ptr()); they change after a reorder
+    reyn_soa soa()
+    {
+        reyn_soa s {};
+        check(reyn_particles_soa(h_, &s));
+        return s;
+    }
+    uint32_t size() const { return n(); }
+    void upload(const float* xx, const float* xy, const float* xz, const float* vx,
+        const float* vy, const float* vz, const float* m, cudaStream_t s = nullptr)
+    {
+        check(reyn_particles_upload(h_, xx, xy, xz, vx, vy, vz, m, s));
+        if (cudaStreamSynchronize(s) != cudaSuccess)
+            throw Error(REYN_ERR_CUDA, "stream synchronisation after upload failed");
+    }
+    void download(float* xx, float* xy, float* xz, float* vx, float* vy, float* vz, float* m,
+        cudaStream_t s = nullptr)
+    {
+        check(reyn_particles_download(h_, xx, xy, xz, vx, vy, vz, m, s));
+    }
+    reyn_particles* handle() { return h_; }
+
+private:
+    uint32_t n() const
+    {
+        reyn_soa s {};
+        reyn_particles_soa(h_, &s);
+        return s.n;
+    }
+    reyn_particles* h_ = nullptr;
+};
+
+// ---- UniformGrid<R> (uniformgrid.cuh:84-179) --------------------------------
+template <Resort R> struct UniformGrid {
+    reyn_grid_info info;
+    const reyn_grid* grid;
+};
+
+// ---- UniformGridBuilder (uniformgrid.cuh:200-489) ---------------------------
+class UniformGridBuilder {
+public:
+    UniformGridBuilder(float3 bound_min, float3 bound_max, float search_radius,
+        float cell_ratio = 0.5f)
+    {
+        const float lo[3] = { bound_min.x, bound_min.y, bound_min.z };
+        const float hi[3] = { bound_max.x, bound_max.y, bound_max.z };
+        check(reyn_grid_create(lo, hi, search_radius, cell_ratio, REYN_ORDER_XYZ, &g_));
+    }
+    ~UniformGridBuilder() { reyn_grid_destroy(g_); }
+    UniformGridBuilder(const UniformGridBuilder&) = delete;
+    UniformGridBuilder& operator=(const UniformGridBuilder&) = delete;
+
+    // construct (uniformgrid.cu:145-156): positions are not moved
+    UniformGrid<Resort::no> construct(float search_radius, const float* xx, const float* xy,
+        const float* xz, uint32_t n, cudaStream_t s = nullptr)
+    {
+        check(reyn_grid_construct(g_, search_radius, xx, xy, xz, n, s));
+        return { info(), g_ };
+    }
+
+    // construct_and_reorder (uniformgrid.cuh:477-483): the state and any
+    // extra device arrays of n floats are permuted into grid order
+    template <class... Extra>
+    UniformGrid<Resort::yes> construct_and_reorder(float search_radius, Particles& state,
+        Extra*... extra)
+    {
+        float* ex[] = { static_cast<float*>(extra)..., nullptr };
+        check(reyn_grid_construct_and_reorder(g_, search_radius, state.handle(), ex,
+            (uint32_t)sizeof...(Extra), nullptr));
+        return { info(), g_ };
+    }
+    UniformGrid<Resort::yes> construct_and_reorder_on(cudaStream_t s, float search_radius,
+        Particles& state, std::vector<float*> extra = {})
+    {
+        check(reyn_grid_construct_and_reorder(g_, search_radius, state.handle(), extra.data(),
+            (uint32_t)extra.size(), s));
+        return { info(), g_ };
+    }
+
+    reyn_grid_info info() const
+    {
+        reyn_grid_info i {};
+        check(reyn_grid_info_get(g_, &i));
+        return i;
+    }
+
+private:
+    reyn_grid* g_ = nullptr;
+};
+
+// ---- BoundarySamples (scene.cuh:29-46) ----------------------------------------
+class BoundarySamples {
+public:
+    // device arrays of nb samples; masses computed (Akinci) when m == nullptr
+    BoundarySamples(const float* xs, const float* ys, const float* zs, const float* m,
+        uint32_t nb, float h, float rho0, uint32_t mass_iters = 5, cudaStream_t s = nullptr)
+    {
+        check(reyn_boundary_create(xs, ys, zs, m, nb, h, rho0, mass_iters, s, &b_));
+    }
+    ~BoundarySamples() { reyn_boundary_destroy(b_); }
+    BoundarySamples(const BoundarySamples&) = delete;
+    BoundarySamples& operator=(const BoundarySamples&) = delete;
+    const reyn_boundary* handle() const { return b_; }
+
+private:
+    reyn_boundary* b_ = nullptr;
+};
+
+// ---- solvers -----------------------------------------------------------------
+namespace detail {
+    template <class K>
+    reyn_params params(reyn_scheme scheme, const K& W, float nu, float h, float rho0)
+    {
+        if (W.h_bar != 2.f * h)
+            throw Error(REYN_ERR_INVALID, "the engine's kernel support is 2h (main.cu:51)");
+        reyn_params p {};
+        check(reyn_params_reference(scheme, K::kind, h, rho0, nu, &p));
+        return p;
+    }
+
+    class Solver {
+    public:
+        Solver(reyn_scheme scheme, const reyn_params& p, uint32_t n)
+        {
+            check(reyn_solver_create(scheme, &p, n, &s_));
+        }
+        ~Solver() { reyn_solver_destroy(s_); }
+        Solver(const Solver&) = delete;
+        Solver& operator=(const Solver&) = delete;
+        uint32_t step(Particles& st, const reyn_grid* g, const BoundarySamples* bdy, float dt,
+            cudaStream_t s)
+        {
+            uint32_t it = 0;
+            check(reyn_solver_step(s_, st.handle(), g, bdy ? bdy->handle() : nullptr, dt, &it, s));
+            return it;
+        }
+        reyn_solver_buffers buffers() const
+        {
+            reyn_solver_buffers b {};
+            check(reyn_solver_buffers_get(s_, &b));
+            return b;
+        }
+        reyn_step_stats stats() const
+        {
+            reyn_step_stats t {};
+            check(reyn_solver_stats(s_, &t));
+            return t;
+        }
+
+    private:
+        reyn_solver* s_ = nullptr;
+    };
+} // namespace detail
+
+// SESPH<K,R> (SESPH.cuh:11-68): step returns nothing, like the reference
+template <class K, Resort R = Resort::yes> class SESPH : public detail::Solver {
+    static_assert(R == Resort::yes, "the engine's solvers run on reordered state");
+
+public:
+    SESPH(K W, uint32_t N, float nu, float h, float rho0,
+        float3 g = make_float3(0.f, -9.81f, 0.f), float k = 500.f)
+        : detail::Solver(REYN_SESPH, with(detail::params(REYN_SESPH, W, nu, h, rho0), g, k), N)
+    {
+    }
+    void step(Particles& st, const UniformGrid<R>& grid, const BoundarySamples& bdy, float dt,
+        cudaStream_t s = nullptr)
+    {
+        detail::Solver::step(st, grid.grid, &bdy, dt, s);
+    }
+
+private:
+    static reyn_params with(reyn_params p, float3 g, float k)
+    {
+        p.g[0] = g.x;
+        p.g[1] = g.y;
+        p.g[2] = g.z;
+        p.k_sesph = k;
+        return p;
+    }
+};
+
+// PCISPH<K,R> (PCISPH.cuh:8-111): step returns the iteration count
+template <class K, Resort R = Resort::yes> class PCISPH : public detail::Solver {
+    static_assert(R == Resort::yes, "the engine's solvers run on reordered state");
+
+public:
+    PCISPH(K W, uint32_t N, float nu, float h, float rho0)
+        : detail::Solver(REYN_PCISPH, detail::params(REYN_PCISPH, W, nu, h, rho0), N)
+    {
+    }
+    uint32_t step(Particles& st, const UniformGrid<R>& grid, const BoundarySamples& bdy,
+        float dt, cudaStream_t s = nullptr)
+    {
+        return detail::Solver::step(st, grid.grid, &bdy, dt, s);
+    }
+};
+
+// IISPH<K,R> (IISPH.cuh:8-93): step returns the iteration count
+template <class K, Resort R = Resort::yes> class IISPH : public detail::Solver {
+    static_assert(R == Resort::yes, "the engine's solvers run on reordered state");
+
+public:
+    IISPH(K W, uint32_t N, float nu, float h, float rho0)
+        : detail::Solver(REYN_IISPH, detail::params(REYN_IISPH, W, nu, h, rho0), N)
+    {
+    }
+    // the configurable form: any reyn_params (e.g. the average-error criterion)
+    IISPH(const reyn_params& p, uint32_t N)
+        : detail::Solver(REYN_IISPH, p, N)
+    {
+    }
+    uint32_t step(Particles& st, const UniformGrid<R>& grid, const BoundarySamples& bdy,
+        float dt, cudaStream_t s = nullptr)
+    {
+        return detail::Solver::step(st, grid.grid, &bdy, dt, s);
+    }
+};
+
+// ---- time step and bounds (cfl.cuh:13-32, scene.cu:485-491) --------------------
+inline float cfl_time_step(float lambda, float h, Particles& state, float3 g,
+    cudaStream_t s = nullptr)
+{
+    const float gg[3] = { g.x, g.y, g.z };
+    float dt = 0.f;
+    check(reyn_cfl_time_step(state.handle(), lambda, h, gg, &dt, s));
+    return dt;
+}
+
+inline float simple_dt_controller(uint32_t iter_last, float dt_last, float lambda, float h,
+    Particles& state, float3 g, uint32_t iter_target = 5, float change_factor = 0.01f,
+    cudaStream_t s = nullptr)
+{
+    const float gg[3] = { g.x, g.y, g.z };
+    float dt = 0.f;
+    check(reyn_dt_controller(state.handle(), iter_last, dt_last, lambda, h, gg, iter_target,
+        change_factor, &dt, s));
+    return dt;
+}
+
+inline void hard_enforce_bounds(Particles& state, float3 bound_min, float3 bound_max,
+    cudaStream_t s = nullptr)
+{
+    const float lo[3] = { bound_min.x, bound_min.y, bound_min.z };
+    const float hi[3] = { bound_max.x, bound_max.y, bound_max.z };
+    check(reyn_enforce_bounds(state.handle(), lo, hi, s));
+}
+
+} // namespace reyn
+
+#endif // REYN_B200_HPP_

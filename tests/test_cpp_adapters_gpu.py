@@ -1,0 +1,85 @@
+"""The C++ adapter layer (include/reyn_b200.hpp): the reference's main loop
+(main.cu:60-78) written against reyn::Particles / UniformGridBuilder /
+IISPH<C2> / simple_dt_controller / hard_enforce_bounds must drive the engine
+to exactly the state the C ABI reaches when called directly, and that state
+must agree with the CPU oracle."""
+import os
+import shutil
+import struct
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+from reyn_b200 import scenes
+from tests.helpers import assert_close
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def compile_main_loop(tmp):
+    exe = os.path.join(tmp, "main_loop")
+    cxx = shutil.which("g++") or "g++"
+    subprocess.run([cxx, "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"),
+                    "-I/usr/local/cuda/include", os.path.join(ROOT, "tests", "cpp", "main_loop.cpp"),
+                    "-L" + os.path.join(ROOT, "reyn_b200"), "-lreyn_b200",
+                    "-L/usr/local/cuda/lib64", "-lcudart",
+                    "-Wl,-rpath," + os.path.join(ROOT, "reyn_b200"), "-o", exe], check=True)
+    return exe
+
+
+def write_scene(path, sc, bm, steps, dt0, lam, nu):
+    with open(path, "wb") as f:
+        f.write(struct.pack("<3I", sc.n, sc.nb, steps))
+        f.write(struct.pack("<11f", sc.h, sc.rho0, nu, dt0, lam, *sc.box_min, *sc.box_max))
+        for k in ("x", "y", "z", "vx", "vy", "vz", "m", "id"):
+            f.write(np.ascontiguousarray(sc.fluid[k], np.float32).tobytes())
+        for a in (sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], bm):
+            f.write(np.ascontiguousarray(a, np.float32).tobytes())
+
+
+def read_out(path, n):
+    raw = open(path, "rb").read()
+    steps = struct.unpack("<I", raw[:4])[0]
+    iters = np.frombuffer(raw[4:4 + 4 * steps], np.uint32)
+    dts = np.frombuffer(raw[4 + 4 * steps:4 + 8 * steps], np.float32)
+    body = np.frombuffer(raw[4 + 8 * steps:], np.float32).reshape(7, n)
+    return iters, dts, dict(zip(("x", "y", "z", "vx", "vy", "vz", "id"), body))
+
+
+def test_cpp_main_loop_matches_oracle(cuda, tmp_path):
+    exe = compile_main_loop(str(tmp_path))
+    sc = scenes.dam_break((14, 12, 10), 0.02, (0.5, 0.5, 0.5), velocity_noise=0.02, seed=21)
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    steps, dt0, lam, nu = 3, 1e-3, 0.4, 0.01
+    inp = os.path.join(str(tmp_path), "in.bin")
+    out = os.path.join(str(tmp_path), "out.bin")
+    write_scene(inp, sc, bm, steps, dt0, lam, nu)
+    subprocess.run([exe, inp, out], check=True)
+    iters, dts, got = read_out(out, sc.n)
+
+    # the same loop on the oracle
+    fl = {k: v.copy() for k, v in sc.fluid.items()}
+    p = np.zeros(sc.n, np.float32)
+    prm = oracle.reference_params(2, 0, sc.h, sc.rho0, nu)
+    it, dt = 0, dt0
+    want_iters, want_dts = [], []
+    for _ in range(steps):
+        dt = float(oracle.lib().orc_dt_controller(it, dt, lam, sc.h, sc.n, fl["vx"], fl["vy"],
+                                                  fl["vz"], oracle.f32([0, -9.81, 0]), 10,
+                                                  0.001))
+        r = oracle.run(prm, fl, dict(sc.bdy, m=bm), sc.box_min, sc.box_max, dt, 1, p0=p)
+        fl, p, it = dict(r.state), r.p, int(r.iters[0])
+        want_iters.append(it)
+        want_dts.append(dt)
+    assert list(iters) == want_iters
+    np.testing.assert_allclose(dts, want_dts, rtol=1e-5)
+    go = np.argsort(got["id"])
+    wo = np.argsort(fl["id"])
+    for k in ("x", "y", "z"):
+        assert_close(got[k][go], fl[k][wo], 1e-6, 1e-6, k)
+    for k in ("vx", "vy", "vz"):
+        assert_close(got[k][go], fl[k][wo], 1e-3, 1e-3, k)
