@@ -71,11 +71,22 @@ def parse_args():
     return ap.parse_args()
 
 
+NU = 0.01
+LAMBDA = 0.4
+DT0 = 5e-4
+
+
 def scene_for(rank: int, scale: int):
     from reyn_b200 import scenes
     counts = (256 // scale, 128 // scale, 128 // scale)
     return scenes.dam_break(counts, 0.005 * scale, (2.0, 1.0, 1.0), 1000.0, 0.05,
-                            seed=3 + rank, name=WORKLOAD, mass_kernel="C2")
+                            seed=3 + rank, name=WORKLOAD, mass_kernel="C2", gap=1.5)
+
+
+def viscous_dt_limit(h: float, nu: float) -> float:
+    """Explicit-viscosity stability bound of the artificial viscosity term
+    (solver.cuh:62-63): dt <= 0.08 h^2 / nu (2e-4 s at h = 0.005, nu = 0.01)."""
+    return 0.08 * h * h / nu
 
 
 def peaks():
@@ -173,6 +184,65 @@ def max_over_ranks(world, v: float) -> float:
 
 # ---- engine arm ---------------------------------------------------------------
 
+class EngineRun:
+    """The workload on the engine: one scene, its grid, boundary and solver,
+    and the main-loop step (main.cu:64-75)."""
+
+    def __init__(self, rank: int, scale: int, dev):
+        import torch
+
+        import reyn_b200 as rb
+
+        self.rb = rb
+        self.sc = sc = scene_for(rank, scale)
+        self.n = sc.n
+        self.st = rb.Particles(sc.n, sc.rho0)
+        self.st.upload(sc.fluid)
+        self.bd = rb.Boundary(*(torch.tensor(sc.bdy[k], device=dev) for k in ("x", "y", "z")),
+                              None, h=sc.h, rho0=sc.rho0, mass_iters=5)
+        self.grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h)
+        prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, NU)
+        prm.convergence = rb.CONV_AVERAGE
+        prm.eta = 0.001
+        prm.max_iter = 1000
+        self.sv = rb.Solver(rb.IISPH, prm, sc.n)
+        self.dt, self.iters = DT0, 0
+        self.dt_visc = viscous_dt_limit(sc.h, NU)
+        self.log = []
+        self.limit_hits = 0
+
+    def step(self, S):
+        rb, sc = self.rb, self.sc
+        # simple_dt_controller (cfl.cu:39-52) at lambda 0.4, capped by the
+        # explicit-viscosity bound
+        self.dt = min(rb.dt_controller(self.st, self.iters, self.dt, LAMBDA, sc.h,
+                                       (0.0, -9.81, 0.0), 10, 0.001, stream=S), self.dt_visc)
+        self.grid.construct_and_reorder(self.st, stream=S)
+        try:
+            it = self.sv.step(self.st, self.grid, self.bd, self.dt, stream=S)
+        except rb.ReynError as e:
+            if e.code != rb.ERR_ITER_LIMIT:
+                raise
+            it = self.sv.stats().iters
+            self.limit_hits += 1
+        self.iters = it
+        self.log.append((it, self.sv.stats().avg_density_error, self.dt))
+        rb.enforce_bounds(self.st, sc.box_min, sc.box_max, stream=S)
+
+    def checkpoint(self):
+        return (self.st.download(), self.sv.pressure(), self.dt, self.iters)
+
+    def restore(self, ck):
+        state, p, dt, iters = ck
+        self.st.upload(state)
+        self.sv.set_pressure(self.st, p)
+        self.dt, self.iters = dt, iters
+
+    def close(self):
+        for o in (self.sv, self.grid, self.bd, self.st):
+            o.close()
+
+
 def run_engine(a, world, rank, local):
     import torch
 
@@ -180,47 +250,16 @@ def run_engine(a, world, rank, local):
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    sc = scene_for(rank, a.scale)
-    n = sc.n
-    st = rb.Particles(n, sc.rho0)
-    st.upload(sc.fluid)
-    bd = rb.Boundary(*(torch.tensor(sc.bdy[k], device=dev) for k in ("x", "y", "z")), None,
-                     h=sc.h, rho0=sc.rho0, mass_iters=5)
-    grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h)
-    prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, 0.01)
-    prm.convergence = rb.CONV_AVERAGE
-    prm.eta = 0.001
-    prm.max_iter = 1000
-    sv = rb.Solver(rb.IISPH, prm, n)
-    g = (0.0, -9.81, 0.0)
-    lam = 0.4
+    run = EngineRun(rank, a.scale, dev)
+    n = run.n
     stream = torch.cuda.current_stream(dev)
     S = stream.cuda_stream
-    state = {"dt": 5e-4, "iters": 0, "errs": [], "iters_log": [], "limit": 0}
-
-    def step():
-        # main.cu:64-75 with lambda = 0.4: dt controller, grid, solver, bounds
-        state["dt"] = rb.dt_controller(st, state["iters"], state["dt"], lam, sc.h, g, 10,
-                                       0.001, stream=S)
-        grid.construct_and_reorder(st, stream=S)
-        try:
-            it = sv.step(st, grid, bd, state["dt"], stream=S)
-        except rb.ReynError as e:
-            if e.code != rb.ERR_ITER_LIMIT:
-                raise
-            it = sv.stats().iters
-            state["limit"] += 1
-        state["iters"] = it
-        s = sv.stats()
-        state["errs"].append(s.avg_density_error)
-        state["iters_log"].append(it)
-        rb.enforce_bounds(st, sc.box_min, sc.box_max, stream=S)
 
     for _ in range(a.warmup):
-        step()
+        run.step(S)
     torch.cuda.synchronize()
-    state["errs"].clear()
-    state["iters_log"].clear()
+    ck = run.checkpoint()  # the timed region starts here (replayed for e2e)
+    run.log.clear()
 
     gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
     clocks = ClockSampler(gpu_uuid)
@@ -233,118 +272,126 @@ def run_engine(a, world, rank, local):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(a.steps):
-        step()
+        run.step(S)
     e1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
     rb.profile_enable(False)
     prof = rb.profile_read()
-    ck = clocks.stop()
+    ck_clocks = clocks.stop()
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(world, ms)
     value = world * n * a.steps / (ms_max / 1e3)
-    iters_log = list(state["iters_log"])
-    errs = list(state["errs"])
-    dt_last = state["dt"]
+    log = list(run.log)
 
-    # dominant kernel and its roofline (live CUDA-event timing)
+    # dominant kernel and its roofline (CUDA events around its launches)
     launches = sum(v[0] for v in prof.values())
-    dom = max(prof.items(), key=lambda kv: kv[1][1])
-    dom_name, (dom_launches, dom_ms) = dom
+    dom_name, (dom_launches, dom_ms) = max(prof.items(), key=lambda kv: kv[1][1])
     per_launch_s = dom_ms / 1e3 / max(dom_launches, 1)
-    alg = ALG_BYTES.get(dom_name, 0) * n + (16 * sc.nb if dom_name == "k_density" else 0)
+    alg = ALG_BYTES.get(dom_name, 0) * n + (16 * run.sc.nb if dom_name == "k_density" else 0)
     peak, peak_kind = peaks()
     achieved = alg / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
-    traffic = profile_traffic(dom_name)
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": traffic, "peak_source": peak_kind,
+                "traffic": profile_traffic(dom_name), "peak_source": peak_kind,
                 "alg_bytes_per_launch": alg, "ms_per_launch": round(per_launch_s * 1e3, 4),
                 "share_of_step": round(dom_ms / ms, 4)}
     kernels = {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in
                sorted(prof.items(), key=lambda kv: -kv[1][1])}
 
-    # e2e: same steps through the C ABI with the state in pinned host memory
+    # e2e: the same K steps again from the checkpoint, through the C ABI
+    # with the state uploaded from / downloaded to pinned host memory
     e2e = None
     if not a.no_e2e:
+        run.restore(ck)
         host = {k: torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
                 for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
-        st_host = st.download()
         for k in host:
-            host[k][:] = st_host[k]
+            host[k][:] = ck[0][k]
         L = rb.lib()
         hp = [host[k].ctypes.data for k in ("x", "y", "z", "vx", "vy", "vz", "m")]
-
-        def e2e_step():
-            rb.check(L.reyn_particles_upload(st.h, *hp, S))
-            step()
-            rb.check(L.reyn_particles_download(st.h, *hp[:6], None, S))
-
+        run.log.clear()
         barrier(world)
         torch.cuda.synchronize()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         for _ in range(a.steps):
-            e2e_step()
+            rb.check(L.reyn_particles_upload(run.st.h, *hp, S))
+            run.step(S)
+            rb.check(L.reyn_particles_download(run.st.h, *hp[:6], None, S))
         t1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
         ems = max_over_ranks(world, t0.elapsed_time(t1))
-        e2e = {"value": world * n * a.steps / (ems / 1e3), "unit": UNIT,
+        e2e = {"value": round(world * n * a.steps / (ems / 1e3), 1), "unit": UNIT,
                "h2d_bytes_per_step": 28 * n, "d2h_bytes_per_step": 24 * n,
-               "ms_per_step": round(ems / a.steps, 3)}
+               "ms_per_step": round(ems / a.steps, 3),
+               "iters_per_step": [x[0] for x in run.log]}
 
-    # CPU baseline: the oracle on one step of the same state (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline_from(st, bd, sc, prm, dt_last)
+        cpu = cpu_baseline_from(ck, run)
 
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
         "data": "synthetic (seeded lattice + jitter dam break; Akinci box walls)",
-        "config": {"workload": WORKLOAD, "particles_per_gpu": n, "boundary_particles": sc.nb,
-                   "kernel": "C2", "h": sc.h, "rho0": sc.rho0, "nu": 0.01, "omega": 0.5,
+        "config": {"workload": WORKLOAD, "particles_per_gpu": n,
+                   "boundary_particles": run.sc.nb, "kernel": "C2", "h": run.sc.h,
+                   "rho0": run.sc.rho0, "nu": NU, "omega": 0.5,
                    "convergence": "avg density error <= 0.1% (FP64 reduction)",
-                   "dt": "simple_dt_controller(lambda=0.4, target 10 iters, 0.1%/step) "
-                         "from 5e-4",
+                   "dt": f"min(simple_dt_controller(lambda={LAMBDA}, target 10 iters, "
+                         f"0.1%/step) from {DT0}, 0.08 h^2/nu = {run.dt_visc:.2e})",
                    "precision": "fp32", "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (state 4M x 28 B + grid 70 MB per step)"},
-        "clocks": ck, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
+        "clocks": ck_clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
         "cpu_baseline": cpu,
-        "iters_per_step": iters_log, "avg_density_error_per_step": [round(e, 6) for e in errs],
-        "iter_limit_hits": state["limit"], "dt_last": dt_last, "kernels": kernels,
+        "iters_per_step": [x[0] for x in log],
+        "avg_density_error_per_step": [round(x[1], 7) for x in log],
+        "dt_per_step": [float(f"{x[2]:.4e}") for x in log],
+        "iter_limit_hits": run.limit_hits, "kernels": kernels,
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
-    for o in (sv, grid, bd, st):
-        o.close()
+    run.close()
 
 
-def cpu_baseline_from(st, bd, sc, prm, dt):
-    """One IISPH step of the oracle (C++/OpenMP, all host threads) from the
-    engine's current state: the same workload point the GPU was timed on."""
+def oracle_params(h: float, rho0: float):
     import oracle
-    import reyn_b200 as rb
-
-    fl = st.download()
-    fl["id"] = np.arange(sc.n, dtype=np.float32)
-    (px, py, pz, pm), nb = bd.arrays()
-    bdy = {"x": rb.device_to_numpy(px, nb), "y": rb.device_to_numpy(py, nb),
-           "z": rb.device_to_numpy(pz, nb), "m": rb.device_to_numpy(pm, nb)}
-    op = oracle.reference_params(2, 0, sc.h, sc.rho0, 0.01)
+    op = oracle.reference_params(2, 0, h, rho0, NU)
     op.iisph_avg = 1
     op.eta = 0.001
     op.max_iter = 1000
+    return op
+
+
+def cpu_baseline_from(ck, run):
+    """One IISPH step of the oracle (C++/OpenMP, all host threads) from the
+    checkpoint the GPU's timed region started from."""
+    import oracle
+    import reyn_b200 as rb
+
+    state, p, dt_prev, iters = ck
+    sc = run.sc
+    fl = {k: v.copy() for k, v in state.items()}
+    fl["id"] = np.arange(sc.n, dtype=np.float32)
+    (px, py, pz, pm), nb = run.bd.arrays()
+    bdy = {"x": rb.device_to_numpy(px, nb), "y": rb.device_to_numpy(py, nb),
+           "z": rb.device_to_numpy(pz, nb), "m": rb.device_to_numpy(pm, nb)}
+    g = oracle.f32([0.0, -9.81, 0.0])
     t0 = time.perf_counter()
-    r = oracle.run(op, fl, bdy, sc.box_min, sc.box_max, dt, 1)
+    dt = min(float(oracle.lib().orc_dt_controller(iters, dt_prev, LAMBDA, sc.h, sc.n,
+                                                  fl["vx"], fl["vy"], fl["vz"], g, 10, 0.001)),
+             viscous_dt_limit(sc.h, NU))
+    r = oracle.run(oracle_params(sc.h, sc.rho0), fl, bdy, sc.box_min, sc.box_max, dt, 1, p0=p)
     secs = time.perf_counter() - t0
     return {"value": round(sc.n / secs, 1), "unit": UNIT, "cores": oracle.threads(),
             "kind": "port",
-            "sample": f"1 IISPH step of the same 4M state (grid build, reorder, "
-                      f"{int(r.iters[0])} Jacobi sweeps) on the C++/OpenMP oracle, {secs:.1f} s"}
+            "sample": f"1 step of the same workload from the state the GPU timing started "
+                      f"from ({sc.n} particles, {int(r.iters[0])} Jacobi sweeps) on the "
+                      f"C++/OpenMP oracle: {secs:.2f} s"}
 
 
 # ---- reference arm -------------------------------------------------------------
@@ -352,41 +399,39 @@ def cpu_baseline_from(st, bd, sc, prm, dt):
 def run_reference(a, world, rank):
     """The reference's path timed on the host cores. The reference has no CPU
     implementation of its step; its algorithm as restated in the C++/OpenMP
-    oracle (every host thread) is timed on the same workload and config."""
+    oracle (every host thread) runs the same scene, parameters and dt rule
+    as the engine arm: W warm-up steps, then K timed steps."""
     if rank != 0:
         return
     import oracle
-    from reyn_b200 import scenes  # noqa: F401
 
     sc = scene_for(0, a.scale)
     t0 = time.perf_counter()
     bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
     setup = time.perf_counter() - t0
     bdy = dict(sc.bdy, m=bm)
-    op = oracle.reference_params(2, 0, sc.h, sc.rho0, 0.01)
-    op.iisph_avg = 1
-    op.eta = 0.001
-    op.max_iter = 1000
+    op = oracle_params(sc.h, sc.rho0)
     fl = {k: v.copy() for k, v in sc.fluid.items()}
     p = np.zeros(sc.n, np.float32)
-    dt = 5e-4
-    iters = 0
-    g = [0.0, -9.81, 0.0]
+    dt, iters = DT0, 0
+    g = oracle.f32([0.0, -9.81, 0.0])
+    dt_visc = viscous_dt_limit(sc.h, NU)
+    log = []
 
     def one():
-        nonlocal dt, iters, p
-        dt = float(oracle.lib().orc_dt_controller(iters, dt, 0.4, sc.h, sc.n,
-                                                  oracle.f32(fl["vx"]), oracle.f32(fl["vy"]),
-                                                  oracle.f32(fl["vz"]), oracle.f32(g), 10,
-                                                  0.001))
+        nonlocal dt, iters, p, fl
+        dt = min(float(oracle.lib().orc_dt_controller(iters, dt, LAMBDA, sc.h, sc.n, fl["vx"],
+                                                      fl["vy"], fl["vz"], g, 10, 0.001)),
+                 dt_visc)
         r = oracle.run(op, fl, bdy, sc.box_min, sc.box_max, dt, 1, p0=p)
-        for k in fl:
-            fl[k] = r.state[k]
+        fl = dict(r.state)
         p = r.p
         iters = int(r.iters[0])
+        log.append(iters)
 
     for _ in range(a.warmup):
         one()
+    log.clear()
     t0 = time.perf_counter()
     for _ in range(a.steps):
         one()
@@ -397,11 +442,13 @@ def run_reference(a, world, rank):
            "ms_per_step": round(secs / a.steps * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
            "config": {"workload": WORKLOAD, "particles_per_gpu": sc.n,
-                      "parallelism": "host threads", "setup_s": round(setup, 1)},
+                      "parallelism": "host threads", "setup_s": round(setup, 1),
+                      "iters_per_step": log},
            "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": oracle.threads(),
                             "kind": "port",
                             "sample": f"{a.steps} timed steps of the full workload after "
-                                      f"{a.warmup} warm-up steps, C++/OpenMP restatement"},
+                                      f"{a.warmup} warm-up steps, C++/OpenMP restatement "
+                                      f"of the reference's algorithm"},
            "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

@@ -218,6 +218,16 @@ typedef struct reyn_solver_buffers {
 } reyn_solver_buffers;
 int reyn_solver_buffers_get(const reyn_solver* s, reyn_solver_buffers* out);
 
+/* the pressure IISPH carries across steps (its warm start, IISPH.cuh:48),
+ * copied to / from host memory: n floats in the particle order of `state`
+ * at the time of the call. With the particle arrays (download/upload) this
+ * is a complete checkpoint of a simulation. Upload binds the pressure to
+ * the current order of `state`. Both synchronise the stream. */
+int reyn_solver_pressure_download(const reyn_solver* s, float* host_p,
+    void* stream);
+int reyn_solver_pressure_upload(reyn_solver* s, const reyn_particles* state,
+    const float* host_p, void* stream);
+
 /* statistics of the last step: iterations and the last sweep's average
  * (max(0, .)) and maximum predicted density error, in units of rho0 */
 typedef struct reyn_step_stats {

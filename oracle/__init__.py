@@ -81,6 +81,7 @@ class Params(ctypes.Structure):
         ("warmstart", ctypes.c_int),
         ("iisph_avg", ctypes.c_int),
         ("cell_ratio", ctypes.c_float),
+        ("projected", ctypes.c_int),
     ]
 
 
@@ -101,6 +102,9 @@ def lib():
                                       ctypes.c_void_p]
         L.orc_boundary_masses.argtypes = [ctypes.c_uint32, _f32p, _f32p, _f32p, ctypes.c_float,
                                           ctypes.c_float, ctypes.c_uint32, _f32p]
+        L.orc_boundary_masses_kernel.argtypes = [ctypes.c_uint32, _f32p, _f32p, _f32p,
+                                                 ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
+                                                 ctypes.c_int, _f32p]
         L.orc_cfl.argtypes = [ctypes.c_uint32, _f32p, _f32p, _f32p, ctypes.c_float, ctypes.c_float,
                               _f32p]
         L.orc_cfl.restype = ctypes.c_float
@@ -179,10 +183,10 @@ def brute_count(x, y, z, r: float):
     return count, len2
 
 
-def boundary_masses(bx, by, bz, h: float, rho0: float, iters: int = 5):
+def boundary_masses(bx, by, bz, h: float, rho0: float, iters: int = 5, kind: int = B3):
     bx, by, bz = f32(bx), f32(by), f32(bz)
     m = np.zeros(bx.size, np.float32)
-    rc = lib().orc_boundary_masses(bx.size, bx, by, bz, h, rho0, iters, m)
+    rc = lib().orc_boundary_masses_kernel(bx.size, bx, by, bz, h, rho0, iters, kind, m)
     if rc:
         raise ValueError(rc)
     return m

@@ -578,7 +578,7 @@ template <class K>
 uint64_t iisph_jacobi(const K& Wk, const State& s, const Grid& G,
     const Bdy& b, const float* ax, const float* ay, const float* az,
     float* p, const float* aii, const float* sii, float dt, float omega,
-    float thr, double* err_sum)
+    float thr, double* err_sum, int projected)
 {
     uint64_t over = 0;
     double es = 0.;
@@ -598,7 +598,14 @@ uint64_t iisph_jacobi(const K& Wk, const State& s, const Grid& G,
             mk(0, 0, 0));
         const float Ap = dt * (ff + dot(ai, gb));
         const float si = sii[i];
-        p[i] = p[i] + jacobi(omega, aii[i], Ap, si);
+        if (projected) {
+            const float a = aii[i];
+            p[i] = ((double)a < 1e-6 && (double)a > -1e-6)
+                ? p[i]
+                : std::fmax(0.f, p[i] + omega * (si - Ap) / a);
+        } else {
+            p[i] = p[i] + jacobi(omega, aii[i], Ap, si);
+        }
         const float err = (Ap - si) * dt;
         over += (err > thr) ? 1 : 0;
         es += std::max(0.0, (double)err);
@@ -751,32 +758,42 @@ int orc_brute_count(uint32_t n, const float* x, const float* y,
     return 0;
 }
 
-int orc_boundary_masses(uint32_t nb, const float* bx, const float* by,
-    const float* bz, float h, float rho0, uint32_t iters, float* m)
+int orc_boundary_masses_kernel(uint32_t nb, const float* bx, const float* by,
+    const float* bz, float h, float rho0, uint32_t iters, int kind, float* m)
 {
     if (iters == 0) // sample_boundary.cu:283-287
         return -1;
     Bdy b;
     if (int e = make_bdy(nb, bx, by, bz, nullptr, h, 0.5f, b))
         return e;
-    const B3 Wk(2.f * h);
     std::vector<float> next(nb);
-    for (uint32_t it = 0; it < iters; ++it) {
+    const int st = with_kernel(kind, 2.f * h, [&](auto Wk) {
+        for (uint32_t it = 0; it < iters; ++it) {
 #pragma omp parallel for schedule(static)
-        for (int64_t i = 0; i < (int64_t)nb; ++i) {
-            const f3 xi = mk(b.x[i], b.y[i], b.z[i]);
-            const float sum = ff_nbrs(b.grid, xi, b.x.data(), b.y.data(),
-                b.z.data(),
-                [&](uint32_t j, f3 xij, float) { return b.m[j] * W(Wk, xij); },
-                0.f);
-            next[i] = rho0 * b.m[i] / sum;
+            for (int64_t i = 0; i < (int64_t)nb; ++i) {
+                const f3 xi = mk(b.x[i], b.y[i], b.z[i]);
+                const float sum = ff_nbrs(b.grid, xi, b.x.data(), b.y.data(),
+                    b.z.data(),
+                    [&](uint32_t j, f3 xij, float) { return b.m[j] * W(Wk, xij); },
+                    0.f);
+                next[i] = rho0 * b.m[i] / sum;
+            }
+            b.m.swap(next);
         }
-        b.m.swap(next);
-    }
+    });
+    if (st)
+        return st;
     // scatter back to the caller's order
     for (uint32_t i = 0; i < nb; ++i)
         m[b.grid.sorted[i]] = b.m[i];
     return 0;
+}
+
+int orc_boundary_masses(uint32_t nb, const float* bx, const float* by,
+    const float* bz, float h, float rho0, uint32_t iters, float* m)
+{
+    // calculate_boundary_masses always refines with B3 (sample_boundary.cu:269)
+    return orc_boundary_masses_kernel(nb, bx, by, bz, h, rho0, iters, 1, m);
 }
 
 float orc_cfl(uint32_t n, const float* vx, const float* vy, const float* vz,
@@ -823,6 +840,7 @@ void orc_params_reference(int scheme, int kind, float h, float rho0,
     p->warmstart = 1; // IISPH.cuh:48
     p->iisph_avg = 0;
     p->cell_ratio = 0.5f;
+    p->projected = 0;
 }
 
 int orc_run(const orc_params* prm, uint32_t n, float* x, float* y, float* z,
@@ -911,7 +929,7 @@ int orc_run(const orc_params* prm, uint32_t n, float* x, float* y, float* z,
                     double es = 0.;
                     const uint64_t over = iisph_jacobi(Wk, s, G, b, ax.data(),
                         ay.data(), az.data(), pbuf.data(), aii.data(),
-                        sii.data(), dt, prm->omega, prm->eta * rho0, &es);
+                        sii.data(), dt, prm->omega, prm->eta * rho0, &es, prm->projected);
                     l += 1;
                     more = prm->iisph_avg
                         ? (es / (double)n > (double)prm->eta * rho0)

@@ -67,6 +67,10 @@ int orc_brute_count(uint32_t n, const float* x, const float* y,
 int orc_boundary_masses(uint32_t nb, const float* bx, const float* by,
     const float* bz, float h, float rho0, uint32_t iters, float* m);
 
+/* the same refinement with smoothing kernel `kind` instead of B3 */
+int orc_boundary_masses_kernel(uint32_t nb, const float* bx, const float* by,
+    const float* bz, float h, float rho0, uint32_t iters, int kind, float* m);
+
 /* cfl_time_step (cfl.cu:5-37) */
 float orc_cfl(uint32_t n, const float* vx, const float* vy, const float* vz,
     float lambda, float h, const float g[3]);
@@ -92,6 +96,8 @@ typedef struct orc_params {
     int iisph_avg;      /* IISPH: stop on average error <= eta instead of
                            "no particle above eta" (reference) */
     float cell_ratio;   /* 0.5 = reference */
+    int projected;      /* IISPH: p = max(0, p + delta) instead of the
+                           reference's p += max(0, delta) */
 } orc_params;
 
 void orc_params_reference(int scheme, int kind, float h, float rho0,

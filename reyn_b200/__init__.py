@@ -102,6 +102,8 @@ _SIGNATURES = {
     "reyn_cfl_time_step": [_vp, _f, _f, _f * 3, ctypes.POINTER(_f), _vp],
     "reyn_dt_controller": [_vp, _u32, _f, _f, _f, _f * 3, _u32, _f, ctypes.POINTER(_f), _vp],
     "reyn_enforce_bounds": [_vp, _f * 3, _f * 3, _vp],
+    "reyn_solver_pressure_download": [_vp, _vp, _vp],
+    "reyn_solver_pressure_upload": [_vp, _vp, _vp, _vp],
     "reyn_profile_enable": [ctypes.c_int],
     "reyn_profile_reset": [],
     "reyn_profile_read": [ctypes.POINTER(ProfileEntry), _u32, ctypes.POINTER(_u32)],
@@ -318,6 +320,16 @@ class Solver:
         b = SolverBuffers()
         check(lib().reyn_solver_buffers_get(self.h, ctypes.byref(b)))
         return b
+
+    def pressure(self, stream=None) -> np.ndarray:
+        """The carried IISPH pressure, in the particle order of the state."""
+        p = np.empty(self.n, np.float32)
+        check(lib().reyn_solver_pressure_download(self.h, p.ctypes.data, _stream(stream)))
+        return p
+
+    def set_pressure(self, state: "Particles", p: np.ndarray, stream=None) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        check(lib().reyn_solver_pressure_upload(self.h, state.h, p.ctypes.data, _stream(stream)))
 
     def stats(self) -> StepStats:
         s = StepStats()

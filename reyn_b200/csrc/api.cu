@@ -365,6 +365,37 @@ int reyn_solver_buffers_get(const reyn_solver* s, reyn_solver_buffers* out)
     });
 }
 
+int reyn_solver_pressure_download(const reyn_solver* s, float* host_p, void* stream)
+{
+    return guard([&] {
+        require(s && host_p, "null argument");
+        const cudaStream_t st = as_stream(stream);
+        if (s->n && s->p.size() == s->n)
+            REYN_CUDA(cudaMemcpyAsync(host_p, s->p.get(), size_t(s->n) * sizeof(float),
+                cudaMemcpyDeviceToHost, st));
+        else
+            std::memset(host_p, 0, size_t(s->n) * sizeof(float));
+        REYN_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int reyn_solver_pressure_upload(reyn_solver* s, const reyn_particles* state,
+    const float* host_p, void* stream)
+{
+    return guard([&] {
+        require(s && state && host_p, "null argument");
+        require(state->n == s->n, "particle count differs from the solver's");
+        const cudaStream_t st = as_stream(stream);
+        s->p.resize(s->n);
+        if (s->n)
+            REYN_CUDA(cudaMemcpyAsync(s->p.get(), host_p, size_t(s->n) * sizeof(float),
+                cudaMemcpyHostToDevice, st));
+        REYN_CUDA(cudaStreamSynchronize(st));
+        s->p_state = state;
+        s->p_epoch = state->epoch;
+    });
+}
+
 int reyn_solver_stats(const reyn_solver* s, reyn_step_stats* out)
 {
     return guard([&] {

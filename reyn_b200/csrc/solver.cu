@@ -23,11 +23,30 @@ namespace reyn {
 
 namespace {
 
+// Per-step neighbour list: the fluid neighbours (self excluded) of every
+// particle, in traversal order, written by the density pass and read by every
+// later pass of the step (positions are fixed until the final integration).
+// Slot k of particle i lives at list_slot(i, k): blocks of 128 particles
+// store their slot rows contiguously, so that a warp reads one 128-byte row
+// per slot. A particle with more than KMAX neighbours keeps its count
+// (> KMAX) and is served by the cell traversal instead.
+constexpr int KMAX = 64;
+static_assert(NBR_THREADS == 128, "list rows are laid out for 128-thread blocks");
+
+__host__ __device__ __forceinline__ size_t list_slot(uint32_t i, uint32_t k)
+{
+    return size_t(i >> 7) * (KMAX * 128) + size_t(k) * 128 + (i & 127u);
+}
+
+inline size_t list_capacity(uint32_t n) { return size_t((n + 127) / 128) * KMAX * 128; }
+
 struct Fluid {
     GridView g;
     KernelConst kc;
     const float4* __restrict__ pm; // (x, y, z, m), grid order
     uint32_t* status;
+    uint32_t* __restrict__ nbr;    // neighbour list (list_slot layout)
+    uint32_t* __restrict__ ncount; // neighbours per particle
 };
 
 struct Bdy {
@@ -47,6 +66,31 @@ __device__ __forceinline__ int3 fluid_cell(const Fluid& f, const float4& me)
         c = clamp_cell(f.g, c, R);
     }
     return c;
+}
+
+// the fluid neighbours j != i of particle i from the step's list (or, for a
+// particle whose list overflowed, from the cell traversal); f(j, pm[j], dx,
+// dy, dz, l2) in the traversal order of the cells
+template <int R, class F>
+__device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3 c,
+    const float4& me, F&& fn)
+{
+    const uint32_t cnt = __ldg(f.ncount + i);
+    if (cnt <= KMAX) {
+        const uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t j = __ldg(row + size_t(k) * 128);
+            const float4 q = __ldg(f.pm + j);
+            const float dx = me.x - q.x, dy = me.y - q.y, dz = me.z - q.z;
+            fn(j, q, dx, dy, dz, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+        }
+    } else {
+        for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+            [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+                if (j != i)
+                    fn(j, q, dx, dy, dz, l2);
+            });
+    }
 }
 
 // boundary neighbours of a point; a point whose cell is outside the
@@ -115,36 +159,59 @@ __device__ __forceinline__ void block_accumulate(SweepStats* st, unsigned over, 
 
 // ---- passes ----------------------------------------------------------------
 
-// compute_densities (solver.cuh:18-38) + cached boundary sums
+// compute_densities (solver.cuh:18-38) + cached boundary sums + the step's
+// neighbour list (staged per block in shared memory, written row by row)
 template <int KIND, int R>
 __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bdy b,
     float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm)
 {
+    __shared__ uint32_t s_list[KMAX][NBR_THREADS];
+    __shared__ uint32_t s_rows[NBR_THREADS / 32];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    const float4 me = f.pm[i];
-    const int3 c = fluid_cell<R>(f, me);
-    float rf = 0.f;
-    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
-        [&](uint32_t, const float4& q, float, float, float, float l2) {
-            rf += q.w * pair_w<KIND>(f.kc, l2);
-        });
-    float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-    for_each_boundary(b, me.x, me.y, me.z,
-        [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
-            float w, g;
-            pair_wg<KIND>(f.kc, l2, w, g);
-            rb += q.w * w;
-            const float mg = q.w * g;
-            gx += mg * dx;
-            gy += mg * dy;
-            gz += mg * dz;
-        });
-    const float r = rf + rb;
-    rho[i] = r;
-    vel[i].w = r;
-    bterm[i] = make_float4(gx, gy, gz, rb);
+    const bool valid = i < n;
+    uint32_t cnt = 0;
+    if (valid) {
+        const float4 me = f.pm[i];
+        const int3 c = fluid_cell<R>(f, me);
+        float rf = 0.f;
+        for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+            [&](uint32_t j, const float4& q, float, float, float, float l2) {
+                rf += q.w * pair_w<KIND>(f.kc, l2);
+                if (j != i) {
+                    if (cnt < KMAX)
+                        s_list[cnt][threadIdx.x] = j;
+                    ++cnt;
+                }
+            });
+        float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+        for_each_boundary(b, me.x, me.y, me.z,
+            [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
+                float w, g;
+                pair_wg<KIND>(f.kc, l2, w, g);
+                rb += q.w * w;
+                const float mg = q.w * g;
+                gx += mg * dx;
+                gy += mg * dy;
+                gz += mg * dz;
+            });
+        const float r = rf + rb;
+        rho[i] = r;
+        vel[i].w = r;
+        bterm[i] = make_float4(gx, gy, gz, rb);
+        f.ncount[i] = cnt;
+    }
+    // rows of the block's list: as many as its longest (stored) list
+    uint32_t rows = min(cnt, (uint32_t)KMAX);
+    rows = __reduce_max_sync(0xffffffffu, rows);
+    if ((threadIdx.x & 31) == 0)
+        s_rows[threadIdx.x >> 5] = rows;
+    __syncthreads();
+#pragma unroll
+    for (int w = 0; w < NBR_THREADS / 32; ++w)
+        rows = max(rows, s_rows[w]);
+    uint32_t* __restrict__ out = f.nbr + size_t(blockIdx.x) * (KMAX * 128) + threadIdx.x;
+    for (uint32_t k = 0; k < rows; ++k)
+        out[size_t(k) * 128] = s_list[k][threadIdx.x];
 }
 
 // write_non_prs_acc_ff (solver.cuh:40-69): gravity + artificial viscosity;
@@ -161,7 +228,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_nonpressure(uint32_t n, Fluid f
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
     float ax = grav.x, ay = grav.y, az = grav.z;
-    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+    for_each_listed<R>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float4 vj = __ldg(vel + j);
             const float vdx = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
@@ -198,7 +265,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_sesph(uint32_t n, Fluid f,
     const float pi = eos_sesph(vi.w, k, rho0);
     const float pri = pi / (vi.w * vi.w);
     float ax = grav.x, ay = grav.y, az = grav.z;
-    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+    for_each_listed<R>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float4 vj = __ldg(vel + j);
             const float pj = eos_sesph(vj.w, k, rho0);
@@ -237,8 +304,9 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_predict(uint32_t n, Flui
         const float4 me = f.pm[i];
         const float4 vi = vel[i];
         const int3 c = fluid_cell<R>(f, me);
-        float r = 0.f;
-        for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        // the list excludes the particle itself: its term is m_i W(0)
+        float r = me.w * pair_w<KIND>(f.kc, 0.f);
+        for_each_listed<R>(f, i, c, me,
             [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
                 const float4 vj = __ldg(vel + j);
                 float w, g;
@@ -269,7 +337,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_pressure(uint32_t n, Flu
     const float pi = fmaxf(0.f, k * (ri - rho0));
     const float pri = pi / (ri * ri);
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+    for_each_listed<R>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float rj = __ldg(rho + j);
             const float pj = fmaxf(0.f, k * (rj - rho0));
@@ -326,7 +394,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
     float gx = 0.f, gy = 0.f, gz = 0.f, vdiv = 0.f, gsq = 0.f;
-    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+    for_each_listed<R>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float4 vj = __ldg(vel + j);
             const float g = pair_g<KIND>(f.kc, l2);
@@ -362,7 +430,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
     const int3 c = fluid_cell<R>(f, me);
     const float pi = p[i];
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+    for_each_listed<R>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float s = q.w * (pi + __ldg(p + j)) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
@@ -392,7 +460,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
         const int3 c = fluid_cell<R>(f, me);
         const float4 ai = acc[i];
         float sum = 0.f;
-        for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        for_each_listed<R>(f, i, c, me,
             [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
                 const float4 aj = __ldg(acc + j);
                 const float d = fmaf(ai.x - aj.x, dx, fmaf(ai.y - aj.y, dy, (ai.z - aj.z) * dz));
@@ -425,7 +493,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f
     const int3 c = fluid_cell<R>(f, me);
     const float pi = p[i];
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+    for_each_listed<R>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float s = q.w * (pi + __ldg(p + j)) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
@@ -534,6 +602,8 @@ static void ensure_buffers(reyn_solver& sv, uint32_t n)
     sv.acc.resize(n);
     sv.vel2.resize(n);
     sv.bterm.resize(n);
+    sv.nbr.resize(list_capacity(n));
+    sv.ncount.resize(n);
     if (sv.p.size() != n) {
         sv.p.resize(n);
         REYN_CUDA(cudaMemset(sv.p.get(), 0, size_t(n) * sizeof(float)));
@@ -582,6 +652,8 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     f.kc = make_kernel(P.kernel, 2.f * P.h);
     f.pm = st.pm.get();
     f.status = const_cast<uint32_t*>(grid.status.get());
+    f.nbr = sv.nbr.get();
+    f.ncount = sv.ncount.get();
     Bdy b {};
     if (bdy && bdy->nb) {
         b.g = bdy->view();
