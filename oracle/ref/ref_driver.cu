@@ -103,6 +103,22 @@ __global__ void _drv_density(const uint N, const float* __restrict__ xx,
         });
 }
 
+// the reference grid benchmark's query kernel (uniformgrid.cu:231-245)
+template <IsKernel K, Resort R>
+__global__ void _drv_query(const uint N, const float* __restrict__ xx,
+    const float* __restrict__ xy, const float* __restrict__ xz,
+    float* __restrict__ res_out, const UniformGrid<R> grid, const K W)
+{
+    auto i { blockIdx.x * blockDim.x + threadIdx.x };
+    if (i >= N)
+        return;
+    const float3 x_i { v3(i, xx, xy, xz) };
+    res_out[i] = grid.ff_nbrs(
+        x_i, xx, xy, xz, [=] __device__(auto j, auto x_ij, auto x_ij_l2) {
+            return xx[i] * xx[j] * W(x_ij);
+        });
+}
+
 template <IsKernel K>
 __global__ void _drv_kernel_eval(const uint N, const float* __restrict__ dx,
     const float* __restrict__ dy, const float* __restrict__ dz,
@@ -387,6 +403,117 @@ int ref_run(int scheme, int kind, uint N, float* x, float* y, float* z,
             to_host(b_ay, ay, N);
             to_host(b_az, az, N);
         }
+    });
+}
+
+/// Timing of the reference's own grid benchmark (uniformgrid.cu:385-423) on
+/// the given points: `reps` x construct_and_reorder of x, y, z plus 4 extra
+/// arrays, and `reps` x the query kernel Σ x_i x_j W_B3(x_ij) at support r.
+/// Device time by CUDA events; ms_out[0] = construction, ms_out[1] = query
+/// (averages per repetition).
+int ref_grid_bench(uint N, const float* x, const float* y, const float* z,
+    const float* bmin, const float* bmax, float r, uint reps, float* ms_out)
+{
+    return guarded([&] {
+        DeviceBuffer<float> xx(1), xy(1), xz(1), tmp(1), e1(1), out(N, 0.f);
+        to_dev(xx, x, N);
+        to_dev(xy, y, N);
+        to_dev(xz, z, N);
+        e1.resize(N);
+        tmp.resize(N);
+        UniformGridBuilder builder(v3(bmin[0], bmin[1], bmin[2]), v3(bmax[0], bmax[1], bmax[2]), r);
+        cudaEvent_t a, b;
+        CUDA_CHECK(cudaEventCreate(&a));
+        CUDA_CHECK(cudaEventCreate(&b));
+        for (uint k = 0; k < 2; ++k) // warm-up
+            builder.construct_and_reorder(r, tmp, xx, xy, xz, &e1, &e1, &e1, &e1);
+        CUDA_CHECK(cudaEventRecord(a));
+        for (uint k = 0; k < reps; ++k)
+            builder.construct_and_reorder(r, tmp, xx, xy, xz, &e1, &e1, &e1, &e1);
+        CUDA_CHECK(cudaEventRecord(b));
+        CUDA_CHECK(cudaEventSynchronize(b));
+        float t = 0.f;
+        CUDA_CHECK(cudaEventElapsedTime(&t, a, b));
+        ms_out[0] = t / reps;
+        const UniformGrid<Resort::yes> grid { builder.construct_and_reorder(
+            r, tmp, xx, xy, xz) };
+        const B3 W(r);
+        _drv_query<<<BLOCKS(N), BLOCK_SIZE>>>(N, xx.ptr(), xy.ptr(), xz.ptr(), out.ptr(), grid, W);
+        CUDA_CHECK(cudaEventRecord(a));
+        for (uint k = 0; k < reps; ++k)
+            _drv_query<<<BLOCKS(N), BLOCK_SIZE>>>(N, xx.ptr(), xy.ptr(), xz.ptr(), out.ptr(),
+                grid, W);
+        CUDA_CHECK(cudaEventRecord(b));
+        CUDA_CHECK(cudaEventSynchronize(b));
+        CUDA_CHECK(cudaEventElapsedTime(&t, a, b));
+        ms_out[1] = t / reps;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    });
+}
+
+/// ref_run with device timing of the step loop: ms_out = average device time
+/// per main-loop step (grid build + reorder, solver step, bounds), CUDA events
+/// around the loop (the reference's host syncs inside the solvers included).
+int ref_run_timed(int scheme, int kind, uint N, float* x, float* y, float* z,
+    float* vx, float* vy, float* vz, float* m, float* id, uint Nb,
+    const float* bx, const float* by, const float* bz, const float* bm,
+    const float* scene_min, const float* scene_max, float h, float rho0,
+    float nu, float dt, uint steps, uint* iters, float* ms_out)
+{
+    return guarded([&] {
+        DeviceBuffer<float> tmp(1);
+        BoundarySamples bdy { make_boundary(
+            Nb, bx, by, bz, bm, h, rho0, 1, tmp) };
+        Particles state(N, rho0);
+        to_dev(state.xx, x, N);
+        to_dev(state.xy, y, N);
+        to_dev(state.xz, z, N);
+        to_dev(state.vx, vx, N);
+        to_dev(state.vy, vy, N);
+        to_dev(state.vz, vz, N);
+        to_dev(state.m, m, N);
+        DeviceBuffer<float> tmp1(1), b_rho(1), b_p(1), b_aii(1), b_sii(1), b_ax(1), b_ay(1),
+            b_az(1);
+        DeviceBuffer<uint32_t> b_bits(1);
+        const float3 smin { v3(scene_min[0], scene_min[1], scene_min[2]) };
+        const float3 smax { v3(scene_max[0], scene_max[1], scene_max[2]) };
+        UniformGridBuilder builder(smin, smax, 2.f * h);
+        cudaEvent_t a, b;
+        CUDA_CHECK(cudaEventCreate(&a));
+        CUDA_CHECK(cudaEventCreate(&b));
+        with_kernel(kind, 2.f * h, [&](auto W) {
+            using K = decltype(W);
+            auto bounds = [&] {
+                _hard_enforce_bounds<<<BLOCKS(N), BLOCK_SIZE>>>(smin, smax, N,
+                    state.xx.ptr(), state.xy.ptr(), state.xz.ptr(),
+                    state.vx.ptr(), state.vy.ptr(), state.vz.ptr());
+                CUDA_CHECK(cudaGetLastError());
+            };
+            if (scheme != 2)
+                throw std::runtime_error("ref_run_timed times IISPH only");
+            IISPH<K, Resort::yes> solver(W, N, nu, h, rho0, b_rho, b_aii, b_sii, b_ax, b_ay,
+                b_az, b_p, b_bits);
+            CUDA_CHECK(cudaEventRecord(a));
+            for (uint s { 0 }; s < steps; ++s) {
+                const auto grid { builder.construct_and_reorder(2.f * h, tmp1, state, &b_p) };
+                iters[s] = solver.step(state, grid, bdy, dt);
+                bounds();
+            }
+            CUDA_CHECK(cudaEventRecord(b));
+            CUDA_CHECK(cudaEventSynchronize(b));
+            float t = 0.f;
+            CUDA_CHECK(cudaEventElapsedTime(&t, a, b));
+            *ms_out = t / (float)steps;
+        });
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        to_host(state.xx, x, N);
+        to_host(state.xy, y, N);
+        to_host(state.xz, z, N);
+        to_host(state.vx, vx, N);
+        to_host(state.vy, vy, N);
+        to_host(state.vz, vz, N);
     });
 }
 

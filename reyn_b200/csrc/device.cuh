@@ -155,6 +155,7 @@ __device__ __forceinline__ void pair_wg(
 struct GridView {
     float lox, loy, loz;
     float cell;
+    float inv_cell; // 1 / cell, for the strip trimming only (never for keys)
     float r2;
     int nx, ny, nz, nxny;
     const uint32_t* __restrict__ prefix;
@@ -185,20 +186,48 @@ __device__ __forceinline__ int3 clamp_cell(const GridView& g, int3 c, int R)
 // 2R+1 x-cells in the sorted arrays bounded by two prefix entries. `pts` are
 // packed (x, y, z, mass) in grid order; f(j, pts[j], dx, dy, dz, l2) is
 // called for every candidate with l2 <= r^2 (self included, as the
-// reference's accumulation does).
+// reference's accumulation does), in the reference's row order.
+//
+// Each row is trimmed to the part the search sphere can reach: rows whose
+// (y, z) distance from the point exceeds r are skipped, and the x-run is cut
+// to the cells overlapping the sphere's chord at that distance. The trimming
+// is conservative by a margin of 1e-3 cells, so exactly the candidates within
+// r are still visited, in the same order; only provably empty cells are
+// skipped.
 template <int R, class F>
 __device__ __forceinline__ void for_each_neighbour(const GridView& g, int3 c,
     float xi, float yi, float zi, const float4* __restrict__ pts, F&& f)
 {
-    constexpr int ROW = 2 * R + 1;
-    int plane = (c.z - R) * g.nxny + (c.y - R) * g.nx + (c.x - R);
+    constexpr float EPS = 1e-3f;
+    // the point in cell units, relative to its own cell's lower corner
+    const float fx = (xi - g.lox) * g.inv_cell - (float)c.x;
+    const float fy = (yi - g.loy) * g.inv_cell - (float)c.y;
+    const float fz = (zi - g.loz) * g.inv_cell - (float)c.z;
+    const float rr = g.r2 * g.inv_cell * g.inv_cell * (1.f + EPS) + EPS;
 #pragma unroll 1
-    for (int dz = 0; dz < ROW; ++dz, plane += g.nxny) {
-        int cid = plane;
+    for (int dz = -R; dz <= R; ++dz) {
+        // distance (cells) from the point to the slab of cells at c.z + dz
+        const float gz = dz > 0 ? fmaxf((float)dz - fz, 0.f)
+                                : (dz < 0 ? fmaxf(fz - (float)(dz + 1), 0.f) : 0.f);
+        const float gz2 = gz * gz;
+        if (gz2 > rr)
+            continue;
+        const int plane = (c.z + dz) * g.nxny;
 #pragma unroll 1
-        for (int dy = 0; dy < ROW; ++dy, cid += g.nx) {
+        for (int dy = -R; dy <= R; ++dy) {
+            const float gy = dy > 0 ? fmaxf((float)dy - fy, 0.f)
+                                    : (dy < 0 ? fmaxf(fy - (float)(dy + 1), 0.f) : 0.f);
+            const float d2 = gz2 + gy * gy;
+            if (d2 > rr)
+                continue;
+            const float w = sqrtf(rr - d2) + EPS; // half chord, cells
+            const int x0 = max(-R, (int)floorf(fx - w));
+            const int x1 = min(R, (int)floorf(fx + w));
+            if (x0 > x1) // only for points clamped into the grid from outside
+                continue;
+            const int cid = plane + (c.y + dy) * g.nx + c.x + x0;
             const uint32_t s = __ldg(g.prefix + cid);
-            const uint32_t e = __ldg(g.prefix + cid + ROW);
+            const uint32_t e = __ldg(g.prefix + cid + (x1 - x0 + 1));
             for (uint32_t j = s; j < e; ++j) {
                 const float4 q = __ldg(pts + j);
                 const float dx = xi - q.x, dy_ = yi - q.y, dz_ = zi - q.z;

@@ -83,6 +83,9 @@ struct reyn_boundary {
     reyn::Grid grid;
     reyn::DevArray<float> x, y, z, m;
     reyn::DevArray<float4> pm;
+    // per boundary-grid cell: 1 if a sample lies within its (2R+1)^3 block
+    // of cells, so that fluid particles elsewhere skip the boundary walk
+    reyn::DevArray<uint8_t> near;
     reyn::GridView view() const;
 };
 

@@ -47,6 +47,7 @@ GridView Grid::view(float search_radius) const
     v.loy = geom.lo[1];
     v.loz = geom.lo[2];
     v.cell = geom.cell;
+    v.inv_cell = 1.f / geom.cell;
     v.r2 = search_radius * search_radius;
     v.nx = geom.n[0];
     v.ny = geom.n[1];
@@ -603,6 +604,23 @@ __global__ void __launch_bounds__(NBR_THREADS) k_boundary_mass(uint32_t n, GridV
     out[i] = make_float4(me.x, me.y, me.z, rho0 * me.w / sum);
 }
 
+// marks the (2R+1)^3 cells around every boundary sample
+__global__ void k_mark_near(uint32_t n, GridView g, const float4* __restrict__ pts,
+    uint8_t* __restrict__ near)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 me = pts[i];
+    const int3 c = clamp_cell(g, cell_of(g, me.x, me.y, me.z), 2);
+    for (int dz = -2; dz <= 2; ++dz)
+        for (int dy = -2; dy <= 2; ++dy) {
+            const int base = (c.z + dz) * g.nxny + (c.y + dy) * g.nx + c.x;
+            for (int dx = -2; dx <= 2; ++dx)
+                near[base + dx] = 1;
+        }
+}
+
 __global__ void k_unpack_mass(uint32_t n, const float4* __restrict__ pts, float* __restrict__ m)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -666,6 +684,11 @@ void boundary_build(reyn_boundary& b, const float* bx, const float* by, const fl
         k_pack_positions<<<blocks_for(nb, THREADS), THREADS, 0, s>>>(
         nb, nullptr, b.x.get(), b.y.get(), b.z.get(), b.m.get(), b.pm.get()));
     b.grid.reordered = true;
+    b.near.resize(size_t(b.grid.geom.cells()));
+    b.near.zero(s);
+    REYN_KERNEL("k_mark_near", s,
+        k_mark_near<<<blocks_for(nb, THREADS), THREADS, 0, s>>>(nb, b.view(), b.pm.get(),
+            b.near.get()));
     if (!bm) {
         DevArray<float4> other(nb);
         const GridView v = b.view();

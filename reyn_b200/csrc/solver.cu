@@ -52,6 +52,7 @@ struct Fluid {
 struct Bdy {
     GridView g;
     const float4* __restrict__ pm;
+    const uint8_t* __restrict__ near; // cells with samples within reach
     uint32_t n;
 };
 
@@ -78,7 +79,25 @@ __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3
     const uint32_t cnt = __ldg(f.ncount + i);
     if (cnt <= KMAX) {
         const uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
-        for (uint32_t k = 0; k < cnt; ++k) {
+        uint32_t k = 0;
+        // four neighbours per round: their index and position loads are
+        // independent, which keeps more of the latency-bound loads in flight
+        for (; k + 4 <= cnt; k += 4) {
+            uint32_t j[4];
+            float4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                j[u] = __ldg(row + size_t(k + u) * 128);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                q[u] = __ldg(f.pm + j[u]);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float dx = me.x - q[u].x, dy = me.y - q[u].y, dz = me.z - q[u].z;
+                fn(j[u], q[u], dx, dy, dz, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+            }
+        }
+        for (; k < cnt; ++k) {
             const uint32_t j = __ldg(row + size_t(k) * 128);
             const float4 q = __ldg(f.pm + j);
             const float dx = me.x - q.x, dy = me.y - q.y, dz = me.z - q.z;
@@ -103,14 +122,26 @@ __device__ __forceinline__ void for_each_boundary(const Bdy& b, float x, float y
     const int3 c = cell_of(b.g, x, y, z);
     if (!cell_inside(b.g, c, 2))
         return;
+    if (!__ldg(b.near + (c.z * b.g.nxny + c.y * b.g.nx + c.x)))
+        return;
     for_each_neighbour<2>(b.g, c, x, y, z, b.pm, f);
 }
 
-// jacobi_update (IISPH.cu:108-117)
-__device__ __forceinline__ float jacobi_update(float omega, float a_ii, float Ap, float s)
+// jacobi_update (IISPH.cu:108-117). The reference compares the float a_ii
+// with the double 1e-6; `tiny` is the smallest float above 1e-6, for which
+// a < tiny holds exactly when (double)a < 1e-6 does (tiny_threshold()).
+__device__ __forceinline__ float jacobi_update(float omega, float a_ii, float Ap, float s,
+    float tiny)
 {
-    return ((double)a_ii < 1e-6 && (double)a_ii > -1e-6) ? 0.f
-                                                          : fmaxf(0.f, omega * (s - Ap) / a_ii);
+    return (a_ii < tiny && a_ii > -tiny) ? 0.f : fmaxf(0.f, omega * (s - Ap) / a_ii);
+}
+
+float tiny_threshold()
+{
+    float t = (float)1e-6;
+    while ((double)t < 1e-6)
+        t = std::nextafterf(t, INFINITY);
+    return t;
 }
 
 // per-sweep reductions (one slot per sweep, zeroed before use)
@@ -160,58 +191,45 @@ __device__ __forceinline__ void block_accumulate(SweepStats* st, unsigned over, 
 // ---- passes ----------------------------------------------------------------
 
 // compute_densities (solver.cuh:18-38) + cached boundary sums + the step's
-// neighbour list (staged per block in shared memory, written row by row)
+// neighbour list, written entry by entry (a block's rows form one 32 KB
+// region, so the L2 merges the scattered 4-byte stores into full lines)
 template <int KIND, int R>
 __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bdy b,
     float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm)
 {
-    __shared__ uint32_t s_list[KMAX][NBR_THREADS];
-    __shared__ uint32_t s_rows[NBR_THREADS / 32];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < n;
+    if (i >= n)
+        return;
+    const float4 me = f.pm[i];
+    const int3 c = fluid_cell<R>(f, me);
+    uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
     uint32_t cnt = 0;
-    if (valid) {
-        const float4 me = f.pm[i];
-        const int3 c = fluid_cell<R>(f, me);
-        float rf = 0.f;
-        for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
-            [&](uint32_t j, const float4& q, float, float, float, float l2) {
-                rf += q.w * pair_w<KIND>(f.kc, l2);
-                if (j != i) {
-                    if (cnt < KMAX)
-                        s_list[cnt][threadIdx.x] = j;
-                    ++cnt;
-                }
-            });
-        float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-        for_each_boundary(b, me.x, me.y, me.z,
-            [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
-                float w, g;
-                pair_wg<KIND>(f.kc, l2, w, g);
-                rb += q.w * w;
-                const float mg = q.w * g;
-                gx += mg * dx;
-                gy += mg * dy;
-                gz += mg * dz;
-            });
-        const float r = rf + rb;
-        rho[i] = r;
-        vel[i].w = r;
-        bterm[i] = make_float4(gx, gy, gz, rb);
-        f.ncount[i] = cnt;
-    }
-    // rows of the block's list: as many as its longest (stored) list
-    uint32_t rows = min(cnt, (uint32_t)KMAX);
-    rows = __reduce_max_sync(0xffffffffu, rows);
-    if ((threadIdx.x & 31) == 0)
-        s_rows[threadIdx.x >> 5] = rows;
-    __syncthreads();
-#pragma unroll
-    for (int w = 0; w < NBR_THREADS / 32; ++w)
-        rows = max(rows, s_rows[w]);
-    uint32_t* __restrict__ out = f.nbr + size_t(blockIdx.x) * (KMAX * 128) + threadIdx.x;
-    for (uint32_t k = 0; k < rows; ++k)
-        out[size_t(k) * 128] = s_list[k][threadIdx.x];
+    float rf = 0.f;
+    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        [&](uint32_t j, const float4& q, float, float, float, float l2) {
+            rf += q.w * pair_w<KIND>(f.kc, l2);
+            if (j != i) {
+                if (cnt < KMAX)
+                    row[size_t(cnt) * 128] = j;
+                ++cnt;
+            }
+        });
+    float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+    for_each_boundary(b, me.x, me.y, me.z,
+        [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
+            float w, g;
+            pair_wg<KIND>(f.kc, l2, w, g);
+            rb += q.w * w;
+            const float mg = q.w * g;
+            gx += mg * dx;
+            gy += mg * dy;
+            gz += mg * dz;
+        });
+    const float r = rf + rb;
+    rho[i] = r;
+    vel[i].w = r;
+    bterm[i] = make_float4(gx, gy, gz, rb);
+    f.ncount[i] = cnt;
 }
 
 // write_non_prs_acc_ff (solver.cuh:40-69): gravity + artificial viscosity;
@@ -384,7 +402,7 @@ __global__ void k_advect(uint32_t n, const float4* __restrict__ pm,
 template <int KIND, int R>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const float4* __restrict__ bterm, float rho0, float dt,
-    float omega, int warmstart, float* __restrict__ aii, float* __restrict__ sii,
+    float omega, int warmstart, float tiny, float* __restrict__ aii, float* __restrict__ sii,
     float* __restrict__ p)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -414,7 +432,55 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
     const float s = (rho0 - vi.w) / dt - (vdiv + fmaf(vi.x, bt.x, fmaf(vi.y, bt.y, vi.z * bt.z)));
     aii[i] = a;
     sii[i] = s;
-    p[i] = warmstart ? p[i] * 0.5f : jacobi_update(omega, a, 0.f, s);
+    p[i] = warmstart ? p[i] * 0.5f : jacobi_update(omega, a, 0.f, s, tiny);
+}
+
+// the diagonal pass fused with the first sweep's pressure accelerations
+// under the warm start: every neighbour's warm-started pressure is half its
+// carried pressure, so a_i = -(1/rho0^2)(sum m_j (p_i' + p_j') grad W_ij +
+// p_i' g_b) with p' = 0.5 p can be summed in the same neighbour loop. p_old
+// is read, p_new written (p_new = 0.5 p_old).
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Fluid f,
+    const float4* __restrict__ vel, const float4* __restrict__ bterm, float rho0, float dt,
+    float r0i, const float* __restrict__ p_old, float* __restrict__ aii,
+    float* __restrict__ sii, float* __restrict__ p_new, float4* __restrict__ acc)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float4 me = f.pm[i];
+    const float4 vi = vel[i];
+    const int3 c = fluid_cell<R>(f, me);
+    const float pi = p_old[i] * 0.5f;
+    float gx = 0.f, gy = 0.f, gz = 0.f, vdiv = 0.f, gsq = 0.f;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    for_each_listed<R>(f, i, c, me,
+        [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
+            const float4 vj = __ldg(vel + j);
+            const float pj = __ldg(p_old + j) * 0.5f;
+            const float g = pair_g<KIND>(f.kc, l2);
+            const float mg = q.w * g;
+            gx += mg * dx;
+            gy += mg * dy;
+            gz += mg * dz;
+            vdiv += mg * fmaf(dx, vi.x - vj.x, fmaf(dy, vi.y - vj.y, dz * (vi.z - vj.z)));
+            gsq += mg * g * l2;
+            const float sp = q.w * (pi + pj) * g;
+            ax += sp * dx;
+            ay += sp * dy;
+            az += sp * dz;
+        });
+    const float4 bt = bterm[i];
+    acc[i] = make_float4(-r0i * (ax + pi * bt.x), -r0i * (ay + pi * bt.y),
+        -r0i * (az + pi * bt.z), 0.f);
+    gx += bt.x;
+    gy += bt.y;
+    gz += bt.z;
+    const float gss = fmaf(gx, gx, fmaf(gy, gy, gz * gz));
+    aii[i] = -dt * (gss + me.w * gsq) / (rho0 * rho0);
+    sii[i] = (rho0 - vi.w) / dt - (vdiv + fmaf(vi.x, bt.x, fmaf(vi.y, bt.y, vi.z * bt.z)));
+    p_new[i] = pi;
 }
 
 // _set_pressure_accelerations (IISPH.cu:68-98)
@@ -449,7 +515,7 @@ template <int KIND, int R>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid f,
     const float4* __restrict__ acc, const float4* __restrict__ bterm,
     const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
-    float dt, float omega, float thr, SweepStats* stats)
+    float dt, float omega, float tiny, float thr, SweepStats* stats)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned over = 0;
@@ -469,7 +535,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
         const float4 bt = bterm[i];
         const float Ap = dt * (sum + fmaf(ai.x, bt.x, fmaf(ai.y, bt.y, ai.z * bt.z)));
         const float s = sii[i];
-        p[i] = p[i] + jacobi_update(omega, aii[i], Ap, s);
+        p[i] = p[i] + jacobi_update(omega, aii[i], Ap, s, tiny);
         const float err = (Ap - s) * dt;
         over = err > thr ? 1u : 0u;
         epos = err > 0.f ? (double)err : 0.0;
@@ -659,6 +725,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         b.g = bdy->view();
         b.g.r2 = f.g.r2;
         b.pm = bdy->pm.get();
+        b.near = bdy->near.get();
         b.n = bdy->nb;
     }
     const unsigned nb = blocks_for(n, NBR_THREADS);
@@ -731,24 +798,41 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             REYN_KERNEL("k_nonpressure", s,
                 k_nonpressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), nu10, eps, grav,
                 dt, sv.acc.get(), sv.vel2.get()));
-            REYN_KERNEL("k_iisph_diag", s,
-                k_iisph_diag<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(), sv.bterm.get(),
-                rho0, dt, P.omega, P.warmstart, sv.aii.get(), sv.sii.get(), sv.p.get()));
+            const float tiny = tiny_threshold();
+            auto pacc = [&] {
+                REYN_KERNEL("k_iisph_pacc", s,
+                    k_iisph_pacc<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(),
+                    sv.bterm.get(), r0i, sv.acc.get()));
+            };
+            if (P.warmstart) {
+                REYN_KERNEL("k_iisph_diag_pacc", s,
+                    k_iisph_diag_pacc<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
+                    sv.bterm.get(), rho0, dt, r0i, sv.p.get(), sv.aii.get(), sv.sii.get(),
+                    sv.p_tmp.get(), sv.acc.get()));
+                sv.p.swap(sv.p_tmp);
+            } else {
+                REYN_KERNEL("k_iisph_diag", s,
+                    k_iisph_diag<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
+                    sv.bterm.get(), rho0, dt, P.omega, P.warmstart, tiny, sv.aii.get(),
+                    sv.sii.get(), sv.p.get()));
+                pacc();
+            }
             const float thr = P.eta * rho0;
+            // IISPH.cu:219-250: [pressure accelerations, Jacobi update]* with
+            // the first accelerations computed above
             for (;;) {
                 SweepStats* slot = slots + (iters % 64);
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats), s));
-                REYN_KERNEL("k_iisph_pacc", s,
-                    k_iisph_pacc<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
-                    r0i, sv.acc.get()));
                 REYN_KERNEL("k_iisph_jacobi", s,
                     k_iisph_jacobi<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.acc.get(),
-                    sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, thr,
-                    slot));
+                    sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, tiny,
+                    thr, slot));
                 iters += 1;
                 const bool last = P.max_iter && iters >= P.max_iter;
-                if (iters < P.min_iter && !last)
+                if (iters < P.min_iter && !last) {
+                    pacc();
                     continue;
+                }
                 readback(slot);
                 sv.stats.avg_density_error = host.err_sum / n / rho0;
                 sv.stats.max_density_error = host.err_max / rho0;
@@ -761,6 +845,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                     converged = false;
                     break;
                 }
+                pacc();
             }
             REYN_KERNEL("k_iisph_final", s,
                 k_iisph_final<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
@@ -781,13 +866,19 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
 __global__ void k_vmax(uint32_t n, const float* __restrict__ vx, const float* __restrict__ vy,
     const float* __restrict__ vz, float* out)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ float s_max[THREADS / 32];
     float v = 0.f;
-    if (i < n)
-        v = norm3df(vx[i], vy[i], vz[i]); // cfl.cu:13-18
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        v = fmaxf(v, norm3df(vx[i], vy[i], vz[i])); // cfl.cu:13-18
     v = warp_max(v);
     if ((threadIdx.x & 31) == 0)
+        s_max[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < THREADS / 32; ++w)
+            v = fmaxf(v, s_max[w]);
         atomic_max_nonneg(out, v);
+    }
 }
 
 float cfl_time_step(reyn_particles& st, float lambda, float h, const float g[3], cudaStream_t s)
@@ -796,7 +887,7 @@ float cfl_time_step(reyn_particles& st, float lambda, float h, const float g[3],
     d.zero(s);
     if (st.n) {
         REYN_KERNEL("k_vmax", s,
-            k_vmax<<<blocks_for(st.n, THREADS), THREADS, 0, s>>>(st.n, st.cur[FVX].get(),
+            k_vmax<<<std::min<unsigned>(blocks_for(st.n, THREADS), 148 * 8), THREADS, 0, s>>>(st.n, st.cur[FVX].get(),
             st.cur[FVY].get(), st.cur[FVZ].get(), d.get()));
     }
     float vmax = 0.f;
