@@ -140,6 +140,31 @@ int reyn_grid_neighbour_stats(const reyn_grid* g, const float* xx,
     const float* xy, const float* xz, const float* m, reyn_kernel kernel,
     uint32_t* count, float* len2, float* rho, void* stream);
 
+/* ---- uniform grid without allocation --------------------------------------
+ * No counterpart in the reference: an added entry point for callers that
+ * cannot allocate device memory — code recorded into CUDA graphs or running
+ * under stream capture, real-time loops that must not wait on the allocator,
+ * and hosts whose device memory belongs to another runtime's pool. It builds
+ * the same grid as reyn_grid_create + reyn_grid_construct (identical prefix
+ * and canonical sorted indices) into the caller's buffers, with its scratch
+ * in one file-scope device array of REYN_GRID_NOALLOC_SCRATCH_WORDS 32-bit
+ * words (32 MiB) that every GPU loading the library holds until exit.
+ *
+ * Limit: nx*ny*nz + 2 n + ceil(nx*ny*nz / 4096) + 2 <= the scratch words
+ * (e.g. 1M particles over 5M cells); larger sizes fail with REYN_ERR_INVALID.
+ * dims (may be NULL) receives nx, ny, nz; prefix == NULL only reports dims.
+ * prefix needs nx*ny*nz + 1 entries (prefix_capacity), sorted n entries.
+ * The first call on each device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) and should come before any stream capture. All
+ * calls share the array: calls that overlap on the GPU race; serialise them.
+ * It synchronises `stream` (to report particles outside the grid). */
+#define REYN_GRID_NOALLOC_SCRATCH_WORDS (8u * 1024u * 1024u)
+int reyn_grid_construct_noalloc(const float bound_min[3],
+    const float bound_max[3], float search_radius, float cell_ratio,
+    const float* xx, const float* xy, const float* xz, uint32_t n,
+    uint32_t* prefix, uint64_t prefix_capacity, uint32_t* sorted,
+    int32_t dims[3], void* stream);
+
 /* ---- boundary (src/scene/scene.cuh:14-46) -------------------------------- */
 typedef struct reyn_boundary reyn_boundary;
 

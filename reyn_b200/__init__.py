@@ -104,6 +104,8 @@ _SIGNATURES = {
     "reyn_enforce_bounds": [_vp, _f * 3, _f * 3, _vp],
     "reyn_solver_pressure_download": [_vp, _vp, _vp],
     "reyn_solver_pressure_upload": [_vp, _vp, _vp, _vp],
+    "reyn_grid_construct_noalloc": [_f * 3, _f * 3, _f, _f, _vp, _vp, _vp, _u32, _vp,
+                                    ctypes.c_uint64, _vp, ctypes.POINTER(ctypes.c_int32), _vp],
     "reyn_profile_enable": [ctypes.c_int],
     "reyn_profile_reset": [],
     "reyn_profile_read": [ctypes.POINTER(ProfileEntry), _u32, ctypes.POINTER(_u32)],
@@ -283,6 +285,23 @@ class Boundary:
         check(lib().reyn_boundary_arrays(self.h, *[ctypes.byref(p) for p in ps],
                                          ctypes.byref(nb)))
         return [p.value for p in ps], nb.value
+
+
+NOALLOC_SCRATCH_WORDS = 8 * 1024 * 1024
+
+
+def grid_construct_noalloc(bmin, bmax, search_radius: float, x, y, z, prefix, sorted_,
+                           cell_ratio: float = 0.5, stream=None):
+    """Uniform-grid build into caller-owned device tensors without any device
+    allocation (reyn_grid_construct_noalloc). prefix=None only returns dims.
+    Returns (nx, ny, nz)."""
+    dims = (ctypes.c_int32 * 3)()
+    n = 0 if x is None else x.numel()
+    cap = 0 if prefix is None else prefix.numel()
+    check(lib().reyn_grid_construct_noalloc(_f3(bmin), _f3(bmax), search_radius, cell_ratio,
+                                            _ptr(x), _ptr(y), _ptr(z), n, _ptr(prefix), cap,
+                                            _ptr(sorted_), dims, _stream(stream)))
+    return tuple(dims)
 
 
 def reference_params(scheme: int, kernel: int, h: float, rho0: float, nu: float) -> Params:
