@@ -12,7 +12,13 @@ state, IISPH step, hard bounds. Inputs are resident in HBM for `value`; `e2e`
 repeats the step through the C ABI with the state uploaded from and downloaded
 to pinned host memory inside the timed region.
 
+The headline is the mixed-precision solver (neighbour positions cell-relative
+FP16, neighbour velocities FP16, FP32 arithmetic, FP64 convergence reduction);
+by default the plain FP32 solver is timed first on the same scene and reported
+beside it ("fp32", "mixed_over_fp32").
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                       [--precision both|mixed|fp32]
 Under torchrun (N > 1) every rank advances its own independently seeded scene
 (weak scaling, no data-path collective); rank 0 prints one JSON line.
 """
@@ -66,6 +72,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--scale", type=int, default=1,
                     help="divide the lattice by this factor per axis (testing only)")
+    ap.add_argument("--precision", choices=["both", "mixed", "fp32"], default="both",
+                    help="both: time the FP32 path, then report the mixed path beside it")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -98,10 +106,12 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(kernel: str):
+def profile_traffic(kernel: str, precision: str):
     """DRAM bytes per launch of `kernel` on this workload, from the committed
-    ncu summary (profiles/<kernel>_iisph_4m.txt, line 'traffic_bytes_per_launch:')."""
-    path = os.path.join(ROOT, "profiles", f"{kernel}_iisph_4m.txt")
+    ncu summary (profiles/<kernel>_iisph_4m[_mixed].txt, line
+    'traffic_bytes_per_launch:')."""
+    suffix = "_mixed" if precision == "mixed" else ""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_iisph_4m{suffix}.txt")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -188,12 +198,13 @@ class EngineRun:
     """The workload on the engine: one scene, its grid, boundary and solver,
     and the main-loop step (main.cu:64-75)."""
 
-    def __init__(self, rank: int, scale: int, dev):
+    def __init__(self, rank: int, scale: int, dev, precision: str):
         import torch
 
         import reyn_b200 as rb
 
         self.rb = rb
+        self.precision = precision
         self.sc = sc = scene_for(rank, scale)
         self.n = sc.n
         self.st = rb.Particles(sc.n, sc.rho0)
@@ -205,6 +216,7 @@ class EngineRun:
         prm.convergence = rb.CONV_AVERAGE
         prm.eta = 0.001
         prm.max_iter = 1000
+        prm.precision = rb.PRECISION_MIXED if precision == "mixed" else rb.PRECISION_FP32
         self.sv = rb.Solver(rb.IISPH, prm, sc.n)
         self.dt, self.iters = DT0, 0
         self.dt_visc = viscous_dt_limit(sc.h, NU)
@@ -243,24 +255,19 @@ class EngineRun:
             o.close()
 
 
-def run_engine(a, world, rank, local):
+def timed_steps(run, a, world, stream, dev):
+    """W warm-up steps, checkpoint, then K steps timed with CUDA events
+    (max over ranks), with per-kernel launch counts and device time and the
+    SM clocks sampled during the timed region."""
     import torch
 
-    import reyn_b200 as rb
-
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    run = EngineRun(rank, a.scale, dev)
-    n = run.n
-    stream = torch.cuda.current_stream(dev)
+    rb = run.rb
     S = stream.cuda_stream
-
     for _ in range(a.warmup):
         run.step(S)
     torch.cuda.synchronize()
     ck = run.checkpoint()  # the timed region starts here (replayed for e2e)
     run.log.clear()
-
     gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
     clocks = ClockSampler(gpu_uuid)
     time.sleep(0.3)
@@ -281,8 +288,42 @@ def run_engine(a, world, rank, local):
     ck_clocks = clocks.stop()
     ms = e0.elapsed_time(e1)
     ms_max = max_over_ranks(world, ms)
+    return ck, ms, ms_max, prof, ck_clocks, list(run.log)
+
+
+def leg_summary(run, a, world, ms_max, log):
+    return {"value": round(world * run.n * a.steps / (ms_max / 1e3), 1), "unit": UNIT,
+            "ms_per_step": round(ms_max / a.steps, 3),
+            "iters_per_step": [x[0] for x in log],
+            "avg_density_error_per_step": [round(x[1], 7) for x in log],
+            "iter_limit_hits": run.limit_hits}
+
+
+def run_engine(a, world, rank, local):
+    import torch
+
+    import reyn_b200 as rb
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    S = stream.cuda_stream
+
+    # the plain FP32 path first, on the same scene, as the comparison leg
+    fp32 = None
+    if a.precision == "both":
+        run = EngineRun(rank, a.scale, dev, "fp32")
+        _, _, ms32, _, clk32, log32 = timed_steps(run, a, world, stream, dev)
+        fp32 = leg_summary(run, a, world, ms32, log32)
+        fp32["clocks"] = clk32
+        run.close()
+        torch.cuda.synchronize()
+
+    headline = "fp32" if a.precision == "fp32" else "mixed"
+    run = EngineRun(rank, a.scale, dev, headline)
+    n = run.n
+    ck, ms, ms_max, prof, ck_clocks, log = timed_steps(run, a, world, stream, dev)
     value = world * n * a.steps / (ms_max / 1e3)
-    log = list(run.log)
 
     # dominant kernel and its roofline (CUDA events around its launches)
     launches = sum(v[0] for v in prof.values())
@@ -293,7 +334,7 @@ def run_engine(a, world, rank, local):
     achieved = alg / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": profile_traffic(dom_name), "peak_source": peak_kind,
+                "traffic": profile_traffic(dom_name, headline), "peak_source": peak_kind,
                 "alg_bytes_per_launch": alg, "ms_per_launch": round(per_launch_s * 1e3, 4),
                 "share_of_step": round(dom_ms / ms, 4)}
     kernels = {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in
@@ -333,10 +374,13 @@ def run_engine(a, world, rank, local):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline_from(ck, run)
 
+    precision = ("fp32 storage and math" if headline == "fp32" else
+                 "mixed: neighbour positions cell-relative FP16, neighbour velocities FP16, "
+                 "own data and all arithmetic FP32, FP64 convergence reduction")
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 3),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded lattice + jitter dam break; Akinci box walls)",
         "config": {"workload": WORKLOAD, "particles_per_gpu": n,
                    "boundary_particles": run.sc.nb, "kernel": "C2", "h": run.sc.h,
@@ -344,7 +388,7 @@ def run_engine(a, world, rank, local):
                    "convergence": "avg density error <= 0.1% (FP64 reduction)",
                    "dt": f"min(simple_dt_controller(lambda={LAMBDA}, target 10 iters, "
                          f"0.1%/step) from {DT0}, 0.08 h^2/nu = {run.dt_visc:.2e})",
-                   "precision": "fp32", "parallelism": f"replicas{world}",
+                   "precision": precision, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (state 4M x 28 B + grid 70 MB per step)"},
         "clocks": ck_clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
         "cpu_baseline": cpu,
@@ -353,6 +397,9 @@ def run_engine(a, world, rank, local):
         "dt_per_step": [float(f"{x[2]:.4e}") for x in log],
         "iter_limit_hits": run.limit_hits, "kernels": kernels,
     }
+    if fp32 is not None:
+        out["fp32"] = fp32
+        out["mixed_over_fp32"] = round(value / fp32["value"], 3)
     if rank == 0:
         print(json.dumps(out), flush=True)
     run.close()

@@ -199,6 +199,16 @@ typedef enum reyn_convergence {
     REYN_CONV_AVERAGE = 1
 } reyn_convergence;
 
+typedef enum reyn_precision {
+    /* FP32 storage and arithmetic, as the reference */
+    REYN_PRECISION_FP32 = 0,
+    /* IISPH only: neighbour positions stored as FP16 offsets within their
+     * grid cell and neighbour velocities/densities as FP16; the particle's
+     * own data and all arithmetic stay FP32, the convergence reduction FP64.
+     * Up to 2^25 particles. */
+    REYN_PRECISION_MIXED = 1
+} reyn_precision;
+
 typedef struct reyn_params {
     reyn_kernel kernel;     /* support radius = 2h (main.cu:51) */
     float h;                /* particle spacing */
@@ -212,6 +222,7 @@ typedef struct reyn_params {
     float omega;            /* IISPH Jacobi weight (0.5, IISPH.cuh:45) */
     int32_t warmstart;      /* IISPH p *= 0.5 (IISPH.cuh:48) */
     reyn_convergence convergence;
+    reyn_precision precision; /* REYN_PRECISION_FP32 unless set */
 } reyn_params;
 
 /* the reference's constants for `scheme` (gravity (0,-9.81,0)) */

@@ -1,0 +1,161 @@
+"""FP64 restatement of the IISPH step — TEST INFRASTRUCTURE ONLY.
+
+The error reference for the engine's precision modes: the same algorithm as
+the FP32 oracle (oracle.cpp, which follows the reference's IISPH.cu), carried
+out in double precision with numpy over explicit pair lists (scipy's k-d tree
+finds the pairs; the summation order differs from any grid traversal, which
+FP64 makes irrelevant at the tolerances the tests use). Both the FP32 engine
+and the mixed-precision engine are measured against it, so the cost of FP16
+storage is stated as an error against the exact arithmetic rather than
+against another FP32 result.
+
+Reference functions restated (reyn, src/):
+* kernels.cuh:32-64 (W, nabla) and :78-165 (C2, B3, W6, COS shapes)
+* solver.cuh:18-38 compute_densities, :40-69 write_non_prs_acc_ff
+* solver.cu:3-32 integrate_a_v_only, integrate
+* IISPH.cu:11-66 diagonal element and source term, :68-98 pressure
+  accelerations, :108-162 Jacobi update, :165-262 the step
+* scene.cu:466-483 hard_enforce_bounds
+
+Only tests/ import this module.
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy.spatial import cKDTree
+
+C2, B3, W6, COS = 0, 1, 2, 3
+
+_ALPHA = {C2: 21.0 / 2.0 / np.pi, B3: 16.0 / np.pi, W6: 1365.0 / 64.0 / np.pi,
+          COS: np.pi / (4.0 * np.pi * np.pi - 30.0)}
+
+
+def _w(kind: int, q):
+    """kernels.cuh:78-165, w(q) on [0, 1]."""
+    t1 = np.maximum(0.0, 1.0 - q)
+    if kind == C2:
+        return t1 ** 4 * (4.0 * q + 1.0)
+    if kind == B3:
+        t2 = np.clip(0.5 - q, 0.0, 1.0)
+        return t1 ** 3 - 4.0 * t2 ** 3
+    if kind == W6:
+        return t1 ** 8 * (32.0 * q ** 3 + 25.0 * q * q + 8.0 * q + 1.0)
+    s = np.pi * np.minimum(1.0, q)
+    return 4.0 * np.cos(s) + np.cos(2.0 * s) + 3.0
+
+
+def _dw(kind: int, q):
+    """kernels.cuh:78-165, dw/dq on [0, 1]."""
+    t1 = np.maximum(0.0, 1.0 - q)
+    if kind == C2:
+        return t1 ** 3 * (-20.0 * q)
+    if kind == B3:
+        t2 = np.clip(0.5 - q, 0.0, 1.0)
+        return -3.0 * t1 * t1 + 12.0 * t2 * t2
+    if kind == W6:
+        return t1 ** 7 * (16.0 * q * q + 7.0 * q + 1.0) * (-22.0 * q)
+    s = np.pi * np.minimum(1.0, q)
+    return -4.0 * np.pi * np.sin(s) - 2.0 * np.pi * np.sin(2.0 * s)
+
+
+class _Pairs:
+    """All pairs (i, j) with |x_i - x_j| < r, i from `a`, j from `b`, with the
+    kernel value and the gradient factor: grad W_ij = gf * x_ij."""
+
+    def __init__(self, kind: int, hbar: float, a: np.ndarray, b: np.ndarray, same: bool):
+        ta = cKDTree(a)
+        tb = ta if same else cKDTree(b)
+        sp = ta.sparse_distance_matrix(tb, hbar, output_type="ndarray")
+        # for a tree against itself the pairs include i == j (distance 0)
+        i, j = sp["i"].astype(np.int64), sp["j"].astype(np.int64)
+        x = a[i] - b[j]
+        r = np.sqrt((x * x).sum(1))
+        q = np.minimum(r / hbar, 1.0)
+        alpha = _ALPHA[kind]
+        self.i, self.j, self.x, self.r2 = i, j, x, r * r
+        self.w = alpha / hbar ** 3 * _w(kind, q)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            gf = alpha / hbar ** 4 * _dw(kind, q) / r
+        self.gf = np.where(np.isfinite(gf), gf, 0.0)
+        self.n = a.shape[0]
+
+    def sum(self, v):
+        """sum over j of v (per pair, scalar or (P, 3)) into i."""
+        if v.ndim == 1:
+            return np.bincount(self.i, weights=v, minlength=self.n)
+        return np.stack([np.bincount(self.i, weights=v[:, c], minlength=self.n)
+                         for c in range(v.shape[1])], 1)
+
+
+def iisph_run(kind: int, fluid: dict, bdy: dict, box_min, box_max, h: float, rho0: float,
+              nu: float, g, dt: float, steps: int, iters: int, omega: float = 0.5,
+              warmstart: bool = True, p=None):
+    """`steps` IISPH steps with exactly `iters` Jacobi sweeps each (the
+    convergence test is left out, so that every precision runs the same
+    arithmetic). fluid: x, y, z, vx, vy, vz, m (any order); bdy: x, y, z, m.
+    Returns dict of float64 arrays in the input order: x, y, z, vx, vy, vz,
+    rho, p, aii, sii."""
+    X = np.stack([np.asarray(fluid[k], np.float64) for k in ("x", "y", "z")], 1)
+    V = np.stack([np.asarray(fluid[k], np.float64) for k in ("vx", "vy", "vz")], 1)
+    m = np.asarray(fluid["m"], np.float64)
+    B = np.stack([np.asarray(bdy[k], np.float64) for k in ("x", "y", "z")], 1)
+    mb = np.asarray(bdy["m"], np.float64)
+    n = m.size
+    P = np.zeros(n) if p is None else np.asarray(p, np.float64).copy()
+    lo = np.asarray(box_min, np.float64)
+    hi = np.asarray(box_max, np.float64)
+    grav = np.asarray(g, np.float64)
+    hbar = 2.0 * h
+    r0i = 1.0 / (rho0 * rho0)
+    rho = aii = sii = None
+    for _ in range(steps):
+        F = _Pairs(kind, hbar, X, X, True)
+        Bp = _Pairs(kind, hbar, X, B, False) if mb.size else None
+        mj = m[F.j]
+        # densities (solver.cuh:18-38)
+        rho = F.sum(mj * F.w)
+        gb = np.zeros((n, 3))
+        if Bp is not None:
+            rho += Bp.sum(mb[Bp.j] * Bp.w)
+            gb = Bp.sum((mb[Bp.j] * Bp.gf)[:, None] * Bp.x)
+        # gravity + artificial viscosity (solver.cuh:40-69), then v*
+        vij = V[F.i] - V[F.j]
+        vx = (vij * F.x).sum(1)
+        s = 10.0 * nu * mj / rho[F.j] * vx / (F.r2 + 0.01 * h * h) * F.gf
+        V = V + dt * (grav + F.sum(s[:, None] * F.x))
+        # diagonal element and source term (IISPH.cu:11-66)
+        vij = V[F.i] - V[F.j]
+        mg = mj * F.gf
+        gff = F.sum(mg[:, None] * F.x)
+        gsq = F.sum(mg * F.gf * F.r2)
+        vdiv = F.sum(mg * (vij * F.x).sum(1))
+        grad = gff + gb
+        aii = -dt * ((grad * grad).sum(1) + m * gsq) * r0i
+        sii = (rho0 - rho) / dt - (vdiv + (V * gb).sum(1))
+
+        def jacobi(Ap):  # IISPH.cu:108-117
+            small = np.abs(aii) < 1e-6
+            with np.errstate(divide="ignore", invalid="ignore"):
+                d = np.maximum(0.0, omega * (sii - Ap) / aii)
+            return np.where(small, 0.0, d)
+
+        def pacc(P):  # IISPH.cu:68-98
+            sp = mj * (P[F.i] + P[F.j]) * F.gf
+            return -r0i * (F.sum(sp[:, None] * F.x) + P[:, None] * gb)
+
+        P = 0.5 * P if warmstart else jacobi(np.zeros(n))
+        for _ in range(iters):  # IISPH.cu:119-162
+            A = pacc(P)
+            aij = A[F.i] - A[F.j]
+            Ap = dt * (F.sum(mj * F.gf * (aij * F.x).sum(1)) + (A * gb).sum(1))
+            P = P + jacobi(Ap)
+        A = pacc(P)
+        # integrate (solver.cu:15-32)
+        V = V + dt * A
+        X = X + dt * V
+        # hard_enforce_bounds (scene.cu:466-483)
+        touch = ((X <= lo) | (X >= hi)).any(1)
+        V[touch] *= -0.1
+        X = np.clip(X, lo, hi)
+    return {"x": X[:, 0], "y": X[:, 1], "z": X[:, 2], "vx": V[:, 0], "vy": V[:, 1],
+            "vz": V[:, 2], "rho": rho, "p": P, "aii": aii, "sii": sii}

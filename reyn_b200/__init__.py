@@ -23,6 +23,7 @@ C2, B3, W6, COS = 0, 1, 2, 3
 KERNELS = {"C2": C2, "B3": B3, "W6": W6, "COS": COS}
 SESPH, PCISPH, IISPH = 0, 1, 2
 CONV_REFERENCE, CONV_AVERAGE = 0, 1
+PRECISION_FP32, PRECISION_MIXED = 0, 1
 
 OK = 0
 ERR_INVALID, ERR_OUT_OF_BOUNDS, ERR_NONFINITE, ERR_ITER_LIMIT = -1, -2, -3, -4
@@ -53,7 +54,8 @@ class GridInfo(ctypes.Structure):
 class Params(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int), ("h", _f), ("rho0", _f), ("nu", _f), ("g", _f * 3),
                 ("k_sesph", _f), ("eta", _f), ("min_iter", _u32), ("max_iter", _u32),
-                ("omega", _f), ("warmstart", ctypes.c_int32), ("convergence", ctypes.c_int)]
+                ("omega", _f), ("warmstart", ctypes.c_int32), ("convergence", ctypes.c_int),
+                ("precision", ctypes.c_int)]
 
 
 class SolverBuffers(ctypes.Structure):

@@ -33,6 +33,10 @@ void check_params(reyn_scheme scheme, const reyn_params* p)
     require(p->omega > 0.f && p->omega < 2.f, "omega must lie in (0, 2)");
     require(p->convergence == REYN_CONV_REFERENCE || p->convergence == REYN_CONV_AVERAGE,
         "unknown convergence criterion");
+    require(p->precision == REYN_PRECISION_FP32 || p->precision == REYN_PRECISION_MIXED,
+        "unknown precision");
+    require(p->precision == REYN_PRECISION_FP32 || scheme == REYN_IISPH,
+        "mixed precision is implemented for IISPH");
 }
 
 void check_vec3(const float* v, const char* what)
@@ -298,6 +302,7 @@ int reyn_params_reference(reyn_scheme scheme, reyn_kernel kernel, float h, float
         p.omega = 0.5f; // IISPH.cuh:45
         p.warmstart = 1; // IISPH.cuh:48
         p.convergence = REYN_CONV_REFERENCE;
+        p.precision = REYN_PRECISION_FP32;
         *out = p;
     });
 }
@@ -309,6 +314,8 @@ int reyn_solver_create(reyn_scheme scheme, const reyn_params* params, uint32_t n
         require(out != nullptr, "null output handle");
         *out = nullptr;
         check_params(scheme, params);
+        require(params->precision == REYN_PRECISION_FP32 || n <= (1u << 25),
+            "mixed precision handles at most 2^25 particles");
         auto s = std::make_unique<reyn_solver>();
         s->scheme = scheme;
         s->prm = *params;

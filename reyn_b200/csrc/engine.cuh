@@ -97,6 +97,7 @@ struct reyn_solver {
     reyn::DevArray<float4> acc, vel2, bterm;
     reyn::DevArray<float> p_tmp;
     reyn::DevArray<uint32_t> nbr, ncount; // per-step neighbour list
+    reyn::DevArray<uint2> pmh, velh, velh2; // mixed-precision neighbour records
     reyn::DevArray<unsigned char> sweep_stats; // per-sweep reductions
     std::unique_ptr<reyn::PinnedArray<unsigned char>> readback;
     uint64_t p_epoch = 0;      // particle epoch p is ordered for

@@ -16,6 +16,8 @@
 // PCISPH.cu:15-111, IISPH.cu:11-262.
 #include "engine.cuh"
 
+#include <cuda_fp16.h>
+
 #include <cmath>
 #include <type_traits>
 
@@ -47,7 +49,75 @@ struct Fluid {
     uint32_t* status;
     uint32_t* __restrict__ nbr;    // neighbour list (list_slot layout)
     uint32_t* __restrict__ ncount; // neighbours per particle
+    // mixed precision: per particle (ox, oy, oz, m / m_0) as four FP16, the
+    // offsets relative to the particle's cell in cell units, m_0 = pm[0].w
+    const uint2* __restrict__ pmh;
 };
+
+// ---- mixed precision ----------------------------------------------------------
+// Neighbour data is stored as FP16 (positions relative to their cell,
+// velocities, density); the particle's own data and all arithmetic stay
+// FP32. x_ij = ((o_i - o_j) - (c_j - c_i)) * cell: the integer cell delta is
+// packed into the top 7 bits of the list entry (index in the low 25 bits),
+// the offsets o in [0, 1) are exact FP32 differences of FP16 values, so
+// x_ij carries at most 2^-11 cells of rounding.
+constexpr uint32_t IDX_BITS = 25;
+constexpr uint32_t IDX_MASK = (1u << IDX_BITS) - 1u;
+
+__device__ __forceinline__ float4 half4_to_float4(uint2 u)
+{
+    __half2 a, b;
+    memcpy(&a, &u.x, 4);
+    memcpy(&b, &u.y, 4);
+    const float2 fa = __half22float2(a), fb = __half22float2(b);
+    return make_float4(fa.x, fa.y, fb.x, fb.y);
+}
+
+__device__ __forceinline__ uint2 float4_to_half4(float4 v)
+{
+    const __half2 a = __floats2half2_rn(v.x, v.y), b = __floats2half2_rn(v.z, v.w);
+    uint2 u;
+    memcpy(&u.x, &a, 4);
+    memcpy(&u.y, &b, 4);
+    return u;
+}
+
+// cell (floor of the position in cell units) and offset within it; the
+// mixed path's own decomposition, consistent between writer and readers
+__device__ __forceinline__ void cell_offset(const GridView& g, float x, float y, float z,
+    int3& c, float3& o)
+{
+    const float ux = (x - g.lox) * g.inv_cell, uy = (y - g.loy) * g.inv_cell,
+                uz = (z - g.loz) * g.inv_cell;
+    const float fx = floorf(ux), fy = floorf(uy), fz = floorf(uz);
+    c = make_int3((int)fx, (int)fy, (int)fz);
+    o = make_float3(ux - fx, uy - fy, uz - fz);
+}
+
+// c_j - c_i in [-2, 2]^3 (neighbours lie within two cells) <-> 0..124
+__device__ __forceinline__ uint32_t delta_code(int dx, int dy, int dz)
+{
+    return uint32_t((dz + 2) * 25 + (dy + 2) * 5 + (dx + 2));
+}
+
+__device__ __forceinline__ void delta_decode(uint32_t code, float& dx, float& dy, float& dz)
+{
+    const uint32_t z = code / 25u, r = code - z * 25u, y = r / 5u;
+    dz = (float)z - 2.f;
+    dy = (float)y - 2.f;
+    dx = (float)(r - y * 5u) - 2.f;
+}
+
+// a neighbour's velocity/density record: FP32 or FP16 storage
+template <bool MIX>
+__device__ __forceinline__ float4 nbr_vel(const float4* __restrict__ v32,
+    const uint2* __restrict__ v16, uint32_t j)
+{
+    if constexpr (MIX)
+        return half4_to_float4(__ldg(v16 + j));
+    else
+        return __ldg(v32 + j);
+}
 
 struct Bdy {
     GridView g;
@@ -72,35 +142,63 @@ __device__ __forceinline__ int3 fluid_cell(const Fluid& f, const float4& me)
 // the fluid neighbours j != i of particle i from the step's list (or, for a
 // particle whose list overflowed, from the cell traversal); f(j, pm[j], dx,
 // dy, dz, l2) in the traversal order of the cells
-template <int R, class F>
+template <int R, bool MIX = false, class F>
 __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3 c,
     const float4& me, F&& fn)
 {
     const uint32_t cnt = __ldg(f.ncount + i);
     if (cnt <= KMAX) {
         const uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
+        [[maybe_unused]] float3 oi {};
+        [[maybe_unused]] float m0 = 0.f;
+        if constexpr (MIX) {
+            int3 ci;
+            cell_offset(f.g, me.x, me.y, me.z, ci, oi);
+            m0 = __ldg(&f.pm[0].w);
+            m0 = m0 != 0.f ? m0 : 1.f;
+        }
+        // one neighbour: index (and cell delta), position data, the pair
+        auto pair = [&](uint32_t e, uint32_t& j, float4& q, float& dx, float& dy, float& dz) {
+            if constexpr (MIX) {
+                j = e & IDX_MASK;
+                const float4 h = half4_to_float4(__ldg(f.pmh + j));
+                float ex, ey, ez;
+                delta_decode(e >> IDX_BITS, ex, ey, ez);
+                dx = ((oi.x - h.x) - ex) * f.g.cell;
+                dy = ((oi.y - h.y) - ey) * f.g.cell;
+                dz = ((oi.z - h.z) - ez) * f.g.cell;
+                q = make_float4(0.f, 0.f, 0.f, m0 * h.w);
+            } else {
+                j = e;
+                q = __ldg(f.pm + j);
+                dx = me.x - q.x;
+                dy = me.y - q.y;
+                dz = me.z - q.z;
+            }
+        };
         uint32_t k = 0;
         // four neighbours per round: their index and position loads are
         // independent, which keeps more of the latency-bound loads in flight
         for (; k + 4 <= cnt; k += 4) {
-            uint32_t j[4];
+            uint32_t e[4], j[4];
             float4 q[4];
+            float dx[4], dy[4], dz[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                j[u] = __ldg(row + size_t(k + u) * 128);
+                e[u] = __ldg(row + size_t(k + u) * 128);
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                q[u] = __ldg(f.pm + j[u]);
+                pair(e[u], j[u], q[u], dx[u], dy[u], dz[u]);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const float dx = me.x - q[u].x, dy = me.y - q[u].y, dz = me.z - q[u].z;
-                fn(j[u], q[u], dx, dy, dz, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
-            }
+            for (int u = 0; u < 4; ++u)
+                fn(j[u], q[u], dx[u], dy[u], dz[u],
+                    fmaf(dx[u], dx[u], fmaf(dy[u], dy[u], dz[u] * dz[u])));
         }
         for (; k < cnt; ++k) {
-            const uint32_t j = __ldg(row + size_t(k) * 128);
-            const float4 q = __ldg(f.pm + j);
-            const float dx = me.x - q.x, dy = me.y - q.y, dz = me.z - q.z;
+            uint32_t j;
+            float4 q;
+            float dx, dy, dz;
+            pair(__ldg(row + size_t(k) * 128), j, q, dx, dy, dz);
             fn(j, q, dx, dy, dz, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
         }
     } else {
@@ -192,28 +290,53 @@ __device__ __forceinline__ void block_accumulate(SweepStats* st, unsigned over, 
 
 // compute_densities (solver.cuh:18-38) + cached boundary sums + the step's
 // neighbour list, written entry by entry (a block's rows form one 32 KB
-// region, so the L2 merges the scattered 4-byte stores into full lines)
-template <int KIND, int R>
+// region, so the L2 merges the scattered 4-byte stores into full lines).
+// Mixed precision: list entries carry the neighbour's cell delta, and the
+// particle's FP16 position/velocity records are written for later passes.
+template <int KIND, int R, bool MIX = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bdy b,
-    float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm)
+    float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm,
+    uint2* __restrict__ pmh_out, uint2* __restrict__ velh_out)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
     const float4 me = f.pm[i];
     const int3 c = fluid_cell<R>(f, me);
+    [[maybe_unused]] int3 cm {};
+    [[maybe_unused]] float3 om {};
+    if constexpr (MIX)
+        cell_offset(f.g, me.x, me.y, me.z, cm, om);
     uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
     uint32_t cnt = 0;
+    [[maybe_unused]] bool far = false; // a cell delta outside [-2, 2] (rounding)
     float rf = 0.f;
     for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
         [&](uint32_t j, const float4& q, float, float, float, float l2) {
             rf += q.w * pair_w<KIND>(f.kc, l2);
             if (j != i) {
-                if (cnt < KMAX)
-                    row[size_t(cnt) * 128] = j;
+                if (cnt < KMAX) {
+                    uint32_t e = j;
+                    if constexpr (MIX) {
+                        const int dx = (int)floorf((q.x - f.g.lox) * f.g.inv_cell) - cm.x;
+                        const int dy = (int)floorf((q.y - f.g.loy) * f.g.inv_cell) - cm.y;
+                        const int dz = (int)floorf((q.z - f.g.loz) * f.g.inv_cell) - cm.z;
+                        if (abs(dx) > 2 || abs(dy) > 2 || abs(dz) > 2)
+                            far = true;
+                        else
+                            e |= delta_code(dx, dy, dz) << IDX_BITS;
+                    }
+                    row[size_t(cnt) * 128] = e;
+                }
                 ++cnt;
             }
         });
+    if constexpr (MIX) {
+        // a pair the FP16 record cannot encode: this particle is served by the
+        // FP32 cell traversal in every later pass, like a list overflow
+        if (far)
+            cnt = KMAX + 1;
+    }
     float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     for_each_boundary(b, me.x, me.y, me.z,
         [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
@@ -230,14 +353,22 @@ __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bd
     vel[i].w = r;
     bterm[i] = make_float4(gx, gy, gz, rb);
     f.ncount[i] = cnt;
+    if constexpr (MIX) {
+        const float4 v = vel[i];
+        const float m0 = __ldg(&f.pm[0].w);
+        pmh_out[i] = float4_to_half4(make_float4(om.x, om.y, om.z, me.w / (m0 != 0.f ? m0 : 1.f)));
+        velh_out[i] = float4_to_half4(make_float4(v.x, v.y, v.z, r));
+    }
 }
 
 // write_non_prs_acc_ff (solver.cuh:40-69): gravity + artificial viscosity;
 // optionally fused with integrate_a_v_only (solver.cu:3-13) into vel_out
-template <int KIND, int R>
+// (and its FP16 copy velh_out under mixed precision)
+template <int KIND, int R, bool MIX = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_nonpressure(uint32_t n, Fluid f,
-    const float4* __restrict__ vel, float nu10, float eps, float3 grav, float dt,
-    float4* __restrict__ acc, float4* __restrict__ vel_out)
+    const float4* __restrict__ vel, const uint2* __restrict__ velh, float nu10, float eps,
+    float3 grav, float dt, float4* __restrict__ acc, float4* __restrict__ vel_out,
+    uint2* __restrict__ velh_out)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
@@ -246,9 +377,9 @@ __global__ void __launch_bounds__(NBR_THREADS) k_nonpressure(uint32_t n, Fluid f
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
     float ax = grav.x, ay = grav.y, az = grav.z;
-    for_each_listed<R>(f, i, c, me,
+    for_each_listed<R, MIX>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
-            const float4 vj = __ldg(vel + j);
+            const float4 vj = nbr_vel<MIX>(vel, velh, j);
             const float vdx = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
             const float s = (nu10 * q.w / vj.w * vdx) / (l2 + eps) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
@@ -256,8 +387,12 @@ __global__ void __launch_bounds__(NBR_THREADS) k_nonpressure(uint32_t n, Fluid f
             az += s * dz;
         });
     acc[i] = make_float4(ax, ay, az, 0.f);
-    if (vel_out)
-        vel_out[i] = make_float4(vi.x + dt * ax, vi.y + dt * ay, vi.z + dt * az, vi.w);
+    if (vel_out) {
+        const float4 vs = make_float4(vi.x + dt * ax, vi.y + dt * ay, vi.z + dt * az, vi.w);
+        vel_out[i] = vs;
+        if constexpr (MIX)
+            velh_out[i] = float4_to_half4(vs);
+    }
 }
 
 __device__ __forceinline__ float eos_sesph(float rho, float k, float rho0)
@@ -399,9 +534,10 @@ __global__ void k_advect(uint32_t n, const float4* __restrict__ pm,
 
 // _compute_diagonal_elem_and_source_term (IISPH.cu:11-66) + warm start
 // (IISPH.cu:193-209)
-template <int KIND, int R>
+template <int KIND, int R, bool MIX = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
-    const float4* __restrict__ vel, const float4* __restrict__ bterm, float rho0, float dt,
+    const float4* __restrict__ vel, const uint2* __restrict__ velh,
+    const float4* __restrict__ bterm, float rho0, float dt,
     float omega, int warmstart, float tiny, float* __restrict__ aii, float* __restrict__ sii,
     float* __restrict__ p)
 {
@@ -412,9 +548,9 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
     float gx = 0.f, gy = 0.f, gz = 0.f, vdiv = 0.f, gsq = 0.f;
-    for_each_listed<R>(f, i, c, me,
+    for_each_listed<R, MIX>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
-            const float4 vj = __ldg(vel + j);
+            const float4 vj = nbr_vel<MIX>(vel, velh, j);
             const float g = pair_g<KIND>(f.kc, l2);
             const float mg = q.w * g;
             gx += mg * dx;
@@ -440,9 +576,10 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
 // carried pressure, so a_i = -(1/rho0^2)(sum m_j (p_i' + p_j') grad W_ij +
 // p_i' g_b) with p' = 0.5 p can be summed in the same neighbour loop. p_old
 // is read, p_new written (p_new = 0.5 p_old).
-template <int KIND, int R>
+template <int KIND, int R, bool MIX = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Fluid f,
-    const float4* __restrict__ vel, const float4* __restrict__ bterm, float rho0, float dt,
+    const float4* __restrict__ vel, const uint2* __restrict__ velh,
+    const float4* __restrict__ bterm, float rho0, float dt,
     float r0i, const float* __restrict__ p_old, float* __restrict__ aii,
     float* __restrict__ sii, float* __restrict__ p_new, float4* __restrict__ acc)
 {
@@ -455,9 +592,9 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
     const float pi = p_old[i] * 0.5f;
     float gx = 0.f, gy = 0.f, gz = 0.f, vdiv = 0.f, gsq = 0.f;
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_listed<R>(f, i, c, me,
+    for_each_listed<R, MIX>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
-            const float4 vj = __ldg(vel + j);
+            const float4 vj = nbr_vel<MIX>(vel, velh, j);
             const float pj = __ldg(p_old + j) * 0.5f;
             const float g = pair_g<KIND>(f.kc, l2);
             const float mg = q.w * g;
@@ -484,7 +621,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
 }
 
 // _set_pressure_accelerations (IISPH.cu:68-98)
-template <int KIND, int R>
+template <int KIND, int R, bool MIX = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     float4* __restrict__ acc)
@@ -496,7 +633,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
     const int3 c = fluid_cell<R>(f, me);
     const float pi = p[i];
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_listed<R>(f, i, c, me,
+    for_each_listed<R, MIX>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float s = q.w * (pi + __ldg(p + j)) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
@@ -511,7 +648,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
 // _jacobi_update_pressures (IISPH.cu:119-162); the convergence bitmask of the
 // reference becomes a count of particles above the threshold, reduced per
 // block together with the FP64 sum of max(0, error)
-template <int KIND, int R>
+template <int KIND, int R, bool MIX = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid f,
     const float4* __restrict__ acc, const float4* __restrict__ bterm,
     const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
@@ -526,7 +663,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
         const int3 c = fluid_cell<R>(f, me);
         const float4 ai = acc[i];
         float sum = 0.f;
-        for_each_listed<R>(f, i, c, me,
+        for_each_listed<R, MIX>(f, i, c, me,
             [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
                 const float4 aj = __ldg(acc + j);
                 const float d = fmaf(ai.x - aj.x, dx, fmaf(ai.y - aj.y, dy, (ai.z - aj.z) * dz));
@@ -545,7 +682,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
 }
 
 // final _set_pressure_accelerations + integrate (IISPH.cu:248-257)
-template <int KIND, int R>
+template <int KIND, int R, bool MIX = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     const float4* __restrict__ vel, float dt, float4* __restrict__ acc,
@@ -559,7 +696,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f
     const int3 c = fluid_cell<R>(f, me);
     const float pi = p[i];
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_listed<R>(f, i, c, me,
+    for_each_listed<R, MIX>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float s = q.w * (pi + __ldg(p + j)) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
@@ -670,6 +807,11 @@ static void ensure_buffers(reyn_solver& sv, uint32_t n)
     sv.bterm.resize(n);
     sv.nbr.resize(list_capacity(n));
     sv.ncount.resize(n);
+    if (sv.prm.precision == REYN_PRECISION_MIXED) {
+        sv.pmh.resize(n);
+        sv.velh.resize(n);
+        sv.velh2.resize(n);
+    }
     if (sv.p.size() != n) {
         sv.p.resize(n);
         REYN_CUDA(cudaMemset(sv.p.get(), 0, size_t(n) * sizeof(float)));
@@ -720,6 +862,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     f.status = const_cast<uint32_t*>(grid.status.get());
     f.nbr = sv.nbr.get();
     f.ncount = sv.ncount.get();
+    f.pmh = nullptr;
     Bdy b {};
     if (bdy && bdy->nb) {
         b.g = bdy->view();
@@ -749,12 +892,18 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     uint32_t iters = 0;
     bool converged = true;
 
-    dispatch(P.kernel, grid.geom.range, [&](auto KC, auto RC) {
+    const bool mixed = P.precision == REYN_PRECISION_MIXED;
+    uint2* PMH = mixed ? sv.pmh.get() : nullptr;
+    uint2* VH = mixed ? sv.velh.get() : nullptr;
+    uint2* VH2 = mixed ? sv.velh2.get() : nullptr;
+    f.pmh = PMH;
+    auto body = [&](auto KC, auto RC, auto MC) {
         constexpr int K = decltype(KC)::value;
         constexpr int R = decltype(RC)::value;
+        constexpr bool MIX = decltype(MC)::value;
         REYN_KERNEL("k_density", s,
-            k_density<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, b, sv.rho.get(), st.vel.get(),
-            sv.bterm.get()));
+            k_density<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, b, sv.rho.get(), st.vel.get(),
+            sv.bterm.get(), PMH, VH));
         if (sv.scheme == REYN_SESPH) {
             REYN_KERNEL("k_sesph", s,
                 k_sesph<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), sv.bterm.get(),
@@ -763,8 +912,8 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         } else if (sv.scheme == REYN_PCISPH) {
             const float kp = (float)((sv.pcisph_delta / dt) / dt); // PCISPH.cu:65
             REYN_KERNEL("k_nonpressure", s,
-                k_nonpressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), nu10, eps, grav,
-                dt, sv.acc.get(), sv.vel2.get()));
+                k_nonpressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), nullptr, nu10,
+                eps, grav, dt, sv.acc.get(), sv.vel2.get(), nullptr));
             float4* v = sv.vel2.get();
             for (;;) {
                 SweepStats* slot = slots + (iters % 64);
@@ -796,24 +945,24 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 VX, VY, VZ));
         } else { // IISPH
             REYN_KERNEL("k_nonpressure", s,
-                k_nonpressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), nu10, eps, grav,
-                dt, sv.acc.get(), sv.vel2.get()));
+                k_nonpressure<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), VH, nu10,
+                eps, grav, dt, sv.acc.get(), sv.vel2.get(), VH2));
             const float tiny = tiny_threshold();
             auto pacc = [&] {
                 REYN_KERNEL("k_iisph_pacc", s,
-                    k_iisph_pacc<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(),
+                    k_iisph_pacc<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(),
                     sv.bterm.get(), r0i, sv.acc.get()));
             };
             if (P.warmstart) {
                 REYN_KERNEL("k_iisph_diag_pacc", s,
-                    k_iisph_diag_pacc<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
-                    sv.bterm.get(), rho0, dt, r0i, sv.p.get(), sv.aii.get(), sv.sii.get(),
+                    k_iisph_diag_pacc<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
+                    VH2, sv.bterm.get(), rho0, dt, r0i, sv.p.get(), sv.aii.get(), sv.sii.get(),
                     sv.p_tmp.get(), sv.acc.get()));
                 sv.p.swap(sv.p_tmp);
             } else {
                 REYN_KERNEL("k_iisph_diag", s,
-                    k_iisph_diag<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
-                    sv.bterm.get(), rho0, dt, P.omega, P.warmstart, tiny, sv.aii.get(),
+                    k_iisph_diag<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
+                    VH2, sv.bterm.get(), rho0, dt, P.omega, P.warmstart, tiny, sv.aii.get(),
                     sv.sii.get(), sv.p.get()));
                 pacc();
             }
@@ -824,7 +973,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 SweepStats* slot = slots + (iters % 64);
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats), s));
                 REYN_KERNEL("k_iisph_jacobi", s,
-                    k_iisph_jacobi<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.acc.get(),
+                    k_iisph_jacobi<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.acc.get(),
                     sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, tiny,
                     thr, slot));
                 iters += 1;
@@ -848,9 +997,15 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 pacc();
             }
             REYN_KERNEL("k_iisph_final", s,
-                k_iisph_final<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
+                k_iisph_final<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
                 r0i, sv.vel2.get(), dt, sv.acc.get(), X, Y, Z, VX, VY, VZ));
         }
+    };
+    dispatch(P.kernel, grid.geom.range, [&](auto KC, auto RC) {
+        if (mixed)
+            body(KC, RC, std::true_type {});
+        else
+            body(KC, RC, std::false_type {});
     });
     REYN_KERNEL("k_unpack_acc", s,
         k_unpack_acc<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, sv.acc.get(), sv.ax.get(),

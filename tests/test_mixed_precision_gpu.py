@@ -1,0 +1,101 @@
+"""The mixed-precision IISPH solver (neighbour positions stored cell-relative
+in FP16, neighbour velocities in FP16, FP32 arithmetic) against the FP64
+restatement of the step, beside the FP32 solver on the same inputs.
+
+Both solvers run a fixed number of Jacobi sweeps (min_iter = max_iter, a
+criterion every sweep meets), so that all three carry out the same
+arithmetic; the errors are stated per quantity relative to the field's
+largest magnitude. Bounds: FP16 offsets round to 2^-12 cells, velocities to
+2^-11 relative, which puts the mixed solver's pressure and velocity errors at
+about 1e-3 of their scale, and its position and density errors (dt^2 and
+dt^3 behind) far below; the average density error must stay far below the
+0.1 % convergence tolerance it is run at.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import fp64
+from reyn_b200 import scenes
+from tests.helpers import by_id, run_engine
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("x", "y", "z", "vx", "vy", "vz", "rho", "p", "aii", "sii")
+# per-quantity bound of the mixed solver's error against FP64 (relative to the
+# field's largest magnitude)
+MIXED_TOL = {"x": 1e-5, "y": 1e-5, "z": 1e-5, "vx": 5e-3, "vy": 5e-3, "vz": 5e-3,
+             "rho": 1e-5, "p": 2e-2, "aii": 5e-3, "sii": 2e-2}
+
+
+def _fixed_params(kind, h, rho0, precision, sweeps=4):
+    import reyn_b200 as rb
+    prm = rb.reference_params(rb.IISPH, kind, h, rho0, 0.01)
+    prm.min_iter = prm.max_iter = sweeps
+    prm.eta = 1.0  # met after every sweep: exactly `sweeps` sweeps
+    prm.precision = precision
+    return prm
+
+
+def _errors(got, want_in_input_order, ids_in):
+    g = by_id({k: v for k, v in got.items() if k != "iters"}, got["id"])
+    order = np.argsort(np.asarray(ids_in).astype(np.int64))
+    w = {k: v[order] for k, v in want_in_input_order.items()}
+    err = {k: float(np.abs(g[k] - w[k]).max() / np.abs(w[k]).max()) for k in FIELDS}
+    err["avg_rho_rel"] = float(np.mean(np.abs(g["rho"] - w["rho"])) / 1000.0)
+    return err
+
+
+def _both_vs_fp64(kind, sc, bdy, h, cell_ratio, steps, dt):
+    """errors of the FP32 and the mixed solver against FP64, same inputs"""
+    import reyn_b200 as rb
+    errs = {}
+    for name, prec in (("fp32", rb.PRECISION_FP32), ("mixed", rb.PRECISION_MIXED)):
+        prm = _fixed_params(kind, h, sc.rho0, prec)
+        got = run_engine(2, kind, sc.fluid, bdy, sc.box_min, sc.box_max, h, sc.rho0, 0.01,
+                         dt, steps, params=prm, cell_ratio=cell_ratio)
+        assert got["iters"] == [4] * steps
+        if name == "fp32":
+            want = fp64.iisph_run(kind, sc.fluid, bdy, sc.box_min, sc.box_max, h, sc.rho0,
+                                  0.01, tuple(prm.g), dt, steps, 4, prm.omega,
+                                  bool(prm.warmstart))
+        errs[name] = _errors(got, want, sc.fluid["id"])
+    print(f"kernel {kind} h {h:.4g} cell ratio {cell_ratio}:",
+          {k: f"fp32 {errs['fp32'][k]:.2e} mixed {errs['mixed'][k]:.2e}" for k in errs["fp32"]})
+    return errs
+
+
+@pytest.mark.parametrize("kind", [0, 2])
+def test_mixed_vs_fp64_beside_fp32(cuda, kind):
+    import reyn_b200 as rb
+    sc = scenes.dam_break((20, 18, 16), 0.02, (0.6, 0.6, 0.6), velocity_noise=0.05, seed=5)
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    bdy = dict(sc.bdy, m=bm)
+    errs = _both_vs_fp64(kind, sc, bdy, sc.h, 0.5, steps=3, dt=1e-3)
+    for k, t in MIXED_TOL.items():
+        assert errs["mixed"][k] <= t, (k, errs["mixed"][k], errs["fp32"][k])
+    assert errs["mixed"]["avg_rho_rel"] <= 1e-5
+
+
+def test_mixed_with_list_overflow_and_unit_cells(cuda):
+    """A compressed block (spacing 0.6 h: about 150 neighbours, past the
+    64-entry list) sends the interior particles to the FP32 cell traversal
+    while the corners keep their lists, and cell size = support radius (cell
+    delta within +-1) exercises the other encoding range; both agree with the
+    FP32 solver within the mixed solver's bounds."""
+    import reyn_b200 as rb
+    sc = scenes.dam_break((16, 14, 12), 0.02, (0.6, 0.6, 0.6), velocity_noise=0.05, seed=9)
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    bdy = dict(sc.bdy, m=bm)
+    for h, ratio in ((sc.h / 0.6, 0.5), (sc.h, 1.0)):
+        errs = _both_vs_fp64(0, sc, bdy, h, ratio, steps=2, dt=5e-4)
+        for k, t in MIXED_TOL.items():
+            assert errs["mixed"][k] <= t, (ratio, k, errs["mixed"][k], errs["fp32"][k])
+
+
+def test_mixed_requires_iisph(cuda):
+    import reyn_b200 as rb
+    prm = rb.reference_params(rb.PCISPH, rb.C2, 0.02, 1000.0, 0.01)
+    prm.precision = rb.PRECISION_MIXED
+    with pytest.raises(rb.ReynError):
+        rb.Solver(rb.PCISPH, prm, 100)
