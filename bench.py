@@ -12,8 +12,9 @@ state, IISPH step, hard bounds. Inputs are resident in HBM for `value`; `e2e`
 repeats the step through the C ABI with the state uploaded from and downloaded
 to pinned host memory inside the timed region.
 
-The headline is the mixed-precision solver (neighbour positions cell-relative
-FP16, neighbour velocities FP16, FP32 arithmetic, FP64 convergence reduction);
+The headline is the mixed-precision solver (neighbour positions as 16-bit
+fixed point, neighbour masses, velocities and pressure accelerations FP16,
+FP32 arithmetic, FP64 convergence reduction);
 by default the plain FP32 solver is timed first on the same scene and reported
 beside it ("fp32", "mixed_over_fp32").
 
@@ -74,6 +75,8 @@ def parse_args():
                     help="divide the lattice by this factor per axis (testing only)")
     ap.add_argument("--precision", choices=["both", "mixed", "fp32"], default="both",
                     help="both: time the FP32 path, then report the mixed path beside it")
+    ap.add_argument("--order", choices=["xyz", "zorder"], default="xyz",
+                    help="cell order of the grid the state is sorted by")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -198,7 +201,7 @@ class EngineRun:
     """The workload on the engine: one scene, its grid, boundary and solver,
     and the main-loop step (main.cu:64-75)."""
 
-    def __init__(self, rank: int, scale: int, dev, precision: str):
+    def __init__(self, rank: int, scale: int, dev, precision: str, order: str = "xyz"):
         import torch
 
         import reyn_b200 as rb
@@ -211,7 +214,8 @@ class EngineRun:
         self.st.upload(sc.fluid)
         self.bd = rb.Boundary(*(torch.tensor(sc.bdy[k], device=dev) for k in ("x", "y", "z")),
                               None, h=sc.h, rho0=sc.rho0, mass_iters=5)
-        self.grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h)
+        self.grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h, 0.5,
+                            rb.ORDER_ZORDER if order == "zorder" else rb.ORDER_XYZ)
         prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, NU)
         prm.convergence = rb.CONV_AVERAGE
         prm.eta = 0.001
@@ -312,7 +316,7 @@ def run_engine(a, world, rank, local):
     # the plain FP32 path first, on the same scene, as the comparison leg
     fp32 = None
     if a.precision == "both":
-        run = EngineRun(rank, a.scale, dev, "fp32")
+        run = EngineRun(rank, a.scale, dev, "fp32", a.order)
         _, _, ms32, _, clk32, log32 = timed_steps(run, a, world, stream, dev)
         fp32 = leg_summary(run, a, world, ms32, log32)
         fp32["clocks"] = clk32
@@ -320,7 +324,7 @@ def run_engine(a, world, rank, local):
         torch.cuda.synchronize()
 
     headline = "fp32" if a.precision == "fp32" else "mixed"
-    run = EngineRun(rank, a.scale, dev, headline)
+    run = EngineRun(rank, a.scale, dev, headline, a.order)
     n = run.n
     ck, ms, ms_max, prof, ck_clocks, log = timed_steps(run, a, world, stream, dev)
     value = world * n * a.steps / (ms_max / 1e3)
@@ -375,8 +379,9 @@ def run_engine(a, world, rank, local):
         cpu = cpu_baseline_from(ck, run)
 
     precision = ("fp32 storage and math" if headline == "fp32" else
-                 "mixed: neighbour positions cell-relative FP16, neighbour velocities FP16, "
-                 "own data and all arithmetic FP32, FP64 convergence reduction")
+                 "mixed: neighbour positions 16-bit fixed point (1/16384 cell), neighbour "
+                 "masses, velocities and pressure accelerations FP16, own data and all "
+                 "arithmetic FP32, FP64 convergence reduction")
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 3),
@@ -388,7 +393,8 @@ def run_engine(a, world, rank, local):
                    "convergence": "avg density error <= 0.1% (FP64 reduction)",
                    "dt": f"min(simple_dt_controller(lambda={LAMBDA}, target 10 iters, "
                          f"0.1%/step) from {DT0}, 0.08 h^2/nu = {run.dt_visc:.2e})",
-                   "precision": precision, "parallelism": f"replicas{world}",
+                   "precision": precision, "cell_order": a.order,
+                   "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (state 4M x 28 B + grid 70 MB per step)"},
         "clocks": ck_clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
         "cpu_baseline": cpu,

@@ -89,13 +89,20 @@ int reyn_particles_download(reyn_particles* p, float* xx, float* xy,
 typedef struct reyn_grid reyn_grid;
 
 typedef enum reyn_cell_order {
-    REYN_ORDER_XYZ = 0 /* z*nx*ny + y*nx + x, uniformgrid.cuh:33-40 */
+    REYN_ORDER_XYZ = 0, /* z*nx*ny + y*nx + x, uniformgrid.cuh:33-40 */
+    /* (no counterpart in the reference) Z-order: cells grouped into bricks
+     * of 4x4x4 (x fastest inside a brick), bricks along the Morton curve
+     * inside tiles of 32x32x32 cells, tiles in XYZ order. A reorder then
+     * places particles that are close in space close in memory in all three
+     * directions. Keys run over the tiles covering the grid, so prefix has
+     * n_keys + 1 entries, n_keys >= nx*ny*nz. */
+    REYN_ORDER_ZORDER = 1
 } reyn_cell_order;
 
 /* Device-usable description of a built grid: UniformGrid<R>
  * (uniformgrid.cuh:84-179). `sorted` is NULL after construct_and_reorder
- * (Resort::yes: particle arrays are in grid order). prefix has
- * nx*ny*nz + 1 entries (the last equals n). */
+ * (Resort::yes: particle arrays are in grid order). prefix has n_keys + 1
+ * entries (the last equals n); n_keys = nx*ny*nz in XYZ order. */
 typedef struct reyn_grid_info {
     float bound_min[3]; /* lower bound INCLUDING the 2r safety margin */
     float cell_size;
@@ -105,6 +112,8 @@ typedef struct reyn_grid_info {
     uint32_t n;         /* particles indexed by the last construct */
     const uint32_t* prefix;
     const uint32_t* sorted;
+    int32_t order;      /* reyn_cell_order */
+    uint32_t n_keys;    /* cell keys (prefix has n_keys + 1 entries) */
 } reyn_grid_info;
 
 /* UniformGridBuilder(bound_min, bound_max, search_radius) (uniformgrid.cu:
@@ -202,10 +211,10 @@ typedef enum reyn_convergence {
 typedef enum reyn_precision {
     /* FP32 storage and arithmetic, as the reference */
     REYN_PRECISION_FP32 = 0,
-    /* IISPH only: neighbour positions stored as FP16 offsets within their
-     * grid cell and neighbour velocities/densities as FP16; the particle's
-     * own data and all arithmetic stay FP32, the convergence reduction FP64.
-     * Up to 2^25 particles. */
+    /* IISPH only: neighbour positions stored as 16-bit fixed point relative
+     * to the grid (1/16384 cell), neighbour masses, velocities, densities and
+     * pressure accelerations as FP16; the particle's own data and all
+     * arithmetic stay FP32, the convergence reduction FP64. */
     REYN_PRECISION_MIXED = 1
 } reyn_precision;
 

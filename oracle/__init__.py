@@ -58,11 +58,16 @@ class Geom(ctypes.Structure):
         ("ny", ctypes.c_int32),
         ("nz", ctypes.c_int32),
         ("range", ctypes.c_int32),
+        ("order", ctypes.c_int32),
     ]
 
     @property
     def n_cells(self) -> int:
         return self.nx * self.ny * self.nz
+
+    @property
+    def n_keys(self) -> int:
+        return int(lib().orc_keys(ctypes.byref(self)))
 
 
 class Params(ctypes.Structure):
@@ -92,6 +97,10 @@ def lib():
             build()
         L = ctypes.CDLL(LIB_PATH)
         L.orc_geometry.argtypes = [_f32p, _f32p, ctypes.c_float, ctypes.c_float, ctypes.POINTER(Geom)]
+        L.orc_geometry_order.argtypes = [_f32p, _f32p, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                         ctypes.POINTER(Geom)]
+        L.orc_keys.argtypes = [ctypes.POINTER(Geom)]
+        L.orc_keys.restype = ctypes.c_int64
         L.orc_kernel_eval.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_uint32] + [_f32p] * 7
         L.orc_grid_build.argtypes = [ctypes.POINTER(Geom), ctypes.c_uint32, _f32p, _f32p, _f32p,
                                      _u32p, _u32p, ctypes.c_void_p]
@@ -130,9 +139,9 @@ def f32(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
-def geometry(bmin, bmax, r: float, cell_ratio: float = 0.5) -> Geom:
+def geometry(bmin, bmax, r: float, cell_ratio: float = 0.5, order: int = 0) -> Geom:
     g = Geom()
-    rc = lib().orc_geometry(f32(bmin), f32(bmax), r, cell_ratio, ctypes.byref(g))
+    rc = lib().orc_geometry_order(f32(bmin), f32(bmax), r, cell_ratio, order, ctypes.byref(g))
     if rc:
         raise ValueError(f"orc_geometry failed ({rc})")
     return g
@@ -151,7 +160,7 @@ def kernel_eval(kind: int, h_bar: float, dx, dy, dz):
 def grid_build(g: Geom, x, y, z):
     x, y, z = f32(x), f32(y), f32(z)
     n = x.size
-    prefix = np.zeros(g.n_cells + 1, np.uint32)
+    prefix = np.zeros(g.n_keys + 1, np.uint32)
     sorted_ = np.zeros(max(n, 1), np.uint32)
     keys = np.zeros(max(n, 1), np.uint32)
     rc = lib().orc_grid_build(ctypes.byref(g), n, x, y, z, prefix, sorted_, _vp(keys))

@@ -181,6 +181,40 @@ inline int cell_coord(float p, float lo, float cell)
     return (int)std::floor((p - lo) / cell); // floor_div, vector.cuh:137-141
 }
 
+// The engine's Z-order (no counterpart in the reference): 4x4x4-cell
+// bricks, x fastest inside a brick; bricks numbered along the Morton curve
+// inside 32x32x32-cell tiles (bit k of the brick's x, y, z index goes to bit
+// 3k, 3k+1, 3k+2); tiles in XYZ order. key = (tile * 512 + brick) * 64 + cell.
+inline int ztiles(int n) { return (n + 31) / 32; }
+
+inline int64_t zorder_key(const orc_geom& g, int cx, int cy, int cz)
+{
+    const int64_t tx = ztiles(g.nx), ty = ztiles(g.ny);
+    const int64_t tile = ((int64_t)(cz / 32) * ty + cy / 32) * tx + cx / 32;
+    int64_t brick = 0;
+    const int b[3] = { (cx / 4) % 8, (cy / 4) % 8, (cz / 4) % 8 };
+    for (int bit = 0; bit < 3; ++bit)
+        for (int a = 0; a < 3; ++a)
+            brick |= (int64_t)((b[a] >> bit) & 1) << (3 * bit + a);
+    const int64_t cell = (cx % 4) + 4 * (cy % 4) + 16 * (cz % 4);
+    return (tile * 512 + brick) * 64 + cell;
+}
+
+inline int64_t cell_key(const orc_geom& g, int cx, int cy, int cz)
+{
+    if (g.order == 1)
+        return zorder_key(g, cx, cy, cz);
+    // _linearize, uniformgrid.cuh:33-40
+    return (int64_t)cz * ((int64_t)g.nx * g.ny) + ((int64_t)cy * g.nx + cx);
+}
+
+inline int64_t n_keys(const orc_geom& g)
+{
+    if (g.order == 1)
+        return (int64_t)ztiles(g.nx) * ztiles(g.ny) * ztiles(g.nz) * 32768;
+    return (int64_t)g.nx * g.ny * g.nz;
+}
+
 inline int64_t linear_key(const orc_geom& g, float x, float y, float z)
 {
     const int cx = cell_coord(x, g.bmin[0], g.cell);
@@ -188,15 +222,14 @@ inline int64_t linear_key(const orc_geom& g, float x, float y, float z)
     const int cz = cell_coord(z, g.bmin[2], g.cell);
     if (cx < 0 || cy < 0 || cz < 0 || cx >= g.nx || cy >= g.ny || cz >= g.nz)
         return -1;
-    // _linearize, uniformgrid.cuh:33-40
-    return (int64_t)cz * ((int64_t)g.nx * g.ny) + ((int64_t)cy * g.nx + cx);
+    return cell_key(g, cx, cy, cz);
 }
 
 int build(const orc_geom& g, uint32_t n, const float* x, const float* y,
     const float* z, Grid& out, uint32_t* keys_out)
 {
     out.g = g;
-    const int64_t C = (int64_t)g.nx * g.ny * g.nz;
+    const int64_t C = n_keys(g);
     std::vector<uint32_t> keys(n);
     int bad = 0;
 #pragma omp parallel for schedule(static) reduction(+ : bad)
@@ -237,17 +270,25 @@ inline Acc ff_nbrs(const Grid& G, f3 xi, const float* x, const float* y,
     const int cz = cell_coord(xi.z, g.bmin[2], g.cell);
     const int R = g.range;
     const int64_t nxny = (int64_t)g.nx * g.ny;
+    auto visit = [&](int64_t k0, int64_t k1) {
+        for (uint32_t j = G.prefix[k0]; j < G.prefix[k1]; ++j) {
+            const uint32_t sj = G.identity ? j : G.sorted[j];
+            const f3 xij = xi - load(sj, x, y, z);
+            const float l2 = dot(xij, xij);
+            if (l2 <= g.r2)
+                acc += map(sj, xij, l2);
+        }
+    };
     for (int zz = cz - R; zz <= cz + R; ++zz)
         for (int yy = cy - R; yy <= cy + R; ++yy) {
-            const int64_t cid = (int64_t)zz * nxny + ((int64_t)yy * g.nx + (cx - R));
-            const uint32_t start = G.prefix[cid];
-            const uint32_t end = G.prefix[cid + (2 * R + 1)];
-            for (uint32_t j = start; j < end; ++j) {
-                const uint32_t sj = G.identity ? j : G.sorted[j];
-                const f3 xij = xi - load(sj, x, y, z);
-                const float l2 = dot(xij, xij);
-                if (l2 <= g.r2)
-                    acc += map(sj, xij, l2);
+            if (g.order == 1) { // Z-order: cell by cell
+                for (int xx = cx - R; xx <= cx + R; ++xx) {
+                    const int64_t k = zorder_key(g, xx, yy, zz);
+                    visit(k, k + 1);
+                }
+            } else {
+                const int64_t cid = (int64_t)zz * nxny + ((int64_t)yy * g.nx + (cx - R));
+                visit(cid, cid + (2 * R + 1));
             }
         }
     return acc;
@@ -661,8 +702,22 @@ int orc_geometry(const float bmin[3], const float bmax[3], float r,
     g->ny = n[1];
     g->nz = n[2];
     g->range = cell_ratio == 0.5f ? 2 : 1;
+    g->order = 0;
     return 0;
 }
+
+int orc_geometry_order(const float bmin[3], const float bmax[3], float r,
+    float cell_ratio, int order, orc_geom* g)
+{
+    if (order != 0 && order != 1)
+        return -1;
+    if (int e = orc_geometry(bmin, bmax, r, cell_ratio, g))
+        return e;
+    g->order = order;
+    return 0;
+}
+
+int64_t orc_keys(const orc_geom* g) { return n_keys(*g); }
 
 int orc_kernel_eval(int kind, float h_bar, uint32_t n, const float* dx,
     const float* dy, const float* dz, float* w, float* gx, float* gy,
@@ -699,7 +754,7 @@ int orc_neighbours(const orc_geom* g, uint32_t n, const float* x,
 {
     Grid G;
     G.g = *g;
-    const int64_t C = (int64_t)g->nx * g->ny * g->nz;
+    const int64_t C = n_keys(*g);
     G.prefix.assign(prefix, prefix + C + 1);
     G.sorted.assign(sorted, sorted + n);
     const float r2 = g->r2;

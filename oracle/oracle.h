@@ -30,10 +30,16 @@ typedef struct orc_geom {
     float r2;      /* squared search radius */
     int32_t nx, ny, nz;
     int32_t range; /* cells searched on each side: 2 at cell r/2, 1 at r */
+    int32_t order; /* 0: XYZ keys (the reference's); 1: the engine's Z-order */
 } orc_geom;
 
 int orc_geometry(const float bmin[3], const float bmax[3], float r,
     float cell_ratio, orc_geom* g);
+/* the same geometry with cell order `order`; orc_keys() gives the size of
+ * its key space (prefix arrays hold orc_keys + 1 entries) */
+int orc_geometry_order(const float bmin[3], const float bmax[3], float r,
+    float cell_ratio, int order, orc_geom* g);
+int64_t orc_keys(const orc_geom* g);
 
 /* W(dx) and ∇W(dx) of kernel `kind` (0 C2, 1 B3, 2 W6, 3 COS) with support
  * h_bar, kernels.cuh:19-165 (host flavour: norm = sqrt(dot)). */
@@ -42,7 +48,7 @@ int orc_kernel_eval(int kind, float h_bar, uint32_t n, const float* dx,
     float* gz);
 
 /* counting-sort grid build (uniformgrid.cu:20-63, 98-143), stable within a
- * cell. prefix: nx*ny*nz + 1 entries (exclusive scan, last = N);
+ * cell. prefix: orc_keys + 1 entries (exclusive scan, last = N);
  * sorted: N particle indices; keys (optional): N cell keys. */
 int orc_grid_build(const orc_geom* g, uint32_t n, const float* x,
     const float* y, const float* z, uint32_t* prefix, uint32_t* sorted,

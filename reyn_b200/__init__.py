@@ -24,6 +24,7 @@ KERNELS = {"C2": C2, "B3": B3, "W6": W6, "COS": COS}
 SESPH, PCISPH, IISPH = 0, 1, 2
 CONV_REFERENCE, CONV_AVERAGE = 0, 1
 PRECISION_FP32, PRECISION_MIXED = 0, 1
+ORDER_XYZ, ORDER_ZORDER = 0, 1
 
 OK = 0
 ERR_INVALID, ERR_OUT_OF_BOUNDS, ERR_NONFINITE, ERR_ITER_LIMIT = -1, -2, -3, -4
@@ -48,7 +49,8 @@ class Soa(ctypes.Structure):
 class GridInfo(ctypes.Structure):
     _fields_ = [("bound_min", _f * 3), ("cell_size", _f), ("r_c_2", _f), ("nx", ctypes.c_int32),
                 ("ny", ctypes.c_int32), ("nz", ctypes.c_int32), ("nxny", ctypes.c_int32),
-                ("range", ctypes.c_int32), ("n", _u32), ("prefix", _vp), ("sorted", _vp)]
+                ("range", ctypes.c_int32), ("n", _u32), ("prefix", _vp), ("sorted", _vp),
+                ("order", ctypes.c_int32), ("n_keys", _u32)]
 
 
 class Params(ctypes.Structure):
@@ -214,9 +216,10 @@ class Particles:
 class Grid:
     """UniformGridBuilder (reference uniformgrid.cuh:200-489)."""
 
-    def __init__(self, bmin, bmax, search_radius: float, cell_ratio: float = 0.5):
+    def __init__(self, bmin, bmax, search_radius: float, cell_ratio: float = 0.5,
+                 order: int = 0):
         h = _vp()
-        check(lib().reyn_grid_create(_f3(bmin), _f3(bmax), search_radius, cell_ratio, 0,
+        check(lib().reyn_grid_create(_f3(bmin), _f3(bmax), search_radius, cell_ratio, order,
                                      ctypes.byref(h)))
         self.h = h
         self.r = search_radius

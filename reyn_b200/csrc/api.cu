@@ -145,11 +145,11 @@ int reyn_grid_create(const float bound_min[3], const float bound_max[3], float s
         *out = nullptr;
         check_vec3(bound_min, "bound_min must be 3 finite floats");
         check_vec3(bound_max, "bound_max must be 3 finite floats");
-        require(order == REYN_ORDER_XYZ, "unknown cell order");
+        require(order == REYN_ORDER_XYZ || order == REYN_ORDER_ZORDER, "unknown cell order");
         auto g = std::make_unique<reyn_grid>();
-        g->geom = make_geom(bound_min, bound_max, search_radius, cell_ratio);
+        g->geom = make_geom(bound_min, bound_max, search_radius, cell_ratio, order);
         g->ratio = cell_ratio;
-        const size_t C = size_t(g->geom.cells());
+        const size_t C = size_t(g->geom.keys());
         g->counts.resize(C);
         REYN_CUDA(cudaMemset(g->counts.get(), 0, C * sizeof(uint32_t)));
         g->prefix.resize(C + 1);
@@ -214,6 +214,8 @@ int reyn_grid_info_get(const reyn_grid* g, reyn_grid_info* out)
         out->n = g->n;
         out->prefix = g->prefix.get();
         out->sorted = g->reordered ? nullptr : g->sorted.get();
+        out->order = g->geom.order;
+        out->n_keys = uint32_t(g->geom.keys());
     });
 }
 
@@ -314,8 +316,6 @@ int reyn_solver_create(reyn_scheme scheme, const reyn_params* params, uint32_t n
         require(out != nullptr, "null output handle");
         *out = nullptr;
         check_params(scheme, params);
-        require(params->precision == REYN_PRECISION_FP32 || n <= (1u << 25),
-            "mixed precision handles at most 2^25 particles");
         auto s = std::make_unique<reyn_solver>();
         s->scheme = scheme;
         s->prm = *params;

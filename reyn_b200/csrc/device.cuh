@@ -8,6 +8,8 @@
 #include <cmath>
 #include <cstdint>
 
+#include "reyn_b200.h"
+
 namespace reyn {
 
 // ---- smoothing kernels ----------------------------------------------------
@@ -151,15 +153,47 @@ __device__ __forceinline__ void pair_wg(
 // ---- uniform grid view ----------------------------------------------------
 // The device POD of a built grid, UniformGrid<Resort::yes>
 // (uniformgrid.cuh:84-97): lower bound (with margin), cell size, r^2, cell
-// counts and the prefix over all cells (C + 1 entries).
+// counts and the prefix over all cell keys (keys + 1 entries).
 struct GridView {
     float lox, loy, loz;
     float cell;
     float inv_cell; // 1 / cell, for the strip trimming only (never for keys)
     float r2;
     int nx, ny, nz, nxny;
+    int order;      // REYN_ORDER_XYZ or REYN_ORDER_ZORDER
+    int tx, txy;    // Z-order: 32-cell tiles along x, per xy layer
     const uint32_t* __restrict__ prefix;
 };
+
+// Z-order cell keys: cells are grouped into bricks of 4x4x4 (x fastest
+// inside a brick, so x-runs of up to 4 cells stay contiguous), bricks follow
+// the Morton curve inside tiles of 8x8x8 bricks (32^3 cells), and tiles are
+// in XYZ order. Consecutive particles in this order fill compact 3-D blocks.
+constexpr int ZTILE = 32;
+
+__host__ __device__ __forceinline__ uint32_t spread3(uint32_t v) // 3 bits -> bits 0, 3, 6
+{
+    return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4);
+}
+
+__host__ __device__ __forceinline__ uint32_t zorder_key(int tx, int txy, int cx, int cy, int cz)
+{
+    const uint32_t tile = uint32_t(cz >> 5) * uint32_t(txy) + uint32_t(cy >> 5) * uint32_t(tx)
+        + uint32_t(cx >> 5);
+    const uint32_t brick = spread3(uint32_t(cx >> 2) & 7u) | (spread3(uint32_t(cy >> 2) & 7u) << 1)
+        | (spread3(uint32_t(cz >> 2) & 7u) << 2);
+    const uint32_t local = uint32_t(cx & 3) | (uint32_t(cy & 3) << 2) | (uint32_t(cz & 3) << 4);
+    return (((tile << 9) | brick) << 6) | local;
+}
+
+// the key of cell (cx, cy, cz) in the grid's cell order (_linearize,
+// uniformgrid.cuh:33-40, for XYZ)
+__device__ __forceinline__ uint32_t cell_key(const GridView& g, int cx, int cy, int cz)
+{
+    if (g.order == REYN_ORDER_ZORDER)
+        return zorder_key(g.tx, g.txy, cx, cy, cz);
+    return (uint32_t)cz * (uint32_t)g.nxny + ((uint32_t)cy * (uint32_t)g.nx + (uint32_t)cx);
+}
 
 // _index3 (uniformgrid.cuh:17-22): floor((x - min) / cell), IEEE division so
 // that keys agree with the reference bit for bit
@@ -181,62 +215,86 @@ __device__ __forceinline__ int3 clamp_cell(const GridView& g, int3 c, int R)
         min(max(c.z, R), g.nz - 1 - R));
 }
 
-// Fixed-radius neighbour traversal (the role of UniformGrid::ff_nbrs,
-// uniformgrid.cuh:113-178): (2R+1)^2 rows of cells, each a contiguous run of
-// 2R+1 x-cells in the sorted arrays bounded by two prefix entries. `pts` are
-// packed (x, y, z, mass) in grid order; f(j, pts[j], dx, dy, dz, l2) is
-// called for every candidate with l2 <= r^2 (self included, as the
-// reference's accumulation does), in the reference's row order.
+// The rows of the fixed-radius traversal (the role of UniformGrid::ff_nbrs,
+// uniformgrid.cuh:113-178): (2R+1)^2 rows of cells, each a run of x-cells,
+// visited in the reference's order (z, then y). run(k0, ncell) gets the key
+// of a run's first cell and its length: the run's particles are the sorted
+// range prefix[k0] .. prefix[k0 + ncell]. In XYZ order every row is one run;
+// in Z-order a row that crosses a brick boundary is two.
 //
 // Each row is trimmed to the part the search sphere can reach: rows whose
 // (y, z) distance from the point exceeds r are skipped, and the x-run is cut
 // to the cells overlapping the sphere's chord at that distance. The trimming
 // is conservative by a margin of 1e-3 cells, so exactly the candidates within
 // r are still visited, in the same order; only provably empty cells are
-// skipped.
-template <int R, class F>
-__device__ __forceinline__ void for_each_neighbour(const GridView& g, int3 c,
-    float xi, float yi, float zi, const float4* __restrict__ pts, F&& f)
+// skipped. Every operation is explicitly rounded (no contraction into FMAs),
+// so every kernel that walks the rows of a point gets the same runs.
+template <int R, class Run>
+__device__ __forceinline__ void for_each_row(const GridView& g, int3 c, float xi, float yi,
+    float zi, Run&& run)
 {
     constexpr float EPS = 1e-3f;
     // the point in cell units, relative to its own cell's lower corner
-    const float fx = (xi - g.lox) * g.inv_cell - (float)c.x;
-    const float fy = (yi - g.loy) * g.inv_cell - (float)c.y;
-    const float fz = (zi - g.loz) * g.inv_cell - (float)c.z;
-    const float rr = g.r2 * g.inv_cell * g.inv_cell * (1.f + EPS) + EPS;
+    const float fx = __fsub_rn(__fmul_rn(__fsub_rn(xi, g.lox), g.inv_cell), (float)c.x);
+    const float fy = __fsub_rn(__fmul_rn(__fsub_rn(yi, g.loy), g.inv_cell), (float)c.y);
+    const float fz = __fsub_rn(__fmul_rn(__fsub_rn(zi, g.loz), g.inv_cell), (float)c.z);
+    const float rr = __fadd_rn(
+        __fmul_rn(__fmul_rn(__fmul_rn(g.r2, g.inv_cell), g.inv_cell), 1.f + EPS), EPS);
 #pragma unroll 1
     for (int dz = -R; dz <= R; ++dz) {
         // distance (cells) from the point to the slab of cells at c.z + dz
-        const float gz = dz > 0 ? fmaxf((float)dz - fz, 0.f)
-                                : (dz < 0 ? fmaxf(fz - (float)(dz + 1), 0.f) : 0.f);
-        const float gz2 = gz * gz;
+        const float gz = dz > 0 ? fmaxf(__fsub_rn((float)dz, fz), 0.f)
+                                : (dz < 0 ? fmaxf(__fsub_rn(fz, (float)(dz + 1)), 0.f) : 0.f);
+        const float gz2 = __fmul_rn(gz, gz);
         if (gz2 > rr)
             continue;
         const int plane = (c.z + dz) * g.nxny;
 #pragma unroll 1
         for (int dy = -R; dy <= R; ++dy) {
-            const float gy = dy > 0 ? fmaxf((float)dy - fy, 0.f)
-                                    : (dy < 0 ? fmaxf(fy - (float)(dy + 1), 0.f) : 0.f);
-            const float d2 = gz2 + gy * gy;
+            const float gy = dy > 0 ? fmaxf(__fsub_rn((float)dy, fy), 0.f)
+                                    : (dy < 0 ? fmaxf(__fsub_rn(fy, (float)(dy + 1)), 0.f) : 0.f);
+            const float d2 = __fadd_rn(gz2, __fmul_rn(gy, gy));
             if (d2 > rr)
                 continue;
-            const float w = sqrtf(rr - d2) + EPS; // half chord, cells
-            const int x0 = max(-R, (int)floorf(fx - w));
-            const int x1 = min(R, (int)floorf(fx + w));
+            const float w = __fadd_rn(__fsqrt_rn(__fsub_rn(rr, d2)), EPS); // half chord, cells
+            const int x0 = max(-R, (int)floorf(__fsub_rn(fx, w)));
+            const int x1 = min(R, (int)floorf(__fadd_rn(fx, w)));
             if (x0 > x1) // only for points clamped into the grid from outside
                 continue;
-            const int cid = plane + (c.y + dy) * g.nx + c.x + x0;
-            const uint32_t s = __ldg(g.prefix + cid);
-            const uint32_t e = __ldg(g.prefix + cid + (x1 - x0 + 1));
-            for (uint32_t j = s; j < e; ++j) {
-                const float4 q = __ldg(pts + j);
-                const float dx = xi - q.x, dy_ = yi - q.y, dz_ = zi - q.z;
-                const float l2 = fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_));
-                if (l2 <= g.r2)
-                    f(j, q, dx, dy_, dz_, l2);
+            if (g.order == REYN_ORDER_ZORDER) {
+                const int xa = c.x + x0, xb = c.x + x1, y = c.y + dy, z = c.z + dz;
+                if ((xa >> 2) == (xb >> 2)) {
+                    run(zorder_key(g.tx, g.txy, xa, y, z), xb - xa + 1);
+                } else {
+                    run(zorder_key(g.tx, g.txy, xa, y, z), 4 - (xa & 3));
+                    run(zorder_key(g.tx, g.txy, xb & ~3, y, z), (xb & 3) + 1);
+                }
+            } else {
+                run(uint32_t(plane + (c.y + dy) * g.nx + c.x + x0), x1 - x0 + 1);
             }
         }
     }
+}
+
+// Fixed-radius neighbour traversal: f(j, pts[j], dx, dy, dz, l2) for every
+// candidate with l2 <= r^2 (self included, as the reference's accumulation
+// does), in the reference's row order. `pts` are packed (x, y, z, mass) in
+// grid order.
+template <int R, class F>
+__device__ __forceinline__ void for_each_neighbour(const GridView& g, int3 c,
+    float xi, float yi, float zi, const float4* __restrict__ pts, F&& f)
+{
+    for_each_row<R>(g, c, xi, yi, zi, [&](uint32_t k0, int ncell) {
+        const uint32_t s = __ldg(g.prefix + k0);
+        const uint32_t e = __ldg(g.prefix + k0 + ncell);
+        for (uint32_t j = s; j < e; ++j) {
+            const float4 q = __ldg(pts + j);
+            const float dx = xi - q.x, dy_ = yi - q.y, dz_ = zi - q.z;
+            const float l2 = fmaf(dx, dx, fmaf(dy_, dy_, dz_ * dz_));
+            if (l2 <= g.r2)
+                f(j, q, dx, dy_, dz_, l2);
+        }
+    });
 }
 
 // ---- reductions -------------------------------------------------------------

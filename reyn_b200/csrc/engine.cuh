@@ -28,10 +28,19 @@ struct GridGeom {
     float r;
     int n[3];
     int range; // 2 at ratio 0.5, 1 at ratio 1.0
+    int order = REYN_ORDER_XYZ;
+    int t[3] = { 0, 0, 0 }; // Z-order: tiles of ZTILE cells per axis
     int64_t cells() const { return int64_t(n[0]) * n[1] * n[2]; }
+    // the key space (the prefix covers keys() + 1 entries)
+    int64_t keys() const
+    {
+        return order == REYN_ORDER_ZORDER ? int64_t(t[0]) * t[1] * t[2] * ZTILE * ZTILE * ZTILE
+                                          : cells();
+    }
 };
 
-GridGeom make_geom(const float bmin[3], const float bmax[3], float r, float ratio);
+GridGeom make_geom(const float bmin[3], const float bmax[3], float r, float ratio,
+    int order = REYN_ORDER_XYZ);
 
 // The uniform grid over one set of positions.
 struct Grid {
@@ -97,7 +106,7 @@ struct reyn_solver {
     reyn::DevArray<float4> acc, vel2, bterm;
     reyn::DevArray<float> p_tmp;
     reyn::DevArray<uint32_t> nbr, ncount; // per-step neighbour list
-    reyn::DevArray<uint2> pmh, velh, velh2; // mixed-precision neighbour records
+    reyn::DevArray<uint2> pmh, acch, velh, velh2; // mixed-precision neighbour records
     reyn::DevArray<unsigned char> sweep_stats; // per-sweep reductions
     std::unique_ptr<reyn::PinnedArray<unsigned char>> readback;
     uint64_t p_epoch = 0;      // particle epoch p is ordered for

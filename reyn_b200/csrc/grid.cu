@@ -17,7 +17,7 @@ namespace reyn {
 
 // ---- geometry -------------------------------------------------------------
 
-GridGeom make_geom(const float bmin[3], const float bmax[3], float r, float ratio)
+GridGeom make_geom(const float bmin[3], const float bmax[3], float r, float ratio, int order)
 {
     require(r > 0.f && std::isfinite(r), "search radius must be positive and finite");
     require(ratio == 0.5f || ratio == 1.0f, "cell_ratio must be 0.5 or 1.0");
@@ -36,7 +36,11 @@ GridGeom make_geom(const float bmin[3], const float bmax[3], float r, float rati
         require(n > 0.f && n < 2.0e9f, "grid extent out of range");
         g.n[a] = (int)n;
     }
-    require(g.cells() < (int64_t(1) << 32) - 1, "grid has too many cells for 32-bit keys");
+    require(order == REYN_ORDER_XYZ || order == REYN_ORDER_ZORDER, "unknown cell order");
+    g.order = order;
+    for (int a = 0; a < 3; ++a)
+        g.t[a] = (g.n[a] + ZTILE - 1) / ZTILE;
+    require(g.keys() < (int64_t(1) << 32) - 1, "grid has too many cells for 32-bit keys");
     return g;
 }
 
@@ -53,6 +57,9 @@ GridView Grid::view(float search_radius) const
     v.ny = geom.n[1];
     v.nz = geom.n[2];
     v.nxny = geom.n[0] * geom.n[1];
+    v.order = geom.order;
+    v.tx = geom.t[0];
+    v.txy = geom.t[0] * geom.t[1];
     v.prefix = prefix.get();
     return v;
 }
@@ -87,7 +94,7 @@ __global__ void k_keys_count(uint32_t n, const float* __restrict__ x,
                              min(max(c.z, 0), g.nz - 1))
                        : make_int3(0, 0, 0);
         }
-        key = (uint32_t)c.z * (uint32_t)g.nxny + ((uint32_t)c.y * (uint32_t)g.nx + (uint32_t)c.x);
+        key = cell_key(g, c.x, c.y, c.z);
         keys[i] = key;
     }
     const unsigned group = __match_any_sync(0xffffffffu, key);
@@ -287,7 +294,7 @@ static void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& pa
 void Grid::build(const float* x, const float* y, const float* z, uint32_t np,
     cudaStream_t s)
 {
-    const int64_t C = geom.cells();
+    const int64_t C = geom.keys();
     if (counts.size() != size_t(C) || counts_dirty) {
         // the scatter returns every count to zero; only a fresh array or an
         // interrupted build needs clearing

@@ -49,20 +49,30 @@ struct Fluid {
     uint32_t* status;
     uint32_t* __restrict__ nbr;    // neighbour list (list_slot layout)
     uint32_t* __restrict__ ncount; // neighbours per particle
-    // mixed precision: per particle (ox, oy, oz, m / m_0) as four FP16, the
-    // offsets relative to the particle's cell in cell units, m_0 = pm[0].w
+    // mixed precision: per particle its position as three 16-bit wrapped
+    // fixed-point coordinates and m / m_0 as FP16, m_0 = pm[0].w; its
+    // pressure acceleration as FP16 (scaled by ACC_SCALE) for the Jacobi
+    // sweeps, and the FP32 accelerations for particles off the list
     const uint2* __restrict__ pmh;
+    const uint2* __restrict__ acch;
+    const float4* __restrict__ acc32;
 };
 
 // ---- mixed precision ----------------------------------------------------------
-// Neighbour data is stored as FP16 (positions relative to their cell,
-// velocities, density); the particle's own data and all arithmetic stay
-// FP32. x_ij = ((o_i - o_j) - (c_j - c_i)) * cell: the integer cell delta is
-// packed into the top 7 bits of the list entry (index in the low 25 bits),
-// the offsets o in [0, 1) are exact FP32 differences of FP16 values, so
-// x_ij carries at most 2^-11 cells of rounding.
-constexpr uint32_t IDX_BITS = 25;
-constexpr uint32_t IDX_MASK = (1u << IDX_BITS) - 1u;
+// Neighbour records are 8 bytes: each position coordinate as a 16-bit
+// wrapped fixed-point number, the position in cells modulo 4 at a resolution
+// of 1/16384 cell, and the mass relative to particle 0's as FP16; velocities,
+// densities and pressure accelerations of neighbours are FP16. The
+// particle's own data and all arithmetic stay FP32. Neighbours lie within 2
+// cells (r), so the 16-bit difference u_i - u_j, read as a signed number, is
+// the pair vector x_ij in units of 1/16384 cell exactly, with no cell index
+// stored: three subtractions and conversions per pair. (A coordinate
+// difference of exactly 2 cells reads as -2; such a pair lies on the
+// support's edge, where the kernel and its gradient vanish.) Both ends use
+// their quantised records, so x_ji = -x_ij holds exactly and pair forces stay
+// antisymmetric. The quantisation error is at most 1/32768 cell per
+// coordinate (FP16 offsets within a cell would round to 1/4096).
+constexpr float FIXQ = 16384.f;
 
 __device__ __forceinline__ float4 half4_to_float4(uint2 u)
 {
@@ -82,30 +92,60 @@ __device__ __forceinline__ uint2 float4_to_half4(float4 v)
     return u;
 }
 
-// cell (floor of the position in cell units) and offset within it; the
-// mixed path's own decomposition, consistent between writer and readers
-__device__ __forceinline__ void cell_offset(const GridView& g, float x, float y, float z,
-    int3& c, float3& o)
+// one coordinate: (cell index mod 4) * 16384 + the offset in the cell in
+// units of 1/16384, modulo 2^16 (an offset that rounds up to 16384 carries
+// into the cell index)
+__device__ __forceinline__ uint32_t fix_coord(float p, float lo, float inv_cell, int c)
 {
-    const float ux = (x - g.lox) * g.inv_cell, uy = (y - g.loy) * g.inv_cell,
-                uz = (z - g.loz) * g.inv_cell;
-    const float fx = floorf(ux), fy = floorf(uy), fz = floorf(uz);
-    c = make_int3((int)fx, (int)fy, (int)fz);
-    o = make_float3(ux - fx, uy - fy, uz - fz);
+    const float o = __saturatef(__fsub_rn(__fmul_rn(__fsub_rn(p, lo), inv_cell), (float)c));
+    return ((uint32_t(c) << 14) + __float2uint_rn(o * FIXQ)) & 0xffffu;
 }
 
-// c_j - c_i in [-2, 2]^3 (neighbours lie within two cells) <-> 0..124
-__device__ __forceinline__ uint32_t delta_code(int dx, int dy, int dz)
+// the record of a particle at (x, y, z) with mass ratio mr in grid cell c
+__device__ __forceinline__ uint2 pack_record(const GridView& g, int3 c, float x, float y,
+    float z, float mr)
 {
-    return uint32_t((dz + 2) * 25 + (dy + 2) * 5 + (dx + 2));
+    const uint32_t ux = fix_coord(x, g.lox, g.inv_cell, c.x);
+    const uint32_t uy = fix_coord(y, g.loy, g.inv_cell, c.y);
+    const uint32_t uz = fix_coord(z, g.loz, g.inv_cell, c.z);
+    const __half hm = __float2half_rn(mr);
+    uint16_t bm;
+    memcpy(&bm, &hm, 2);
+    return make_uint2(ux | (uy << 16), uz | (uint32_t(bm) << 16));
 }
 
-__device__ __forceinline__ void delta_decode(uint32_t code, float& dx, float& dy, float& dz)
+// x_i - x_j from two records, in units of 1/FIXQ cell
+__device__ __forceinline__ float3 record_delta(uint2 ri, uint2 rj)
 {
-    const uint32_t z = code / 25u, r = code - z * 25u, y = r / 5u;
-    dz = (float)z - 2.f;
-    dy = (float)y - 2.f;
-    dx = (float)(r - y * 5u) - 2.f;
+    // per-halfword subtraction without a borrow between the halves
+    const uint32_t dxy = __vsub2(ri.x, rj.x);
+    const uint32_t dz = ri.y - rj.y; // the low half is exact modulo 2^16
+    return make_float3(float(int16_t(dxy & 0xffffu)), float(int16_t(dxy >> 16)),
+        float(int16_t(dz & 0xffffu)));
+}
+
+__device__ __forceinline__ float record_mass_ratio(uint2 r)
+{
+    const uint16_t bm = uint16_t(r.y >> 16);
+    __half hm;
+    memcpy(&hm, &bm, 2);
+    return __half2float(hm);
+}
+
+// accelerations are stored as FP16 of a * 2^-6: up to 4e6 m/s^2 before
+// overflow, 11 significant bits
+constexpr float ACC_SCALE = 0.015625f;
+
+__device__ __forceinline__ uint2 pack_acc(float ax, float ay, float az)
+{
+    return float4_to_half4(make_float4(ax * ACC_SCALE, ay * ACC_SCALE, az * ACC_SCALE, 0.f));
+}
+
+__device__ __forceinline__ float3 unpack_acc(uint2 u)
+{
+    const float4 a = half4_to_float4(u);
+    constexpr float S = 1.f / ACC_SCALE;
+    return make_float3(a.x * S, a.y * S, a.z * S);
 }
 
 // a neighbour's velocity/density record: FP32 or FP16 storage
@@ -140,36 +180,41 @@ __device__ __forceinline__ int3 fluid_cell(const Fluid& f, const float4& me)
 }
 
 // the fluid neighbours j != i of particle i from the step's list (or, for a
-// particle whose list overflowed, from the cell traversal); f(j, pm[j], dx,
-// dy, dz, l2) in the traversal order of the cells
-template <int R, bool MIX = false, class F>
+// particle whose list overflowed, from the cell traversal); fn(j, q, dx, dy,
+// dz, l2) in the traversal order of the cells, q.w the neighbour's mass. q.xyz
+// is the neighbour's position on the FP32 path; on the mixed path with ACC it
+// is the neighbour's pressure acceleration (from the FP16 record, or FP32 for
+// a particle off the list).
+template <int R, bool MIX = false, bool ACC = false, class F>
 __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3 c,
     const float4& me, F&& fn)
 {
+    static_assert(MIX || !ACC, "accelerations travel with the mixed records only");
     const uint32_t cnt = __ldg(f.ncount + i);
     if (cnt <= KMAX) {
         const uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
-        [[maybe_unused]] float3 oi {};
-        [[maybe_unused]] float m0 = 0.f;
+        [[maybe_unused]] uint2 ri {};
+        [[maybe_unused]] float m0 = 0.f, unit = 0.f;
         if constexpr (MIX) {
-            int3 ci;
-            cell_offset(f.g, me.x, me.y, me.z, ci, oi);
+            ri = __ldg(f.pmh + i);
             m0 = __ldg(&f.pm[0].w);
-            m0 = m0 != 0.f ? m0 : 1.f;
+            unit = f.g.cell * (1.f / FIXQ);
         }
-        // one neighbour: index (and cell delta), position data, the pair
-        auto pair = [&](uint32_t e, uint32_t& j, float4& q, float& dx, float& dy, float& dz) {
+        // one neighbour: index, position data, the pair
+        auto pair = [&](uint32_t j, float4& q, float& dx, float& dy, float& dz) {
             if constexpr (MIX) {
-                j = e & IDX_MASK;
-                const float4 h = half4_to_float4(__ldg(f.pmh + j));
-                float ex, ey, ez;
-                delta_decode(e >> IDX_BITS, ex, ey, ez);
-                dx = ((oi.x - h.x) - ex) * f.g.cell;
-                dy = ((oi.y - h.y) - ey) * f.g.cell;
-                dz = ((oi.z - h.z) - ez) * f.g.cell;
-                q = make_float4(0.f, 0.f, 0.f, m0 * h.w);
+                const uint2 rj = __ldg(f.pmh + j);
+                const float3 d = record_delta(ri, rj);
+                dx = d.x * unit;
+                dy = d.y * unit;
+                dz = d.z * unit;
+                if constexpr (ACC) {
+                    const float3 a = unpack_acc(__ldg(f.acch + j));
+                    q = make_float4(a.x, a.y, a.z, m0 * record_mass_ratio(rj));
+                } else {
+                    q = make_float4(0.f, 0.f, 0.f, m0 * record_mass_ratio(rj));
+                }
             } else {
-                j = e;
                 q = __ldg(f.pm + j);
                 dx = me.x - q.x;
                 dy = me.y - q.y;
@@ -180,32 +225,38 @@ __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3
         // four neighbours per round: their index and position loads are
         // independent, which keeps more of the latency-bound loads in flight
         for (; k + 4 <= cnt; k += 4) {
-            uint32_t e[4], j[4];
+            uint32_t j[4];
             float4 q[4];
             float dx[4], dy[4], dz[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                e[u] = __ldg(row + size_t(k + u) * 128);
+                j[u] = __ldg(row + size_t(k + u) * 128);
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                pair(e[u], j[u], q[u], dx[u], dy[u], dz[u]);
+                pair(j[u], q[u], dx[u], dy[u], dz[u]);
 #pragma unroll
             for (int u = 0; u < 4; ++u)
                 fn(j[u], q[u], dx[u], dy[u], dz[u],
                     fmaf(dx[u], dx[u], fmaf(dy[u], dy[u], dz[u] * dz[u])));
         }
         for (; k < cnt; ++k) {
-            uint32_t j;
+            const uint32_t j = __ldg(row + size_t(k) * 128);
             float4 q;
             float dx, dy, dz;
-            pair(__ldg(row + size_t(k) * 128), j, q, dx, dy, dz);
+            pair(j, q, dx, dy, dz);
             fn(j, q, dx, dy, dz, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
         }
     } else {
         for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
             [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
-                if (j != i)
+                if (j == i)
+                    return;
+                if constexpr (ACC) {
+                    const float4 a = __ldg(f.acc32 + j);
+                    fn(j, make_float4(a.x, a.y, a.z, q.w), dx, dy, dz, l2);
+                } else {
                     fn(j, q, dx, dy, dz, l2);
+                }
             });
     }
 }
@@ -291,8 +342,8 @@ __device__ __forceinline__ void block_accumulate(SweepStats* st, unsigned over, 
 // compute_densities (solver.cuh:18-38) + cached boundary sums + the step's
 // neighbour list, written entry by entry (a block's rows form one 32 KB
 // region, so the L2 merges the scattered 4-byte stores into full lines).
-// Mixed precision: list entries carry the neighbour's cell delta, and the
-// particle's FP16 position/velocity records are written for later passes.
+// Mixed precision: the particle's 8-byte position and velocity records are
+// written for later passes.
 template <int KIND, int R, bool MIX = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bdy b,
     float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm,
@@ -303,40 +354,18 @@ __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bd
         return;
     const float4 me = f.pm[i];
     const int3 c = fluid_cell<R>(f, me);
-    [[maybe_unused]] int3 cm {};
-    [[maybe_unused]] float3 om {};
-    if constexpr (MIX)
-        cell_offset(f.g, me.x, me.y, me.z, cm, om);
     uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
     uint32_t cnt = 0;
-    [[maybe_unused]] bool far = false; // a cell delta outside [-2, 2] (rounding)
     float rf = 0.f;
     for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
         [&](uint32_t j, const float4& q, float, float, float, float l2) {
             rf += q.w * pair_w<KIND>(f.kc, l2);
             if (j != i) {
-                if (cnt < KMAX) {
-                    uint32_t e = j;
-                    if constexpr (MIX) {
-                        const int dx = (int)floorf((q.x - f.g.lox) * f.g.inv_cell) - cm.x;
-                        const int dy = (int)floorf((q.y - f.g.loy) * f.g.inv_cell) - cm.y;
-                        const int dz = (int)floorf((q.z - f.g.loz) * f.g.inv_cell) - cm.z;
-                        if (abs(dx) > 2 || abs(dy) > 2 || abs(dz) > 2)
-                            far = true;
-                        else
-                            e |= delta_code(dx, dy, dz) << IDX_BITS;
-                    }
-                    row[size_t(cnt) * 128] = e;
-                }
+                if (cnt < KMAX)
+                    row[size_t(cnt) * 128] = j;
                 ++cnt;
             }
         });
-    if constexpr (MIX) {
-        // a pair the FP16 record cannot encode: this particle is served by the
-        // FP32 cell traversal in every later pass, like a list overflow
-        if (far)
-            cnt = KMAX + 1;
-    }
     float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     for_each_boundary(b, me.x, me.y, me.z,
         [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
@@ -356,7 +385,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bd
     if constexpr (MIX) {
         const float4 v = vel[i];
         const float m0 = __ldg(&f.pm[0].w);
-        pmh_out[i] = float4_to_half4(make_float4(om.x, om.y, om.z, me.w / (m0 != 0.f ? m0 : 1.f)));
+        pmh_out[i] = pack_record(f.g, c, me.x, me.y, me.z, me.w / (m0 != 0.f ? m0 : 1.f));
         velh_out[i] = float4_to_half4(make_float4(v.x, v.y, v.z, r));
     }
 }
@@ -581,7 +610,8 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
     const float4* __restrict__ vel, const uint2* __restrict__ velh,
     const float4* __restrict__ bterm, float rho0, float dt,
     float r0i, const float* __restrict__ p_old, float* __restrict__ aii,
-    float* __restrict__ sii, float* __restrict__ p_new, float4* __restrict__ acc)
+    float* __restrict__ sii, float* __restrict__ p_new, float4* __restrict__ acc,
+    uint2* __restrict__ acch_out)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
@@ -609,8 +639,11 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
             az += sp * dz;
         });
     const float4 bt = bterm[i];
-    acc[i] = make_float4(-r0i * (ax + pi * bt.x), -r0i * (ay + pi * bt.y),
+    const float4 ai = make_float4(-r0i * (ax + pi * bt.x), -r0i * (ay + pi * bt.y),
         -r0i * (az + pi * bt.z), 0.f);
+    acc[i] = ai;
+    if constexpr (MIX)
+        acch_out[i] = pack_acc(ai.x, ai.y, ai.z);
     gx += bt.x;
     gy += bt.y;
     gz += bt.z;
@@ -624,7 +657,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
 template <int KIND, int R, bool MIX = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
-    float4* __restrict__ acc)
+    float4* __restrict__ acc, uint2* __restrict__ acch_out)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
@@ -641,8 +674,11 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
             az += s * dz;
         });
     const float4 bt = bterm[i];
-    acc[i] = make_float4(-r0i * (ax + pi * bt.x), -r0i * (ay + pi * bt.y),
+    const float4 ai = make_float4(-r0i * (ax + pi * bt.x), -r0i * (ay + pi * bt.y),
         -r0i * (az + pi * bt.z), 0.f);
+    acc[i] = ai;
+    if constexpr (MIX)
+        acch_out[i] = pack_acc(ai.x, ai.y, ai.z);
 }
 
 // _jacobi_update_pressures (IISPH.cu:119-162); the convergence bitmask of the
@@ -663,9 +699,15 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
         const int3 c = fluid_cell<R>(f, me);
         const float4 ai = acc[i];
         float sum = 0.f;
-        for_each_listed<R, MIX>(f, i, c, me,
+        for_each_listed<R, MIX, MIX>(f, i, c, me,
             [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
-                const float4 aj = __ldg(acc + j);
+                float3 aj;
+                if constexpr (MIX) {
+                    aj = make_float3(q.x, q.y, q.z);
+                } else {
+                    const float4 a = __ldg(acc + j);
+                    aj = make_float3(a.x, a.y, a.z);
+                }
                 const float d = fmaf(ai.x - aj.x, dx, fmaf(ai.y - aj.y, dy, (ai.z - aj.z) * dz));
                 sum += q.w * (pair_g<KIND>(f.kc, l2) * d);
             });
@@ -809,6 +851,7 @@ static void ensure_buffers(reyn_solver& sv, uint32_t n)
     sv.ncount.resize(n);
     if (sv.prm.precision == REYN_PRECISION_MIXED) {
         sv.pmh.resize(n);
+        sv.acch.resize(n);
         sv.velh.resize(n);
         sv.velh2.resize(n);
     }
@@ -863,6 +906,8 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     f.nbr = sv.nbr.get();
     f.ncount = sv.ncount.get();
     f.pmh = nullptr;
+    f.acch = nullptr;
+    f.acc32 = sv.acc.get();
     Bdy b {};
     if (bdy && bdy->nb) {
         b.g = bdy->view();
@@ -894,9 +939,11 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
 
     const bool mixed = P.precision == REYN_PRECISION_MIXED;
     uint2* PMH = mixed ? sv.pmh.get() : nullptr;
+    uint2* ACH = mixed ? sv.acch.get() : nullptr;
     uint2* VH = mixed ? sv.velh.get() : nullptr;
     uint2* VH2 = mixed ? sv.velh2.get() : nullptr;
     f.pmh = PMH;
+    f.acch = ACH;
     auto body = [&](auto KC, auto RC, auto MC) {
         constexpr int K = decltype(KC)::value;
         constexpr int R = decltype(RC)::value;
@@ -951,13 +998,13 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             auto pacc = [&] {
                 REYN_KERNEL("k_iisph_pacc", s,
                     k_iisph_pacc<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(),
-                    sv.bterm.get(), r0i, sv.acc.get()));
+                    sv.bterm.get(), r0i, sv.acc.get(), ACH));
             };
             if (P.warmstart) {
                 REYN_KERNEL("k_iisph_diag_pacc", s,
                     k_iisph_diag_pacc<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
                     VH2, sv.bterm.get(), rho0, dt, r0i, sv.p.get(), sv.aii.get(), sv.sii.get(),
-                    sv.p_tmp.get(), sv.acc.get()));
+                    sv.p_tmp.get(), sv.acc.get(), ACH));
                 sv.p.swap(sv.p_tmp);
             } else {
                 REYN_KERNEL("k_iisph_diag", s,

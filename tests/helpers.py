@@ -39,7 +39,8 @@ def by_id(arrs: dict, ids: np.ndarray) -> dict:
 
 
 def run_engine(scheme: int, kind: int, fluid: dict, bdy: dict, box_min, box_max, h: float,
-               rho0: float, nu: float, dt: float, steps: int, params=None, cell_ratio=0.5):
+               rho0: float, nu: float, dt: float, steps: int, params=None, cell_ratio=0.5,
+               order=0):
     """The reference main loop on the engine: construct_and_reorder (with
     the particle ID as an extra array), solver step, hard bounds."""
     import torch
@@ -55,7 +56,7 @@ def run_engine(scheme: int, kind: int, fluid: dict, bdy: dict, box_min, box_max,
     bt = {k: torch.tensor(np.asarray(bdy[k], np.float32), device=dev) for k in ("x", "y", "z")}
     bm = torch.tensor(np.asarray(bdy["m"], np.float32), device=dev) if "m" in bdy else None
     bd = rb.Boundary(bt["x"], bt["y"], bt["z"], bm, h=h, rho0=rho0, mass_iters=5) if nb else None
-    grid = rb.Grid(box_min, box_max, 2.0 * h, cell_ratio)
+    grid = rb.Grid(box_min, box_max, 2.0 * h, cell_ratio, order)
     prm = params or rb.reference_params(scheme, kind, h, rho0, nu)
     sv = rb.Solver(scheme, prm, n)
     iters = []

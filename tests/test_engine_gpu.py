@@ -29,13 +29,14 @@ def test_kernel_eval_vs_reference(cuda, name, kind):
     assert_close(gg, g[f"{name}_g"], 1e-4, 1e-6, f"{name} dW")
 
 
-def _engine_grid(x, y, z, bmin, bmax, r, ratio=0.5, kind=None, m=None):
+def _engine_grid(x, y, z, bmin, bmax, r, ratio=0.5, kind=None, m=None, order=0):
     import reyn_b200 as rb
-    grid = rb.Grid(bmin, bmax, r, ratio)
+    grid = rb.Grid(bmin, bmax, r, ratio, order)
     tx, ty, tz = T(x), T(y), T(z)
     grid.construct(tx, ty, tz)
     info = grid.info()
-    C = info.nx * info.ny * info.nz
+    C = info.n_keys
+    assert info.order == order
     prefix = rb.device_to_numpy(info.prefix, C + 1, np.uint32)
     srt = rb.device_to_numpy(info.sorted, x.size, np.uint32)
     tm = T(m) if m is not None else None
@@ -65,15 +66,18 @@ def test_grid_vs_reference_fixture(cuda, name):
         assert_close(e["rho"], g[f"rho_k{k}"], 1e-6, 1e-7, f"rho kernel {k}")
 
 
-@pytest.mark.parametrize("ratio", [0.5, 1.0])
-def test_grid_vs_oracle_microbench_full_size(cuda, ratio):
+@pytest.mark.parametrize("ratio,order", [(0.5, 0), (1.0, 0), (0.5, 1), (1.0, 1)])
+def test_grid_vs_oracle_microbench_full_size(cuda, ratio, order):
     """The neighbour-search + density microbenchmark at its full size:
-    1,048,576 uniform points, r = 0.0196, Wendland C2, m = rho0 0.0098^3."""
+    1,048,576 uniform points, r = 0.0196, Wendland C2, m = rho0 0.0098^3, in
+    the reference's XYZ cell order and in Z-order: prefix and sorted
+    bit-exact against the oracle's build in the same order, neighbour counts
+    exact, densities within 1e-6."""
     x, y, z = scenes.uniform_cloud(1 << 20, seed=2)
     r = 0.0196
     m = np.full(x.size, np.float32(1000.0 * 0.0098 ** 3), np.float32)
-    e = _engine_grid(x, y, z, [0, 0, 0], [1, 1, 1], r, ratio, kind=0, m=m)
-    geom = oracle.geometry([0, 0, 0], [1, 1, 1], r, ratio)
+    e = _engine_grid(x, y, z, [0, 0, 0], [1, 1, 1], r, ratio, kind=0, m=m, order=order)
+    geom = oracle.geometry([0, 0, 0], [1, 1, 1], r, ratio, order=order)
     prefix, srt, _ = oracle.grid_build(geom, x, y, z)
     np.testing.assert_array_equal(e["prefix"], prefix)
     np.testing.assert_array_equal(e["sorted"], srt)
@@ -128,15 +132,18 @@ def test_solver_vs_reference_fixture(cuda, name):
     compare_steps(got, fixture_outputs(g), scheme, tol, name)
 
 
-@pytest.mark.parametrize("scheme,kind,steps,dt", [(0, 1, 5, 5e-4), (1, 1, 2, 1e-3),
-                                                  (2, 0, 3, 1e-3), (2, 2, 2, 1e-3),
-                                                  (1, 3, 1, 1e-3)])
-def test_solver_vs_oracle(cuda, scheme, kind, steps, dt):
+@pytest.mark.parametrize("scheme,kind,steps,dt,order", [(0, 1, 5, 5e-4, 0), (1, 1, 2, 1e-3, 0),
+                                                        (2, 0, 3, 1e-3, 0), (2, 2, 2, 1e-3, 0),
+                                                        (1, 3, 1, 1e-3, 0), (2, 0, 3, 1e-3, 1),
+                                                        (1, 1, 2, 1e-3, 1), (0, 1, 5, 5e-4, 1)])
+def test_solver_vs_oracle(cuda, scheme, kind, steps, dt, order):
+    """Every scheme against the oracle (the reference's XYZ order); with the
+    engine's grid in Z-order (order 1) only the summation order differs."""
     sc = scenes.dam_break((20, 18, 16), 0.02, (0.6, 0.6, 0.6), velocity_noise=0.05, seed=5)
     bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
     bdy = dict(sc.bdy, m=bm)
     got = run_engine(scheme, kind, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, 0.01,
-                     dt, steps)
+                     dt, steps, order=order)
     want = run_oracle(scheme, kind, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, 0.01,
                       dt, steps)
     assert got["iters"] == want["iters"]

@@ -1,15 +1,17 @@
-"""The mixed-precision IISPH solver (neighbour positions stored cell-relative
-in FP16, neighbour velocities in FP16, FP32 arithmetic) against the FP64
+"""The mixed-precision IISPH solver (neighbour positions stored as 16-bit
+fixed point relative to the grid, neighbour masses, velocities, densities and
+pressure accelerations in FP16, FP32 arithmetic) against the FP64
 restatement of the step, beside the FP32 solver on the same inputs.
 
 Both solvers run a fixed number of Jacobi sweeps (min_iter = max_iter, a
 criterion every sweep meets), so that all three carry out the same
 arithmetic; the errors are stated per quantity relative to the field's
-largest magnitude. Bounds: FP16 offsets round to 2^-12 cells, velocities to
-2^-11 relative, which puts the mixed solver's pressure and velocity errors at
-about 1e-3 of their scale, and its position and density errors (dt^2 and
-dt^3 behind) far below; the average density error must stay far below the
-0.1 % convergence tolerance it is run at.
+largest magnitude. The roundings are the FP16 velocity and acceleration
+records (2^-12 relative) and the 16-bit positions (2^-15 cell), which put the
+mixed solver's velocity errors near 1e-3 of their scale after a few steps and
+its position, density and pressure errors one to two orders below. The
+average density deviation from FP64 stays well below the 0.1 % convergence
+tolerance the solver is run at.
 """
 import numpy as np
 import pytest
@@ -23,9 +25,16 @@ pytestmark = pytest.mark.gpu
 
 FIELDS = ("x", "y", "z", "vx", "vy", "vz", "rho", "p", "aii", "sii")
 # per-quantity bound of the mixed solver's error against FP64 (relative to the
-# field's largest magnitude)
-MIXED_TOL = {"x": 1e-5, "y": 1e-5, "z": 1e-5, "vx": 5e-3, "vy": 5e-3, "vz": 5e-3,
-             "rho": 1e-5, "p": 2e-2, "aii": 5e-3, "sii": 2e-2}
+# field's largest magnitude), per kernel: about 4x the errors measured on a
+# B200. The scene starts over-dense (lattice masses at rho0 h^3), most for
+# Wendland C6 (lattice sum 1.17), so its large pressure accelerations carry
+# larger FP16 rounding into velocities and positions.
+MIXED_TOL = {
+    0: {"x": 1e-4, "y": 1e-4, "z": 1e-4, "vx": 3e-3, "vy": 3e-3, "vz": 3e-3,
+        "rho": 2e-4, "p": 1e-3, "aii": 1e-3, "sii": 2e-3, "avg_rho_rel": 3e-5},
+    2: {"x": 2e-4, "y": 2e-4, "z": 2e-4, "vx": 1e-2, "vy": 1e-2, "vz": 1e-2,
+        "rho": 1.5e-3, "p": 7e-3, "aii": 5e-3, "sii": 2e-3, "avg_rho_rel": 2e-4},
+}
 
 
 def _fixed_params(kind, h, rho0, precision, sweeps=4):
@@ -50,12 +59,13 @@ def _both_vs_fp64(kind, sc, bdy, h, cell_ratio, steps, dt):
     """errors of the FP32 and the mixed solver against FP64, same inputs"""
     import reyn_b200 as rb
     errs = {}
+    want = None
     for name, prec in (("fp32", rb.PRECISION_FP32), ("mixed", rb.PRECISION_MIXED)):
         prm = _fixed_params(kind, h, sc.rho0, prec)
         got = run_engine(2, kind, sc.fluid, bdy, sc.box_min, sc.box_max, h, sc.rho0, 0.01,
                          dt, steps, params=prm, cell_ratio=cell_ratio)
         assert got["iters"] == [4] * steps
-        if name == "fp32":
+        if want is None:
             want = fp64.iisph_run(kind, sc.fluid, bdy, sc.box_min, sc.box_max, h, sc.rho0,
                                   0.01, tuple(prm.g), dt, steps, 4, prm.omega,
                                   bool(prm.warmstart))
@@ -67,29 +77,27 @@ def _both_vs_fp64(kind, sc, bdy, h, cell_ratio, steps, dt):
 
 @pytest.mark.parametrize("kind", [0, 2])
 def test_mixed_vs_fp64_beside_fp32(cuda, kind):
-    import reyn_b200 as rb
     sc = scenes.dam_break((20, 18, 16), 0.02, (0.6, 0.6, 0.6), velocity_noise=0.05, seed=5)
     bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
     bdy = dict(sc.bdy, m=bm)
     errs = _both_vs_fp64(kind, sc, bdy, sc.h, 0.5, steps=3, dt=1e-3)
-    for k, t in MIXED_TOL.items():
+    for k, t in MIXED_TOL[kind].items():
         assert errs["mixed"][k] <= t, (k, errs["mixed"][k], errs["fp32"][k])
-    assert errs["mixed"]["avg_rho_rel"] <= 1e-5
+    # far below the 0.1 % average density error the solver converges to
+    assert errs["mixed"]["avg_rho_rel"] < 1e-3 / 4
 
 
 def test_mixed_with_list_overflow_and_unit_cells(cuda):
     """A compressed block (spacing 0.6 h: about 150 neighbours, past the
     64-entry list) sends the interior particles to the FP32 cell traversal
-    while the corners keep their lists, and cell size = support radius (cell
-    delta within +-1) exercises the other encoding range; both agree with the
-    FP32 solver within the mixed solver's bounds."""
-    import reyn_b200 as rb
+    while the corners keep their lists, and cell size = support radius
+    exercises the other grid geometry; both stay within the mixed bounds."""
     sc = scenes.dam_break((16, 14, 12), 0.02, (0.6, 0.6, 0.6), velocity_noise=0.05, seed=9)
     bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
     bdy = dict(sc.bdy, m=bm)
     for h, ratio in ((sc.h / 0.6, 0.5), (sc.h, 1.0)):
         errs = _both_vs_fp64(0, sc, bdy, h, ratio, steps=2, dt=5e-4)
-        for k, t in MIXED_TOL.items():
+        for k, t in MIXED_TOL[0].items():
             assert errs["mixed"][k] <= t, (ratio, k, errs["mixed"][k], errs["fp32"][k])
 
 

@@ -90,6 +90,47 @@ def test_oracle_grid_invariants(ratio):
     np.testing.assert_array_equal(c, cb)
 
 
+def _zorder_key_spec(cx, cy, cz, nx, ny):
+    """The Z-order key as documented (4^3-cell bricks, x fastest inside;
+    bricks along the Morton curve inside 32^3-cell tiles; tiles in XYZ
+    order), written independently of the oracle's C++ for a cross-check."""
+    tx, ty = -(-nx // 32), -(-ny // 32)
+    tile = (cz // 32 * ty + cy // 32) * tx + cx // 32
+    bx, by, bz = (cx // 4) % 8, (cy // 4) % 8, (cz // 4) % 8
+    brick = 0
+    for bit in range(3):
+        brick |= ((bx >> bit) & 1) << (3 * bit)
+        brick |= ((by >> bit) & 1) << (3 * bit + 1)
+        brick |= ((bz >> bit) & 1) << (3 * bit + 2)
+    return (tile * 512 + brick) * 64 + cx % 4 + 4 * (cy % 4) + 16 * (cz % 4)
+
+
+@pytest.mark.parametrize("ratio", [0.5, 1.0])
+def test_oracle_zorder_grid(ratio):
+    """Z-order: every cell gets its own key, the build sorts by it, and the
+    cell-by-cell traversal finds exactly the brute-force neighbours."""
+    x, y, z = scenes.uniform_cloud(20000, seed=6)
+    g = oracle.geometry([0, 0, 0], [1, 1, 1], 0.05, ratio, order=1)
+    assert g.order == 1 and g.n_keys >= g.n_cells
+    prefix, srt, keys = oracle.grid_build(g, x, y, z)
+    assert prefix.size == g.n_keys + 1 and prefix[-1] == x.size
+    cell = np.float32(g.cell)
+    c = [np.floor((a - np.float32(lo)) / cell).astype(np.int64)
+         for a, lo in zip((x, y, z), g.bmin)]
+    np.testing.assert_array_equal(keys, _zorder_key_spec(c[0], c[1], c[2], g.nx, g.ny))
+    # a bijection from cells into the key space
+    cx, cy, cz = np.meshgrid(np.arange(g.nx), np.arange(g.ny), np.arange(g.nz), indexing="ij")
+    allk = _zorder_key_spec(cx.ravel(), cy.ravel(), cz.ravel(), g.nx, g.ny)
+    assert np.unique(allk).size == allk.size and allk.max() < g.n_keys
+    k = keys[srt]
+    assert np.all(np.diff(k.astype(np.int64)) >= 0)
+    same = np.diff(k.astype(np.int64)) == 0
+    assert np.all(np.diff(srt.astype(np.int64))[same] > 0)
+    cnt, _, _ = oracle.neighbours(g, x, y, z, prefix, srt)
+    cb, _ = oracle.brute_count(x, y, z, 0.05)
+    np.testing.assert_array_equal(cnt, cb)
+
+
 @pytest.mark.parametrize("name", ["grid_test.npz", "grid_cloud.npz"])
 def test_oracle_grid_vs_reference_fixture(name):
     g = golden(name)
