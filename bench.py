@@ -12,14 +12,14 @@ state, IISPH step, hard bounds. Inputs are resident in HBM for `value`; `e2e`
 repeats the step through the C ABI with the state uploaded from and downloaded
 to pinned host memory inside the timed region.
 
-The headline is the mixed-precision solver (neighbour positions as 16-bit
-fixed point, neighbour masses, velocities and pressure accelerations FP16,
-FP32 arithmetic, FP64 convergence reduction);
-by default the plain FP32 solver is timed first on the same scene and reported
-beside it ("fp32", "mixed_over_fp32").
+The headline is the mixed-precision solver (neighbour velocities, densities
+and pressure accelerations FP16, FP32 positions and arithmetic, FP64
+convergence reduction); by default the plain FP32 solver and the mixed solver
+with 16-bit neighbour positions are timed on the same scene and reported
+beside it ("fp32", "mixed_pos16", "mixed_over_fp32").
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                       [--precision both|mixed|fp32]
+                       [--precision all|mixed|mixed_pos16|fp32]
 Under torchrun (N > 1) every rank advances its own independently seeded scene
 (weak scaling, no data-path collective); rank 0 prints one JSON line.
 """
@@ -73,8 +73,9 @@ def parse_args():
     ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
     ap.add_argument("--scale", type=int, default=1,
                     help="divide the lattice by this factor per axis (testing only)")
-    ap.add_argument("--precision", choices=["both", "mixed", "fp32"], default="both",
-                    help="both: time the FP32 path, then report the mixed path beside it")
+    ap.add_argument("--precision", choices=["all", "mixed", "mixed_pos16", "fp32"],
+                    default="all",
+                    help="all: time FP32 and mixed_pos16, then report the mixed path beside them")
     ap.add_argument("--order", choices=["xyz", "zorder"], default="xyz",
                     help="cell order of the grid the state is sorted by")
     ap.add_argument("--no-e2e", action="store_true")
@@ -113,7 +114,7 @@ def profile_traffic(kernel: str, precision: str):
     """DRAM bytes per launch of `kernel` on this workload, from the committed
     ncu summary (profiles/<kernel>_iisph_4m[_mixed].txt, line
     'traffic_bytes_per_launch:')."""
-    suffix = "_mixed" if precision == "mixed" else ""
+    suffix = "" if precision == "fp32" else "_" + precision
     path = os.path.join(ROOT, "profiles", f"{kernel}_iisph_4m{suffix}.txt")
     try:
         for line in open(path):
@@ -220,7 +221,8 @@ class EngineRun:
         prm.convergence = rb.CONV_AVERAGE
         prm.eta = 0.001
         prm.max_iter = 1000
-        prm.precision = rb.PRECISION_MIXED if precision == "mixed" else rb.PRECISION_FP32
+        prm.precision = {"mixed": rb.PRECISION_MIXED, "mixed_pos16": rb.PRECISION_MIXED_POS16,
+                         "fp32": rb.PRECISION_FP32}[precision]
         self.sv = rb.Solver(rb.IISPH, prm, sc.n)
         self.dt, self.iters = DT0, 0
         self.dt_visc = viscous_dt_limit(sc.h, NU)
@@ -313,17 +315,19 @@ def run_engine(a, world, rank, local):
     stream = torch.cuda.current_stream(dev)
     S = stream.cuda_stream
 
-    # the plain FP32 path first, on the same scene, as the comparison leg
-    fp32 = None
-    if a.precision == "both":
-        run = EngineRun(rank, a.scale, dev, "fp32", a.order)
-        _, _, ms32, _, clk32, log32 = timed_steps(run, a, world, stream, dev)
-        fp32 = leg_summary(run, a, world, ms32, log32)
-        fp32["clocks"] = clk32
-        run.close()
-        torch.cuda.synchronize()
+    # the plain FP32 path and the 16-bit-position variant first, on the same
+    # scene, as the comparison legs
+    legs = {}
+    if a.precision == "all":
+        for name in ("fp32", "mixed_pos16"):
+            run = EngineRun(rank, a.scale, dev, name, a.order)
+            _, _, msl, _, clk, logl = timed_steps(run, a, world, stream, dev)
+            legs[name] = leg_summary(run, a, world, msl, logl)
+            legs[name]["clocks"] = clk
+            run.close()
+            torch.cuda.synchronize()
 
-    headline = "fp32" if a.precision == "fp32" else "mixed"
+    headline = "mixed" if a.precision == "all" else a.precision
     run = EngineRun(rank, a.scale, dev, headline, a.order)
     n = run.n
     ck, ms, ms_max, prof, ck_clocks, log = timed_steps(run, a, world, stream, dev)
@@ -378,10 +382,13 @@ def run_engine(a, world, rank, local):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline_from(ck, run)
 
-    precision = ("fp32 storage and math" if headline == "fp32" else
-                 "mixed: neighbour positions 16-bit fixed point (1/16384 cell), neighbour "
-                 "masses, velocities and pressure accelerations FP16, own data and all "
-                 "arithmetic FP32, FP64 convergence reduction")
+    precision = {
+        "fp32": "fp32 storage and math",
+        "mixed": "mixed: neighbour velocities, densities and pressure accelerations FP16; "
+                 "positions, own data and all arithmetic FP32; Kahan density and divergence "
+                 "sums; FP64 convergence reduction",
+        "mixed_pos16": "mixed with neighbour positions as 16-bit fixed point (1/16384 cell) "
+                       "and masses FP16"}[headline]
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 3),
@@ -403,9 +410,9 @@ def run_engine(a, world, rank, local):
         "dt_per_step": [float(f"{x[2]:.4e}") for x in log],
         "iter_limit_hits": run.limit_hits, "kernels": kernels,
     }
-    if fp32 is not None:
-        out["fp32"] = fp32
-        out["mixed_over_fp32"] = round(value / fp32["value"], 3)
+    out.update(legs)
+    if "fp32" in legs:
+        out["mixed_over_fp32"] = round(value / legs["fp32"]["value"], 3)
     if rank == 0:
         print(json.dumps(out), flush=True)
     run.close()

@@ -211,11 +211,15 @@ typedef enum reyn_convergence {
 typedef enum reyn_precision {
     /* FP32 storage and arithmetic, as the reference */
     REYN_PRECISION_FP32 = 0,
-    /* IISPH only: neighbour positions stored as 16-bit fixed point relative
-     * to the grid (1/16384 cell), neighbour masses, velocities, densities and
-     * pressure accelerations as FP16; the particle's own data and all
-     * arithmetic stay FP32, the convergence reduction FP64. */
-    REYN_PRECISION_MIXED = 1
+    /* IISPH only: the velocities, densities and pressure accelerations the
+     * neighbour loops read of a particle's neighbours are stored as FP16;
+     * positions, the particle's own data and all arithmetic stay FP32, the
+     * convergence reduction FP64. */
+    REYN_PRECISION_MIXED = 1,
+    /* IISPH only: as REYN_PRECISION_MIXED, and neighbour positions stored as
+     * 16-bit fixed point relative to the grid (1/16384 cell) with FP16
+     * masses (relative to particle 0's) */
+    REYN_PRECISION_MIXED_POS16 = 2
 } reyn_precision;
 
 typedef struct reyn_params {

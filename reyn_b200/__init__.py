@@ -23,7 +23,7 @@ C2, B3, W6, COS = 0, 1, 2, 3
 KERNELS = {"C2": C2, "B3": B3, "W6": W6, "COS": COS}
 SESPH, PCISPH, IISPH = 0, 1, 2
 CONV_REFERENCE, CONV_AVERAGE = 0, 1
-PRECISION_FP32, PRECISION_MIXED = 0, 1
+PRECISION_FP32, PRECISION_MIXED, PRECISION_MIXED_POS16 = 0, 1, 2
 ORDER_XYZ, ORDER_ZORDER = 0, 1
 
 OK = 0

@@ -33,7 +33,8 @@ void check_params(reyn_scheme scheme, const reyn_params* p)
     require(p->omega > 0.f && p->omega < 2.f, "omega must lie in (0, 2)");
     require(p->convergence == REYN_CONV_REFERENCE || p->convergence == REYN_CONV_AVERAGE,
         "unknown convergence criterion");
-    require(p->precision == REYN_PRECISION_FP32 || p->precision == REYN_PRECISION_MIXED,
+    require(p->precision == REYN_PRECISION_FP32 || p->precision == REYN_PRECISION_MIXED
+            || p->precision == REYN_PRECISION_MIXED_POS16,
         "unknown precision");
     require(p->precision == REYN_PRECISION_FP32 || scheme == REYN_IISPH,
         "mixed precision is implemented for IISPH");

@@ -74,6 +74,12 @@ struct Fluid {
 // coordinate (FP16 offsets within a cell would round to 1/4096).
 constexpr float FIXQ = 16384.f;
 
+// storage modes of the neighbour loops (the template argument MIX):
+// 0 FP32; MIX_F16 FP16 velocities, densities and pressure accelerations of
+// neighbours; MIX_POS16 those plus the 16-bit position records
+constexpr int MIX_F16 = 1;
+constexpr int MIX_POS16 = 2;
+
 __device__ __forceinline__ float4 half4_to_float4(uint2 u)
 {
     __half2 a, b;
@@ -141,15 +147,28 @@ __device__ __forceinline__ uint2 pack_acc(float ax, float ay, float az)
     return float4_to_half4(make_float4(ax * ACC_SCALE, ay * ACC_SCALE, az * ACC_SCALE, 0.f));
 }
 
-__device__ __forceinline__ float3 unpack_acc(uint2 u)
+// the stored (scaled) acceleration: a * ACC_SCALE
+__device__ __forceinline__ float3 unpack_acc_scaled(uint2 u)
 {
     const float4 a = half4_to_float4(u);
-    constexpr float S = 1.f / ACC_SCALE;
-    return make_float3(a.x * S, a.y * S, a.z * S);
+    return make_float3(a.x, a.y, a.z);
 }
 
+// compensated (Kahan) summation for the mixed modes' density and divergence
+// sums: sum + comp carries the rounding the plain sum would drop
+struct Kahan {
+    float sum = 0.f, comp = 0.f;
+    __device__ __forceinline__ void add(float v)
+    {
+        const float y = __fsub_rn(v, comp);
+        const float t = __fadd_rn(sum, y);
+        comp = __fsub_rn(__fsub_rn(t, sum), y);
+        sum = t;
+    }
+};
+
 // a neighbour's velocity/density record: FP32 or FP16 storage
-template <bool MIX>
+template <int MIX>
 __device__ __forceinline__ float4 nbr_vel(const float4* __restrict__ v32,
     const uint2* __restrict__ v16, uint32_t j)
 {
@@ -183,9 +202,9 @@ __device__ __forceinline__ int3 fluid_cell(const Fluid& f, const float4& me)
 // particle whose list overflowed, from the cell traversal); fn(j, q, dx, dy,
 // dz, l2) in the traversal order of the cells, q.w the neighbour's mass. q.xyz
 // is the neighbour's position on the FP32 path; on the mixed path with ACC it
-// is the neighbour's pressure acceleration (from the FP16 record, or FP32 for
-// a particle off the list).
-template <int R, bool MIX = false, bool ACC = false, class F>
+// is the neighbour's pressure acceleration times ACC_SCALE (from the FP16
+// record, or FP32 for a particle off the list).
+template <int R, int MIX = 0, bool ACC = false, class F>
 __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3 c,
     const float4& me, F&& fn)
 {
@@ -195,30 +214,31 @@ __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3
         const uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
         [[maybe_unused]] uint2 ri {};
         [[maybe_unused]] float m0 = 0.f, unit = 0.f;
-        if constexpr (MIX) {
+        if constexpr (MIX == MIX_POS16) {
             ri = __ldg(f.pmh + i);
             m0 = __ldg(&f.pm[0].w);
             unit = f.g.cell * (1.f / FIXQ);
         }
         // one neighbour: index, position data, the pair
         auto pair = [&](uint32_t j, float4& q, float& dx, float& dy, float& dz) {
-            if constexpr (MIX) {
+            if constexpr (MIX == MIX_POS16) {
                 const uint2 rj = __ldg(f.pmh + j);
                 const float3 d = record_delta(ri, rj);
                 dx = d.x * unit;
                 dy = d.y * unit;
                 dz = d.z * unit;
-                if constexpr (ACC) {
-                    const float3 a = unpack_acc(__ldg(f.acch + j));
-                    q = make_float4(a.x, a.y, a.z, m0 * record_mass_ratio(rj));
-                } else {
-                    q = make_float4(0.f, 0.f, 0.f, m0 * record_mass_ratio(rj));
-                }
+                q.w = m0 * record_mass_ratio(rj);
             } else {
                 q = __ldg(f.pm + j);
                 dx = me.x - q.x;
                 dy = me.y - q.y;
                 dz = me.z - q.z;
+            }
+            if constexpr (ACC) {
+                const float3 a = unpack_acc_scaled(__ldg(f.acch + j));
+                q.x = a.x;
+                q.y = a.y;
+                q.z = a.z;
             }
         };
         uint32_t k = 0;
@@ -253,7 +273,8 @@ __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3
                     return;
                 if constexpr (ACC) {
                     const float4 a = __ldg(f.acc32 + j);
-                    fn(j, make_float4(a.x, a.y, a.z, q.w), dx, dy, dz, l2);
+                    fn(j, make_float4(a.x * ACC_SCALE, a.y * ACC_SCALE, a.z * ACC_SCALE, q.w),
+                        dx, dy, dz, l2);
                 } else {
                     fn(j, q, dx, dy, dz, l2);
                 }
@@ -344,7 +365,7 @@ __device__ __forceinline__ void block_accumulate(SweepStats* st, unsigned over, 
 // region, so the L2 merges the scattered 4-byte stores into full lines).
 // Mixed precision: the particle's 8-byte position and velocity records are
 // written for later passes.
-template <int KIND, int R, bool MIX = false>
+template <int KIND, int R, int MIX = 0>
 __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bdy b,
     float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm,
     uint2* __restrict__ pmh_out, uint2* __restrict__ velh_out)
@@ -357,15 +378,21 @@ __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bd
     uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
     uint32_t cnt = 0;
     float rf = 0.f;
+    [[maybe_unused]] Kahan rk; // mixed modes: compensated density sum
     for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
         [&](uint32_t j, const float4& q, float, float, float, float l2) {
-            rf += q.w * pair_w<KIND>(f.kc, l2);
+            if constexpr (MIX)
+                rk.add(q.w * pair_w<KIND>(f.kc, l2));
+            else
+                rf += q.w * pair_w<KIND>(f.kc, l2);
             if (j != i) {
                 if (cnt < KMAX)
                     row[size_t(cnt) * 128] = j;
                 ++cnt;
             }
         });
+    if constexpr (MIX)
+        rf = rk.sum;
     float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     for_each_boundary(b, me.x, me.y, me.z,
         [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
@@ -384,16 +411,18 @@ __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bd
     f.ncount[i] = cnt;
     if constexpr (MIX) {
         const float4 v = vel[i];
+        velh_out[i] = float4_to_half4(make_float4(v.x, v.y, v.z, r));
+    }
+    if constexpr (MIX == MIX_POS16) {
         const float m0 = __ldg(&f.pm[0].w);
         pmh_out[i] = pack_record(f.g, c, me.x, me.y, me.z, me.w / (m0 != 0.f ? m0 : 1.f));
-        velh_out[i] = float4_to_half4(make_float4(v.x, v.y, v.z, r));
     }
 }
 
 // write_non_prs_acc_ff (solver.cuh:40-69): gravity + artificial viscosity;
 // optionally fused with integrate_a_v_only (solver.cu:3-13) into vel_out
 // (and its FP16 copy velh_out under mixed precision)
-template <int KIND, int R, bool MIX = false>
+template <int KIND, int R, int MIX = 0>
 __global__ void __launch_bounds__(NBR_THREADS) k_nonpressure(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const uint2* __restrict__ velh, float nu10, float eps,
     float3 grav, float dt, float4* __restrict__ acc, float4* __restrict__ vel_out,
@@ -563,7 +592,7 @@ __global__ void k_advect(uint32_t n, const float4* __restrict__ pm,
 
 // _compute_diagonal_elem_and_source_term (IISPH.cu:11-66) + warm start
 // (IISPH.cu:193-209)
-template <int KIND, int R, bool MIX = false>
+template <int KIND, int R, int MIX = 0>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const uint2* __restrict__ velh,
     const float4* __restrict__ bterm, float rho0, float dt,
@@ -577,6 +606,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
     float gx = 0.f, gy = 0.f, gz = 0.f, vdiv = 0.f, gsq = 0.f;
+    [[maybe_unused]] Kahan vk; // mixed modes: compensated divergence sum
     for_each_listed<R, MIX>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float4 vj = nbr_vel<MIX>(vel, velh, j);
@@ -585,9 +615,15 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
             gx += mg * dx;
             gy += mg * dy;
             gz += mg * dz;
-            vdiv += mg * fmaf(dx, vi.x - vj.x, fmaf(dy, vi.y - vj.y, dz * (vi.z - vj.z)));
+            const float dv = mg * fmaf(dx, vi.x - vj.x, fmaf(dy, vi.y - vj.y, dz * (vi.z - vj.z)));
+            if constexpr (MIX)
+                vk.add(dv);
+            else
+                vdiv += dv;
             gsq += mg * g * l2;
         });
+    if constexpr (MIX)
+        vdiv = vk.sum;
     const float4 bt = bterm[i];
     gx += bt.x;
     gy += bt.y;
@@ -605,7 +641,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
 // carried pressure, so a_i = -(1/rho0^2)(sum m_j (p_i' + p_j') grad W_ij +
 // p_i' g_b) with p' = 0.5 p can be summed in the same neighbour loop. p_old
 // is read, p_new written (p_new = 0.5 p_old).
-template <int KIND, int R, bool MIX = false>
+template <int KIND, int R, int MIX = 0>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const uint2* __restrict__ velh,
     const float4* __restrict__ bterm, float rho0, float dt,
@@ -621,6 +657,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
     const int3 c = fluid_cell<R>(f, me);
     const float pi = p_old[i] * 0.5f;
     float gx = 0.f, gy = 0.f, gz = 0.f, vdiv = 0.f, gsq = 0.f;
+    [[maybe_unused]] Kahan vk; // mixed modes: compensated divergence sum
     float ax = 0.f, ay = 0.f, az = 0.f;
     for_each_listed<R, MIX>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
@@ -631,13 +668,19 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
             gx += mg * dx;
             gy += mg * dy;
             gz += mg * dz;
-            vdiv += mg * fmaf(dx, vi.x - vj.x, fmaf(dy, vi.y - vj.y, dz * (vi.z - vj.z)));
+            const float dv = mg * fmaf(dx, vi.x - vj.x, fmaf(dy, vi.y - vj.y, dz * (vi.z - vj.z)));
+            if constexpr (MIX)
+                vk.add(dv);
+            else
+                vdiv += dv;
             gsq += mg * g * l2;
             const float sp = q.w * (pi + pj) * g;
             ax += sp * dx;
             ay += sp * dy;
             az += sp * dz;
         });
+    if constexpr (MIX)
+        vdiv = vk.sum;
     const float4 bt = bterm[i];
     const float4 ai = make_float4(-r0i * (ax + pi * bt.x), -r0i * (ay + pi * bt.y),
         -r0i * (az + pi * bt.z), 0.f);
@@ -654,7 +697,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
 }
 
 // _set_pressure_accelerations (IISPH.cu:68-98)
-template <int KIND, int R, bool MIX = false>
+template <int KIND, int R, int MIX = 0>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     float4* __restrict__ acc, uint2* __restrict__ acch_out)
@@ -684,7 +727,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
 // _jacobi_update_pressures (IISPH.cu:119-162); the convergence bitmask of the
 // reference becomes a count of particles above the threshold, reduced per
 // block together with the FP64 sum of max(0, error)
-template <int KIND, int R, bool MIX = false>
+template <int KIND, int R, int MIX = 0>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid f,
     const float4* __restrict__ acc, const float4* __restrict__ bterm,
     const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
@@ -698,8 +741,12 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
         const float4 me = f.pm[i];
         const int3 c = fluid_cell<R>(f, me);
         const float4 ai = acc[i];
+        // mixed: neighbour accelerations arrive scaled by ACC_SCALE; the own
+        // one is scaled to match and the sum scaled back
+        constexpr float AS = MIX ? ACC_SCALE : 1.f;
+        const float3 as = make_float3(ai.x * AS, ai.y * AS, ai.z * AS);
         float sum = 0.f;
-        for_each_listed<R, MIX, MIX>(f, i, c, me,
+        for_each_listed<R, MIX, (MIX != 0)>(f, i, c, me,
             [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
                 float3 aj;
                 if constexpr (MIX) {
@@ -708,9 +755,11 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
                     const float4 a = __ldg(acc + j);
                     aj = make_float3(a.x, a.y, a.z);
                 }
-                const float d = fmaf(ai.x - aj.x, dx, fmaf(ai.y - aj.y, dy, (ai.z - aj.z) * dz));
+                const float d = fmaf(as.x - aj.x, dx, fmaf(as.y - aj.y, dy, (as.z - aj.z) * dz));
                 sum += q.w * (pair_g<KIND>(f.kc, l2) * d);
             });
+        if constexpr (MIX)
+            sum *= 1.f / ACC_SCALE;
         const float4 bt = bterm[i];
         const float Ap = dt * (sum + fmaf(ai.x, bt.x, fmaf(ai.y, bt.y, ai.z * bt.z)));
         const float s = sii[i];
@@ -724,7 +773,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
 }
 
 // final _set_pressure_accelerations + integrate (IISPH.cu:248-257)
-template <int KIND, int R, bool MIX = false>
+template <int KIND, int R, int MIX = 0>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     const float4* __restrict__ vel, float dt, float4* __restrict__ acc,
@@ -849,8 +898,9 @@ static void ensure_buffers(reyn_solver& sv, uint32_t n)
     sv.bterm.resize(n);
     sv.nbr.resize(list_capacity(n));
     sv.ncount.resize(n);
-    if (sv.prm.precision == REYN_PRECISION_MIXED) {
-        sv.pmh.resize(n);
+    if (sv.prm.precision != REYN_PRECISION_FP32) {
+        if (sv.prm.precision == REYN_PRECISION_MIXED_POS16)
+            sv.pmh.resize(n);
         sv.acch.resize(n);
         sv.velh.resize(n);
         sv.velh2.resize(n);
@@ -937,8 +987,8 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     uint32_t iters = 0;
     bool converged = true;
 
-    const bool mixed = P.precision == REYN_PRECISION_MIXED;
-    uint2* PMH = mixed ? sv.pmh.get() : nullptr;
+    const bool mixed = P.precision != REYN_PRECISION_FP32;
+    uint2* PMH = P.precision == REYN_PRECISION_MIXED_POS16 ? sv.pmh.get() : nullptr;
     uint2* ACH = mixed ? sv.acch.get() : nullptr;
     uint2* VH = mixed ? sv.velh.get() : nullptr;
     uint2* VH2 = mixed ? sv.velh2.get() : nullptr;
@@ -947,7 +997,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     auto body = [&](auto KC, auto RC, auto MC) {
         constexpr int K = decltype(KC)::value;
         constexpr int R = decltype(RC)::value;
-        constexpr bool MIX = decltype(MC)::value;
+        constexpr int MIX = decltype(MC)::value;
         REYN_KERNEL("k_density", s,
             k_density<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, b, sv.rho.get(), st.vel.get(),
             sv.bterm.get(), PMH, VH));
@@ -1049,10 +1099,12 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         }
     };
     dispatch(P.kernel, grid.geom.range, [&](auto KC, auto RC) {
-        if (mixed)
-            body(KC, RC, std::true_type {});
+        if (P.precision == REYN_PRECISION_MIXED_POS16)
+            body(KC, RC, std::integral_constant<int, MIX_POS16> {});
+        else if (mixed)
+            body(KC, RC, std::integral_constant<int, MIX_F16> {});
         else
-            body(KC, RC, std::false_type {});
+            body(KC, RC, std::integral_constant<int, 0> {});
     });
     REYN_KERNEL("k_unpack_acc", s,
         k_unpack_acc<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, sv.acc.get(), sv.ax.get(),
