@@ -8,7 +8,8 @@ lambda = 0.4).
 
 A step is one iteration of the reference main loop (main.cu:60-78): dt
 controller (CFL max-velocity reduction), uniform-grid build + reorder of the
-state, IISPH step, hard bounds. Inputs are resident in HBM for `value`; `e2e`
+state, IISPH step, hard bounds; the bounds and the max-velocity reduction run
+inside the step's integrating kernel. Inputs are resident in HBM for `value`; `e2e`
 repeats the step through the C ABI with the state uploaded from and downloaded
 to pinned host memory inside the timed region.
 
@@ -232,12 +233,15 @@ class EngineRun:
     def step(self, S):
         rb, sc = self.rb, self.sc
         # simple_dt_controller (cfl.cu:39-52) at lambda 0.4, capped by the
-        # explicit-viscosity bound
-        self.dt = min(rb.dt_controller(self.st, self.iters, self.dt, LAMBDA, sc.h,
-                                       (0.0, -9.81, 0.0), 10, 0.001, stream=S), self.dt_visc)
+        # explicit-viscosity bound; its max |v| comes from the previous
+        # step's integrating kernel, which also applied the hard bounds
+        # (scene.cu:466-491)
+        self.dt = min(self.sv.next_dt(self.st, self.iters, self.dt, LAMBDA, sc.h,
+                                      (0.0, -9.81, 0.0), 10, 0.001, stream=S), self.dt_visc)
         self.grid.construct_and_reorder(self.st, stream=S)
         try:
-            it = self.sv.step(self.st, self.grid, self.bd, self.dt, stream=S)
+            it = self.sv.step(self.st, self.grid, self.bd, self.dt, stream=S,
+                              bounds=(sc.box_min, sc.box_max))
         except rb.ReynError as e:
             if e.code != rb.ERR_ITER_LIMIT:
                 raise
@@ -245,7 +249,6 @@ class EngineRun:
             self.limit_hits += 1
         self.iters = it
         self.log.append((it, self.sv.stats().avg_density_error, self.dt))
-        rb.enforce_bounds(self.st, sc.box_min, sc.box_max, stream=S)
 
     def checkpoint(self):
         return (self.st.download(), self.sv.pressure(), self.dt, self.iters)

@@ -260,6 +260,18 @@ int reyn_solver_step(reyn_solver* s, reyn_particles* state,
     const reyn_grid* grid, const reyn_boundary* bdy, float dt,
     uint32_t* iters, void* stream);
 
+/* (no counterpart: the reference's main loop, main.cu:64-75, runs the step,
+ * hard_enforce_bounds and the next dt controller's max-velocity reduction
+ * as separate passes) The step with its tail fused: the kernel that writes
+ * the new positions and velocities applies hard_enforce_bounds
+ * (scene.cu:466-491) to them and max-reduces |v| of what it stores. The
+ * result equals reyn_solver_step followed by reyn_enforce_bounds; the
+ * recorded max |v| serves reyn_solver_next_dt. */
+int reyn_solver_step_bounded(reyn_solver* s, reyn_particles* state,
+    const reyn_grid* grid, const reyn_boundary* bdy, float dt,
+    const float bound_min[3], const float bound_max[3], uint32_t* iters,
+    void* stream);
+
 /* per-particle solver buffers (device, grid order of the last step) */
 typedef struct reyn_solver_buffers {
     const float *rho, *p, *aii, *sii, *ax, *ay, *az;
@@ -293,6 +305,14 @@ int reyn_cfl_time_step(reyn_particles* state, float lambda, float h,
 /* simple_dt_controller (cfl.cu:39-52); synchronises the stream */
 int reyn_dt_controller(reyn_particles* state, uint32_t iter_last,
     float dt_last, float lambda, float h, const float g[3],
+    uint32_t iter_target, float change_factor, float* dt_out, void* stream);
+/* simple_dt_controller with the max |v| that the solver's last
+ * reyn_solver_step_bounded reduced, when `state` has not changed through
+ * this library since (otherwise a reduction pass, as reyn_dt_controller).
+ * Writes to the state through raw device pointers are not seen: after such
+ * writes use reyn_dt_controller. Waits for that step's last kernel. */
+int reyn_solver_next_dt(reyn_solver* s, reyn_particles* state,
+    uint32_t iter_last, float dt_last, float lambda, float h, const float g[3],
     uint32_t iter_target, float change_factor, float* dt_out, void* stream);
 
 /* ---- bounds (src/scene/scene.cu:466-491) ---------------------------------- */

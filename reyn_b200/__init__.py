@@ -101,6 +101,10 @@ _SIGNATURES = {
     "reyn_solver_create": [ctypes.c_int, ctypes.POINTER(Params), _u32, ctypes.POINTER(_vp)],
     "reyn_solver_destroy": [_vp],
     "reyn_solver_step": [_vp, _vp, _vp, _vp, _f, ctypes.POINTER(_u32), _vp],
+    "reyn_solver_step_bounded": [_vp, _vp, _vp, _vp, _f, _f * 3, _f * 3, ctypes.POINTER(_u32),
+                                 _vp],
+    "reyn_solver_next_dt": [_vp, _vp, _u32, _f, _f, _f, _f * 3, _u32, _f, ctypes.POINTER(_f),
+                            _vp],
     "reyn_solver_buffers_get": [_vp, ctypes.POINTER(SolverBuffers)],
     "reyn_solver_stats": [_vp, ctypes.POINTER(StepStats)],
     "reyn_cfl_time_step": [_vp, _f, _f, _f * 3, ctypes.POINTER(_f), _vp],
@@ -334,11 +338,28 @@ class Solver:
     __del__ = close
 
     def step(self, state: Particles, grid: Grid, bdy: Optional[Boundary], dt: float,
-             stream=None) -> int:
+             stream=None, bounds=None) -> int:
+        """One step; with bounds=(bmin, bmax) the step also applies the hard
+        bounds in its integrating kernel and records max |v| for next_dt."""
         it = _u32()
-        check(lib().reyn_solver_step(self.h, state.h, grid.h, bdy.h if bdy else None, dt,
-                                     ctypes.byref(it), _stream(stream)))
+        if bounds is None:
+            check(lib().reyn_solver_step(self.h, state.h, grid.h, bdy.h if bdy else None, dt,
+                                         ctypes.byref(it), _stream(stream)))
+        else:
+            check(lib().reyn_solver_step_bounded(self.h, state.h, grid.h,
+                                                 bdy.h if bdy else None, dt, _f3(bounds[0]),
+                                                 _f3(bounds[1]), ctypes.byref(it),
+                                                 _stream(stream)))
         return it.value
+
+    def next_dt(self, state: Particles, iter_last: int, dt_last: float, lam: float, h: float,
+                g, iter_target: int = 5, change: float = 0.01, stream=None) -> float:
+        """simple_dt_controller on the max |v| of the last bounded step."""
+        dt = _f()
+        check(lib().reyn_solver_next_dt(self.h, state.h, iter_last, dt_last, lam, h, _f3(g),
+                                        iter_target, change, ctypes.byref(dt),
+                                        _stream(stream)))
+        return dt.value
 
     def buffers(self) -> SolverBuffers:
         b = SolverBuffers()

@@ -118,6 +118,7 @@ int reyn_particles_upload(reyn_particles* p, const float* xx, const float* xy, c
                 REYN_CUDA(cudaMemcpyAsync(p->cur[k].get(), src[k], size_t(p->n) * sizeof(float),
                     cudaMemcpyHostToDevice, s));
         p->packed_valid = false;
+        p->version += 1;
     });
 }
 
@@ -332,18 +333,23 @@ int reyn_solver_destroy(reyn_solver* s)
     return guard([&] { delete s; });
 }
 
-int reyn_solver_step(reyn_solver* s, reyn_particles* state, const reyn_grid* grid,
-    const reyn_boundary* bdy, float dt, uint32_t* iters, void* stream)
+static int step_impl(reyn_solver* s, reyn_particles* state, const reyn_grid* grid,
+    const reyn_boundary* bdy, float dt, const float* bmin, const float* bmax, uint32_t* iters,
+    void* stream)
 {
     return guard([&] {
         require(s && state && grid, "null argument");
+        if (bmin || bmax) {
+            check_vec3(bmin, "bound_min must be 3 finite floats");
+            check_vec3(bmax, "bound_max must be 3 finite floats");
+        }
         const cudaStream_t st = as_stream(stream);
         if (iters)
             *iters = 0;
         int code = REYN_OK;
         std::string msg;
         try {
-            solver_step(*s, *state, *grid, bdy, dt, st);
+            solver_step(*s, *state, *grid, bdy, dt, st, bmin, bmax);
         } catch (const Error& e) {
             if (e.code != REYN_ERR_ITER_LIMIT)
                 throw;
@@ -356,6 +362,23 @@ int reyn_solver_step(reyn_solver* s, reyn_particles* state, const reyn_grid* gri
         if (code)
             fail(code, msg);
     });
+}
+
+int reyn_solver_step(reyn_solver* s, reyn_particles* state, const reyn_grid* grid,
+    const reyn_boundary* bdy, float dt, uint32_t* iters, void* stream)
+{
+    return step_impl(s, state, grid, bdy, dt, nullptr, nullptr, iters, stream);
+}
+
+int reyn_solver_step_bounded(reyn_solver* s, reyn_particles* state, const reyn_grid* grid,
+    const reyn_boundary* bdy, float dt, const float bound_min[3], const float bound_max[3],
+    uint32_t* iters, void* stream)
+{
+    if (!bound_min || !bound_max) {
+        set_last_error("null bounds");
+        return REYN_ERR_INVALID;
+    }
+    return step_impl(s, state, grid, bdy, dt, bound_min, bound_max, iters, stream);
 }
 
 int reyn_solver_buffers_get(const reyn_solver* s, reyn_solver_buffers* out)
@@ -424,6 +447,17 @@ int reyn_cfl_time_step(reyn_particles* state, float lambda, float h, const float
     });
 }
 
+// simple_dt_controller, cfl.cu:39-52
+static float dt_controller(reyn_solver* sv, reyn_particles& st, uint32_t iter_last,
+    float dt_last, float lambda, float h, const float g[3], uint32_t iter_target,
+    float change_factor, cudaStream_t s)
+{
+    const float f = iter_last < iter_target ? 1.f + change_factor : 1.f - change_factor;
+    const float suggested = dt_last * f;
+    const float cfl = cfl_time_step(st, lambda, h, g, s, sv);
+    return std::min(cfl, suggested);
+}
+
 int reyn_dt_controller(reyn_particles* state, uint32_t iter_last, float dt_last, float lambda,
     float h, const float g[3], uint32_t iter_target, float change_factor, float* dt_out,
     void* stream)
@@ -431,11 +465,20 @@ int reyn_dt_controller(reyn_particles* state, uint32_t iter_last, float dt_last,
     return guard([&] {
         require(state && dt_out, "null argument");
         check_vec3(g, "gravity must be 3 finite floats");
-        // simple_dt_controller, cfl.cu:39-52
-        const float f = iter_last < iter_target ? 1.f + change_factor : 1.f - change_factor;
-        const float suggested = dt_last * f;
-        const float cfl = cfl_time_step(*state, lambda, h, g, as_stream(stream));
-        *dt_out = std::min(cfl, suggested);
+        *dt_out = dt_controller(nullptr, *state, iter_last, dt_last, lambda, h, g, iter_target,
+            change_factor, as_stream(stream));
+    });
+}
+
+int reyn_solver_next_dt(reyn_solver* s, reyn_particles* state, uint32_t iter_last,
+    float dt_last, float lambda, float h, const float g[3], uint32_t iter_target,
+    float change_factor, float* dt_out, void* stream)
+{
+    return guard([&] {
+        require(s && state && dt_out, "null argument");
+        check_vec3(g, "gravity must be 3 finite floats");
+        *dt_out = dt_controller(s, *state, iter_last, dt_last, lambda, h, g, iter_target,
+            change_factor, as_stream(stream));
     });
 }
 

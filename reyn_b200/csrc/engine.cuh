@@ -81,7 +81,8 @@ struct reyn_particles {
     reyn::DevArray<float4> pm;  // (x, y, z, m) in grid order
     reyn::DevArray<float4> vel; // (vx, vy, vz, rho)
     bool packed_valid = false;
-    uint64_t epoch = 0; // number of reorders applied
+    uint64_t epoch = 0;   // number of reorders applied
+    uint64_t version = 0; // changes through this library (uploads, reorders, steps, bounds)
 };
 
 struct reyn_grid : reyn::Grid { };
@@ -113,6 +114,18 @@ struct reyn_solver {
     const reyn_particles* p_state = nullptr;
     reyn_step_stats stats {};
     double pcisph_delta = 0.0; // k_c_pcisph template stiffness
+    // max |v| after the last bounded step, for the next dt controller
+    reyn::DevArray<float> vmax;
+    std::unique_ptr<reyn::PinnedArray<float>> vmax_host;
+    cudaEvent_t vmax_ready = nullptr;
+    const reyn_particles* vmax_state = nullptr;
+    uint64_t vmax_version = 0;
+    bool vmax_valid = false;
+    ~reyn_solver()
+    {
+        if (vmax_ready)
+            cudaEventDestroy(vmax_ready);
+    }
 };
 
 namespace reyn {
@@ -147,11 +160,19 @@ void boundary_build(reyn_boundary& b, const float* bx, const float* by,
     const float* bz, const float* bm, uint32_t nb, float h, float rho0,
     uint32_t mass_iters, cudaStream_t s);
 
+// one step; with bounds (bmin and bmax not null) the step also applies
+// hard_enforce_bounds and records max |v| in sv.vmax (step tail fusion)
 void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& g,
-    const reyn_boundary* bdy, float dt, cudaStream_t s);
+    const reyn_boundary* bdy, float dt, cudaStream_t s, const float* bmin = nullptr,
+    const float* bmax = nullptr);
 
+// max |v| over the state: the recorded value of the solver's last bounded
+// step when the state has not changed since, else a reduction pass
+float state_vmax(reyn_solver* sv, reyn_particles& st, cudaStream_t s);
+
+// cfl_time_step (cfl.cu:5-37); max |v| from state_vmax(sv, st)
 float cfl_time_step(reyn_particles& st, float lambda, float h,
-    const float g[3], cudaStream_t s);
+    const float g[3], cudaStream_t s, reyn_solver* sv = nullptr);
 
 void enforce_bounds(reyn_particles& st, const float lo[3], const float hi[3],
     cudaStream_t s);

@@ -428,6 +428,7 @@ void reorder_state(reyn_particles& st, Grid& g, float* const* extra, uint32_t n_
         st.cur[k].swap(st.alt[k]);
     st.packed_valid = true;
     st.epoch += 1;
+    st.version += 1;
     g.reordered = true;
     g.reordered_state = &st;
     g.reorder_epoch = st.epoch;

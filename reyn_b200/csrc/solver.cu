@@ -358,6 +358,66 @@ __device__ __forceinline__ void block_accumulate(SweepStats* st, unsigned over, 
     }
 }
 
+// ---- step tail ---------------------------------------------------------------
+// The reference's main loop follows every step with hard_enforce_bounds
+// (scene.cu:466-483) and starts the next with simple_dt_controller, whose CFL
+// part reduces max |v| over the state (cfl.cu:5-37). A bounded step does both
+// in the kernel that writes the new state: the bounds are applied to each
+// particle's new position and velocity before they are stored, and the
+// norm of the stored velocity is max-reduced into `vmax`.
+struct Tail {
+    float3 lo, hi;
+    float* vmax; // nullptr: no bounds, no reduction (the plain step)
+};
+
+// stores the new state of particle i (bounds applied when tail.vmax is set)
+// and returns |v| of what was stored
+__device__ __forceinline__ float store_state(const Tail& t, uint32_t i, float px, float py,
+    float pz, float nvx, float nvy, float nvz, float* __restrict__ x, float* __restrict__ y,
+    float* __restrict__ z, float* __restrict__ vx, float* __restrict__ vy,
+    float* __restrict__ vz)
+{
+    if (t.vmax) {
+        // _hard_enforce_bounds, scene.cu:466-483
+        if (px <= t.lo.x || py <= t.lo.y || pz <= t.lo.z || t.hi.x <= px || t.hi.y <= py
+            || t.hi.z <= pz) {
+            const float d = (float)-0.1;
+            nvx = nvx * d;
+            nvy = nvy * d;
+            nvz = nvz * d;
+        }
+        px = fmaxf(fminf(px, t.hi.x), t.lo.x);
+        py = fmaxf(fminf(py, t.hi.y), t.lo.y);
+        pz = fmaxf(fminf(pz, t.hi.z), t.lo.z);
+    }
+    vx[i] = nvx;
+    vy[i] = nvy;
+    vz[i] = nvz;
+    x[i] = px;
+    y[i] = py;
+    z[i] = pz;
+    return t.vmax ? norm3df(nvx, nvy, nvz) : 0.f; // cfl.cu:13-18
+}
+
+// block maximum of v into *t.vmax (all threads of the block call this)
+__device__ __forceinline__ void tail_reduce(const Tail& t, float v)
+{
+    if (!t.vmax)
+        return;
+    __shared__ float s_max[32];
+    v = warp_max(v);
+    if ((threadIdx.x & 31) == 0)
+        s_max[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (unsigned w = 1; w < (blockDim.x + 31) / 32; ++w)
+            v = fmaxf(v, s_max[w]);
+        // most blocks find a larger maximum already there: skip their atomic
+        if (v > __ldcg(t.vmax))
+            atomic_max_nonneg(t.vmax, v);
+    }
+}
+
 // ---- passes ----------------------------------------------------------------
 
 // compute_densities (solver.cuh:18-38) + cached boundary sums + the step's
@@ -465,11 +525,11 @@ __global__ void __launch_bounds__(NBR_THREADS) k_sesph(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const float4* __restrict__ bterm, float k, float rho0,
     float nu10, float eps, float3 grav, float dt, float4* __restrict__ acc,
     float* __restrict__ x, float* __restrict__ y, float* __restrict__ z,
-    float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz)
+    float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz, Tail tail)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
+    float vn = 0.f;
+    if (i < n) {
     const float4 me = f.pm[i];
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
@@ -494,12 +554,10 @@ __global__ void __launch_bounds__(NBR_THREADS) k_sesph(uint32_t n, Fluid f,
     az -= pri * bt.z;
     acc[i] = make_float4(ax, ay, az, 0.f);
     const float nvx = vi.x + dt * ax, nvy = vi.y + dt * ay, nvz = vi.z + dt * az;
-    vx[i] = nvx;
-    vy[i] = nvy;
-    vz[i] = nvz;
-    x[i] = me.x + dt * nvx;
-    y[i] = me.y + dt * nvy;
-    z[i] = me.z + dt * nvz;
+    vn = store_state(tail, i, me.x + dt * nvx, me.y + dt * nvy, me.z + dt * nvz, nvx, nvy, nvz,
+        x, y, z, vx, vy, vz);
+    }
+    tail_reduce(tail, vn);
 }
 
 // predict_rho (solver.cuh:71-105); the boundary part uses the cached sums:
@@ -575,19 +633,17 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_pressure(uint32_t n, Flu
 __global__ void k_advect(uint32_t n, const float4* __restrict__ pm,
     const float4* __restrict__ vel, float dt, float* __restrict__ x, float* __restrict__ y,
     float* __restrict__ z, float* __restrict__ vx, float* __restrict__ vy,
-    float* __restrict__ vz)
+    float* __restrict__ vz, Tail tail)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    const float4 p = pm[i];
-    const float4 v = vel[i];
-    vx[i] = v.x;
-    vy[i] = v.y;
-    vz[i] = v.z;
-    x[i] = p.x + dt * v.x;
-    y[i] = p.y + dt * v.y;
-    z[i] = p.z + dt * v.z;
+    float vn = 0.f;
+    if (i < n) {
+        const float4 p = pm[i];
+        const float4 v = vel[i];
+        vn = store_state(tail, i, p.x + dt * v.x, p.y + dt * v.y, p.z + dt * v.z, v.x, v.y, v.z,
+            x, y, z, vx, vy, vz);
+    }
+    tail_reduce(tail, vn);
 }
 
 // _compute_diagonal_elem_and_source_term (IISPH.cu:11-66) + warm start
@@ -778,11 +834,11 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     const float4* __restrict__ vel, float dt, float4* __restrict__ acc,
     float* __restrict__ x, float* __restrict__ y, float* __restrict__ z,
-    float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz)
+    float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz, Tail tail)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
+    float vn = 0.f;
+    if (i < n) {
     const float4 me = f.pm[i];
     const int3 c = fluid_cell<R>(f, me);
     const float pi = p[i];
@@ -801,12 +857,10 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f
     acc[i] = make_float4(ax, ay, az, 0.f);
     const float4 v = vel[i];
     const float nvx = v.x + dt * ax, nvy = v.y + dt * ay, nvz = v.z + dt * az;
-    vx[i] = nvx;
-    vy[i] = nvy;
-    vz[i] = nvz;
-    x[i] = me.x + dt * nvx;
-    y[i] = me.y + dt * nvy;
-    z[i] = me.z + dt * nvz;
+    vn = store_state(tail, i, me.x + dt * nvx, me.y + dt * nvy, me.z + dt * nvz, nvx, nvy, nvz,
+        x, y, z, vx, vy, vz);
+    }
+    tail_reduce(tail, vn);
 }
 
 __global__ void k_unpack_acc(uint32_t n, const float4* __restrict__ acc, float* __restrict__ ax,
@@ -918,10 +972,11 @@ static void ensure_buffers(reyn_solver& sv, uint32_t n)
 }
 
 void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
-    const reyn_boundary* bdy, float dt, cudaStream_t s)
+    const reyn_boundary* bdy, float dt, cudaStream_t s, const float* bmin, const float* bmax)
 {
     const reyn_params& P = sv.prm;
     const uint32_t n = st.n;
+    sv.vmax_valid = false;
     require(n == sv.n, "particle count differs from the solver's");
     require(dt > 0.f && std::isfinite(dt), "dt must be positive and finite");
     if (!(grid.reordered && grid.reordered_state == &st && grid.reorder_epoch == st.epoch
@@ -966,6 +1021,18 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         b.near = bdy->near.get();
         b.n = bdy->nb;
     }
+    Tail tail {};
+    if (bmin && bmax) {
+        if (sv.vmax.size() == 0) {
+            sv.vmax.resize(1);
+            sv.vmax_host = std::make_unique<PinnedArray<float>>(1);
+            REYN_CUDA(cudaEventCreateWithFlags(&sv.vmax_ready, cudaEventDisableTiming));
+        }
+        REYN_CUDA(cudaMemsetAsync(sv.vmax.get(), 0, sizeof(float), s));
+        tail.lo = make_float3(bmin[0], bmin[1], bmin[2]);
+        tail.hi = make_float3(bmax[0], bmax[1], bmax[2]);
+        tail.vmax = sv.vmax.get();
+    }
     const unsigned nb = blocks_for(n, NBR_THREADS);
     const float rho0 = P.rho0;
     const float r0i = 1.f / (rho0 * rho0);
@@ -1004,7 +1071,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         if (sv.scheme == REYN_SESPH) {
             REYN_KERNEL("k_sesph", s,
                 k_sesph<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), sv.bterm.get(),
-                P.k_sesph, rho0, nu10, eps, grav, dt, sv.acc.get(), X, Y, Z, VX, VY, VZ));
+                P.k_sesph, rho0, nu10, eps, grav, dt, sv.acc.get(), X, Y, Z, VX, VY, VZ, tail));
             iters = 1;
         } else if (sv.scheme == REYN_PCISPH) {
             const float kp = (float)((sv.pcisph_delta / dt) / dt); // PCISPH.cu:65
@@ -1039,7 +1106,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             }
             REYN_KERNEL("k_advect", s,
                 k_advect<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, st.pm.get(), v, dt, X, Y, Z,
-                VX, VY, VZ));
+                VX, VY, VZ, tail));
         } else { // IISPH
             REYN_KERNEL("k_nonpressure", s,
                 k_nonpressure<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), VH, nu10,
@@ -1095,7 +1162,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             }
             REYN_KERNEL("k_iisph_final", s,
                 k_iisph_final<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
-                r0i, sv.vel2.get(), dt, sv.acc.get(), X, Y, Z, VX, VY, VZ));
+                r0i, sv.vel2.get(), dt, sv.acc.get(), X, Y, Z, VX, VY, VZ, tail));
         }
     };
     dispatch(P.kernel, grid.geom.range, [&](auto KC, auto RC) {
@@ -1110,6 +1177,15 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         k_unpack_acc<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, sv.acc.get(), sv.ax.get(),
         sv.ay.get(), sv.az.get()));
     st.packed_valid = false; // positions moved: the packed copy is stale
+    st.version += 1;
+    if (tail.vmax) {
+        REYN_CUDA(cudaMemcpyAsync(sv.vmax_host->get(), tail.vmax, sizeof(float),
+            cudaMemcpyDeviceToHost, s));
+        REYN_CUDA(cudaEventRecord(sv.vmax_ready, s));
+        sv.vmax_state = &st;
+        sv.vmax_version = st.version;
+        sv.vmax_valid = true;
+    }
     sv.stats.iters = iters;
     if (!converged)
         fail(REYN_ERR_ITER_LIMIT, "solver reached max_iter before converging (step completed)");
@@ -1135,8 +1211,12 @@ __global__ void k_vmax(uint32_t n, const float* __restrict__ vx, const float* __
     }
 }
 
-float cfl_time_step(reyn_particles& st, float lambda, float h, const float g[3], cudaStream_t s)
+float state_vmax(reyn_solver* sv, reyn_particles& st, cudaStream_t s)
 {
+    if (sv && sv->vmax_valid && sv->vmax_state == &st && sv->vmax_version == st.version) {
+        REYN_CUDA(cudaEventSynchronize(sv->vmax_ready));
+        return *sv->vmax_host->get();
+    }
     DevArray<float> d(1);
     d.zero(s);
     if (st.n) {
@@ -1147,6 +1227,13 @@ float cfl_time_step(reyn_particles& st, float lambda, float h, const float g[3],
     float vmax = 0.f;
     REYN_CUDA(cudaMemcpyAsync(&vmax, d.get(), sizeof(float), cudaMemcpyDeviceToHost, s));
     REYN_CUDA(cudaStreamSynchronize(s));
+    return vmax;
+}
+
+float cfl_time_step(reyn_particles& st, float lambda, float h, const float g[3], cudaStream_t s,
+    reyn_solver* sv)
+{
+    const float vmax = state_vmax(sv, st, s);
     // cfl.cu:22-36
     const float dt_vel = lambda * h / vmax;
     const float gn = (float)std::sqrt((double)std::fmaf(g[0], g[0], std::fmaf(g[1], g[1], g[2] * g[2])));
@@ -1184,6 +1271,7 @@ void enforce_bounds(reyn_particles& st, const float lo[3], const float hi[3], cu
         st.cur[FY].get(), st.cur[FZ].get(), st.cur[FVX].get(), st.cur[FVY].get(),
         st.cur[FVZ].get()));
     st.packed_valid = false;
+    st.version += 1;
 }
 
 } // namespace reyn
