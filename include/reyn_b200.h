@@ -84,6 +84,17 @@ int reyn_particles_upload(reyn_particles* p, const float* xx, const float* xy,
     const float* m, void* stream);
 int reyn_particles_download(reyn_particles* p, float* xx, float* xy,
     float* xz, float* vx, float* vy, float* vz, float* m, void* stream);
+/* save_to_ply (ply_io.cu:7-55): the positions as a binary PLY point cloud
+ * (header: format binary_<native>_endian 1.0, element vertex n, float32
+ * properties x, y, z; payload x y z per particle). Synchronises the stream. */
+int reyn_particles_save_ply(reyn_particles* p, const char* path, void* stream);
+/* (no counterpart in the reference) the whole state as a raw dump for
+ * checkpoints: 8-byte magic "REYNSOA1", uint32 n, float rho0, uint32 field
+ * count (7), then xx, xy, xz, vx, vy, vz, m as n native-endian floats each.
+ * load_raw requires a file with this state's particle count. Both
+ * synchronise the stream. */
+int reyn_particles_save_raw(reyn_particles* p, const char* path, void* stream);
+int reyn_particles_load_raw(reyn_particles* p, const char* path, void* stream);
 
 /* ---- uniform grid (src/datastructure/uniformgrid.cuh:200-489) ----------- */
 typedef struct reyn_grid reyn_grid;

@@ -23,6 +23,7 @@
 #include "solvers/PCISPH.cuh"
 #include "solvers/IISPH.cuh"
 #include "timestep/cfl.cuh"
+#include "scene/ply_io.cuh"
 
 #include <thrust/copy.h>
 #include <cstring>
@@ -301,6 +302,18 @@ int ref_cfl(uint N, const float* vx, const float* vy, const float* vz,
         to_dev(state.vy, vy, N);
         to_dev(state.vz, vz, N);
         *dt_out = cfl_time_step(lambda, h, state, v3(g[0], g[1], g[2]));
+    });
+}
+
+/// save_to_ply (ply_io.cu:7-55) on the given positions.
+int ref_save_ply(uint N, const float* x, const float* y, const float* z, const char* path)
+{
+    return guarded([&] {
+        DeviceBuffer<float> xs(N), ys(N), zs(N);
+        to_dev(xs, x, N);
+        to_dev(ys, y, N);
+        to_dev(zs, z, N);
+        save_to_ply(path, xs, ys, zs);
     });
 }
 

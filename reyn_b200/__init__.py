@@ -100,6 +100,9 @@ _SIGNATURES = {
     "reyn_params_reference": [ctypes.c_int, ctypes.c_int, _f, _f, _f, ctypes.POINTER(Params)],
     "reyn_solver_create": [ctypes.c_int, ctypes.POINTER(Params), _u32, ctypes.POINTER(_vp)],
     "reyn_solver_destroy": [_vp],
+    "reyn_particles_save_ply": [_vp, ctypes.c_char_p, _vp],
+    "reyn_particles_save_raw": [_vp, ctypes.c_char_p, _vp],
+    "reyn_particles_load_raw": [_vp, ctypes.c_char_p, _vp],
     "reyn_solver_step": [_vp, _vp, _vp, _vp, _f, ctypes.POINTER(_u32), _vp],
     "reyn_solver_step_bounded": [_vp, _vp, _vp, _vp, _f, _f * 3, _f * 3, ctypes.POINTER(_u32),
                                  _vp],
@@ -215,6 +218,16 @@ class Particles:
                                                       ("x", "y", "z", "vx", "vy", "vz", "m")],
                                             _stream(stream)))
         return out
+
+    def save_ply(self, path: str, stream=None) -> None:
+        """save_to_ply (reference ply_io.cu:7-55): positions as binary PLY."""
+        check(lib().reyn_particles_save_ply(self.h, os.fsencode(path), _stream(stream)))
+
+    def save_raw(self, path: str, stream=None) -> None:
+        check(lib().reyn_particles_save_raw(self.h, os.fsencode(path), _stream(stream)))
+
+    def load_raw(self, path: str, stream=None) -> None:
+        check(lib().reyn_particles_load_raw(self.h, os.fsencode(path), _stream(stream)))
 
 
 class Grid:
