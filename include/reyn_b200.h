@@ -330,6 +330,40 @@ int reyn_solver_next_dt(reyn_solver* s, reyn_particles* state,
 int reyn_enforce_bounds(reyn_particles* state, const float bound_min[3],
     const float bound_max[3], void* stream);
 
+/* ---- scene generation (src/scene/scene.cu) ------------------------------- */
+/* _init_box_kernel (scene.cu:14-37) with seeded jitter (scene.cu:232-253):
+ * particles first .. first + nx*ny*nz - 1 of the state become a lattice of
+ * spacing `spacing` from `origin`, x fastest, each coordinate moved by a
+ * uniform jitter in [-jitter, jitter] * spacing and each velocity component
+ * uniform in [-velocity_noise, velocity_noise]. The random numbers are
+ * counter-based (SplitMix64 of seed and particle index), so the result does
+ * not depend on the launch and is reproducible on the host. mass <= 0 gives
+ * the reference's rest mass rho0 spacing^3. */
+int reyn_scene_fluid_block(reyn_particles* p, uint32_t first,
+    const uint32_t counts[3], const float origin[3], float spacing, float mass,
+    float jitter, float velocity_noise, uint64_t seed, void* stream);
+/* (no counterpart in the reference, which samples boundaries from meshes,
+ * sample_boundary.cu:100-248) one layer of boundary samples on the six faces
+ * of an axis-aligned box, n = rint(extent / spacing) intervals per axis, no
+ * duplicates at edges and corners. *count receives the number of samples;
+ * with x == NULL nothing is written (size query). x, y, z: device arrays. */
+int reyn_scene_box_walls(const float bound_min[3], const float bound_max[3],
+    float spacing, float* x, float* y, float* z, uint64_t capacity,
+    uint64_t* count, void* stream);
+/* (no counterpart in the reference) a sphere sampled by the golden-angle
+ * (Fibonacci) spiral, max(1, rint(4 pi r^2 / spacing^2)) samples; size query
+ * with x == NULL as above. */
+int reyn_scene_sphere(const float center[3], float radius, float spacing,
+    float* x, float* y, float* z, uint32_t capacity, uint32_t* count,
+    void* stream);
+/* the reference's cull of fluid particles too close to the boundary
+ * (CullPredicate + remove_if, scene.cu:59-83, 176-205): removes, keeping the
+ * order of the rest, every particle with a boundary sample within `radius`
+ * (at most the boundary grid's search radius 2h); the state's particle count
+ * shrinks to *n_out. Synchronises the stream. */
+int reyn_scene_cull(reyn_particles* p, const reyn_boundary* bdy, float radius,
+    uint32_t* n_out, void* stream);
+
 /* ---- launch accounting (no counterpart in the reference, which has no
  * tracing): per-kernel launch counts and CUDA-event device time ----------- */
 typedef struct reyn_profile_entry {

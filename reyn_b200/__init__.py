@@ -103,6 +103,12 @@ _SIGNATURES = {
     "reyn_particles_save_ply": [_vp, ctypes.c_char_p, _vp],
     "reyn_particles_save_raw": [_vp, ctypes.c_char_p, _vp],
     "reyn_particles_load_raw": [_vp, ctypes.c_char_p, _vp],
+    "reyn_scene_fluid_block": [_vp, _u32, _u32 * 3, _f * 3, _f, _f, _f, _f, ctypes.c_uint64,
+                               _vp],
+    "reyn_scene_box_walls": [_f * 3, _f * 3, _f, _vp, _vp, _vp, ctypes.c_uint64,
+                             ctypes.POINTER(ctypes.c_uint64), _vp],
+    "reyn_scene_sphere": [_f * 3, _f, _f, _vp, _vp, _vp, _u32, ctypes.POINTER(_u32), _vp],
+    "reyn_scene_cull": [_vp, _vp, _f, ctypes.POINTER(_u32), _vp],
     "reyn_solver_step": [_vp, _vp, _vp, _vp, _f, ctypes.POINTER(_u32), _vp],
     "reyn_solver_step_bounded": [_vp, _vp, _vp, _vp, _f, _f * 3, _f * 3, ctypes.POINTER(_u32),
                                  _vp],
@@ -411,6 +417,54 @@ def dt_controller(state: Particles, iter_last: int, dt_last: float, lam: float, 
 
 def enforce_bounds(state: Particles, bmin, bmax, stream=None) -> None:
     check(lib().reyn_enforce_bounds(state.h, _f3(bmin), _f3(bmax), _stream(stream)))
+
+
+# ---- scene generation on the device ---------------------------------------------
+
+def scene_fluid_block(state: Particles, counts, origin, spacing: float, mass: float = 0.0,
+                      jitter: float = 0.0, velocity_noise: float = 0.0, seed: int = 1,
+                      first: int = 0, stream=None) -> None:
+    """Lattice + seeded jitter into particles first .. first + prod(counts) - 1."""
+    check(lib().reyn_scene_fluid_block(state.h, first, (_u32 * 3)(*counts), _f3(origin),
+                                       spacing, mass, jitter, velocity_noise, seed,
+                                       _stream(stream)))
+
+
+def _device_f32(n: int):
+    import torch
+    return [torch.empty(max(n, 1), dtype=torch.float32, device="cuda") for _ in range(3)]
+
+
+def scene_box_walls(bmin, bmax, spacing: float, stream=None):
+    """Box-wall samples as three device tensors."""
+    cnt = ctypes.c_uint64()
+    check(lib().reyn_scene_box_walls(_f3(bmin), _f3(bmax), spacing, None, None, None, 0,
+                                     ctypes.byref(cnt), None))
+    x, y, z = _device_f32(cnt.value)
+    check(lib().reyn_scene_box_walls(_f3(bmin), _f3(bmax), spacing, x.data_ptr(), y.data_ptr(),
+                                     z.data_ptr(), cnt.value, ctypes.byref(cnt),
+                                     _stream(stream)))
+    return x[:cnt.value], y[:cnt.value], z[:cnt.value]
+
+
+def scene_sphere(center, radius: float, spacing: float, stream=None):
+    """Fibonacci-sphere samples as three device tensors."""
+    cnt = _u32()
+    check(lib().reyn_scene_sphere(_f3(center), radius, spacing, None, None, None, 0,
+                                  ctypes.byref(cnt), None))
+    x, y, z = _device_f32(cnt.value)
+    check(lib().reyn_scene_sphere(_f3(center), radius, spacing, x.data_ptr(), y.data_ptr(),
+                                  z.data_ptr(), cnt.value, ctypes.byref(cnt), _stream(stream)))
+    return x[:cnt.value], y[:cnt.value], z[:cnt.value]
+
+
+def scene_cull(state: Particles, bdy: Boundary, radius: float, stream=None) -> int:
+    """Removes fluid particles within `radius` of a boundary sample; returns
+    the new particle count (the state shrinks)."""
+    n = _u32()
+    check(lib().reyn_scene_cull(state.h, bdy.h, radius, ctypes.byref(n), _stream(stream)))
+    state.n = n.value
+    return n.value
 
 
 def profile_enable(on: bool = True) -> None:

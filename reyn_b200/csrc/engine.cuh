@@ -142,6 +142,11 @@ struct GatherArgs {
 void launch_gather(uint32_t n, const uint32_t* perm, const GatherArgs& a,
     cudaStream_t s);
 
+// exclusive prefix sum of C counts into out[0..C] (out[C] = total); `part`
+// holds the per-tile partials
+void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& part, uint32_t* out,
+    cudaStream_t s);
+
 // packs the particle arrays into pm/vel (after a direct SoA write)
 void pack_state(reyn_particles& st, cudaStream_t s);
 

@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(
         out[C] = part[nparts];
 }
 
-static void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& part,
+void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& part,
     uint32_t* out, cudaStream_t s)
 {
     const uint32_t nparts = (uint32_t)((C + SCAN_TILE - 1) / SCAN_TILE);

@@ -8,8 +8,10 @@ IISPH.cuh:37). Fluid masses are rho0 h^3 (the reference's _init_box_kernel,
 scene.cu:14-37). Boundary masses are left to the Akinci refinement
 (calculate_boundary_masses, sample_boundary.cu:267-297).
 
-The generator is numpy with a PCG64 seed, so every machine builds the same
-scene bit for bit.
+The generator is numpy with counter-based random numbers (SplitMix64 of the
+seed and the particle index), so every machine builds the same scene bit for
+bit, and the GPU generator (reyn_scene_fluid_block, reyn_scene_box_walls)
+writes the same arrays on the device.
 """
 from __future__ import annotations
 
@@ -40,13 +42,19 @@ class Scene:
 
 def box_walls(box_min, box_max, spacing: float) -> dict:
     """One layer of samples on the six faces of an axis-aligned box, on a
-    square lattice of the given spacing (no duplicates at edges/corners)."""
-    lo = np.asarray(box_min, np.float64)
-    hi = np.asarray(box_max, np.float64)
-    n = np.rint((hi - lo) / spacing).astype(np.int64)
+    square lattice of n = rint((hi - lo) / spacing) intervals per axis (no
+    duplicates at edges/corners): the x faces (all j, k), the y faces
+    (interior i), the z faces (interior i, j), the first index slowest;
+    sample (i, j, k) at lo + (i, j, k) * step, step = (hi - lo) / n, in
+    float32 arithmetic (the same samples reyn_scene_box_walls writes on the
+    GPU)."""
+    lo = np.asarray(box_min, np.float32)
+    hi = np.asarray(box_max, np.float32)
+    ext = hi - lo
+    n = np.rint(ext.astype(np.float64) / float(spacing)).astype(np.int64)
+    step = ext / n.astype(np.float32)
     axes = [np.arange(k + 1) for k in n]
     pts = []
-    # x faces (full), y faces (x interior), z faces (x, y interior)
     for ix in (0, n[0]):
         j, k = np.meshgrid(axes[1], axes[2], indexing="ij")
         pts.append(np.stack([np.full(j.size, ix), j.ravel(), k.ravel()], 1))
@@ -56,10 +64,33 @@ def box_walls(box_min, box_max, spacing: float) -> dict:
     for iz in (0, n[2]):
         i, j = np.meshgrid(axes[0][1:-1], axes[1][1:-1], indexing="ij")
         pts.append(np.stack([i.ravel(), j.ravel(), np.full(i.size, iz)], 1))
-    p = np.concatenate(pts, 0).astype(np.float64)
-    xyz = lo + p * ((hi - lo) / n)
-    return {"x": xyz[:, 0].astype(np.float32), "y": xyz[:, 1].astype(np.float32),
-            "z": xyz[:, 2].astype(np.float32)}
+    p = np.concatenate(pts, 0).astype(np.float32)
+    xyz = lo + p * step
+    return {"x": xyz[:, 0].copy(), "y": xyz[:, 1].copy(), "z": xyz[:, 2].copy()}
+
+
+# counter-based random numbers shared with the GPU scene generator: value k of
+# stream t under seed s is SplitMix64(s + 0x9E3779B97F4A7C15 * (t * 2^40 + k + 1)),
+# its top 24 bits an exact float in [0, 1)
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+
+
+def _splitmix64(z: np.ndarray) -> np.ndarray:
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def uniform01(seed: int, stream: int, k: np.ndarray) -> np.ndarray:
+    """float32 uniforms in [0, 1) of `stream` at counters k."""
+    with np.errstate(over="ignore"):
+        c = (np.uint64(stream) << np.uint64(40)) + k.astype(np.uint64) + np.uint64(1)
+        z = _splitmix64(np.uint64(seed) + _GOLDEN * c)
+    return (z >> np.uint64(40)).astype(np.uint32).astype(np.float32) * np.float32(1.0 / 16777216.0)
+
+
+def _symmetric(u: np.ndarray, a: np.float32) -> np.ndarray:
+    return (np.float32(2.0) * u - np.float32(1.0)) * a
 
 
 _ALPHA = {"C2": 21.0 / (2.0 * np.pi), "B3": 16.0 / np.pi, "W6": 1365.0 / (64.0 * np.pi),
@@ -90,28 +121,39 @@ def lattice_density_factor(kernel: str) -> float:
 
 
 def fluid_block(counts, h: float, origin, rho0: float, jitter: float, seed: int,
-                velocity_noise: float = 0.0, mass_kernel: str | None = None) -> dict:
-    """counts[0] x counts[1] x counts[2] lattice at spacing h from `origin`
-    with uniform jitter in [-jitter, jitter] * h; x varies fastest."""
+                velocity_noise: float = 0.0, mass_kernel: str | None = None,
+                first: int = 0) -> dict:
+    """counts[0] x counts[1] x counts[2] lattice at spacing h from `origin`,
+    x fastest (the reference's _init_box_kernel, scene.cu:14-37), with
+    uniform jitter in [-jitter, jitter] * h per axis and velocities uniform
+    in [-velocity_noise, velocity_noise], drawn from the counter-based
+    generator at the particle's index (first + q): bit for bit what
+    reyn_scene_fluid_block writes on the GPU."""
     nx, ny, nz = counts
-    rng = np.random.Generator(np.random.PCG64(seed))
-    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
-    base = np.stack([i.ravel(), j.ravel(), k.ravel()], 1).astype(np.float64) * h
-    base += np.asarray(origin, np.float64)
-    n = base.shape[0]
-    if jitter:
-        base += rng.uniform(-jitter, jitter, size=(n, 3)) * h
-    v = np.zeros((n, 3))
-    if velocity_noise:
-        v = rng.uniform(-velocity_noise, velocity_noise, size=(n, 3))
-    m = np.float32(np.float32(np.float32(rho0) * np.float32(h)) * np.float32(h)) * np.float32(h)
+    q = np.arange(nx * ny * nz, dtype=np.int64)
+    i, j, k = q % nx, (q // nx) % ny, q // (nx * ny)
+    hh = np.float32(h)
+    o = np.asarray(origin, np.float32)
+    g = q + first
+    pos = []
+    for axis, idx in enumerate((i, j, k)):
+        p = o[axis] + idx.astype(np.float32) * hh
+        if jitter:
+            p = p + _symmetric(uniform01(seed, axis, g), np.float32(jitter) * hh)
+        pos.append(p.astype(np.float32))
+    n = q.size
+    vel = []
+    for axis in range(3):
+        if velocity_noise:
+            vel.append(_symmetric(uniform01(seed, 3 + axis, g), np.float32(velocity_noise)))
+        else:
+            vel.append(np.zeros(n, np.float32))
+    m = np.float32(np.float32(np.float32(rho0) * hh) * hh) * hh
     if mass_kernel:
         # calibrated so that the unjittered lattice sits exactly at rho0
         m = np.float32(float(m) / lattice_density_factor(mass_kernel))
-    return {"x": base[:, 0].astype(np.float32), "y": base[:, 1].astype(np.float32),
-            "z": base[:, 2].astype(np.float32), "vx": v[:, 0].astype(np.float32),
-            "vy": v[:, 1].astype(np.float32), "vz": v[:, 2].astype(np.float32),
-            "m": np.full(n, m, np.float32), "id": np.arange(n, dtype=np.float32)}
+    return {"x": pos[0], "y": pos[1], "z": pos[2], "vx": vel[0], "vy": vel[1], "vz": vel[2],
+            "m": np.full(n, m, np.float32), "id": np.arange(first, first + n, dtype=np.float32)}
 
 
 def dam_break(counts, h: float, box, rho0: float = 1000.0, jitter: float = 0.1,
