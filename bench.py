@@ -89,11 +89,28 @@ LAMBDA = 0.4
 DT0 = 5e-4
 
 
+def scene_spec(rank: int, scale: int) -> dict:
+    return dict(counts=(256 // scale, 128 // scale, 128 // scale), h=0.005 * scale,
+                box=(2.0, 1.0, 1.0), rho0=1000.0, jitter=0.05, seed=3 + rank,
+                mass_kernel="C2", gap=1.5)
+
+
 def scene_for(rank: int, scale: int):
+    """The workload built on the host (for the CPU arms)."""
     from reyn_b200 import scenes
-    counts = (256 // scale, 128 // scale, 128 // scale)
-    return scenes.dam_break(counts, 0.005 * scale, (2.0, 1.0, 1.0), 1000.0, 0.05,
-                            seed=3 + rank, name=WORKLOAD, mass_kernel="C2", gap=1.5)
+    return scenes.dam_break(name=WORKLOAD, **scene_spec(rank, scale))
+
+
+class DeviceScene:
+    """The workload generated on the GPU: the same arrays as scene_for."""
+
+    def __init__(self, rank: int, scale: int):
+        from reyn_b200 import scenes
+        spec = scene_spec(rank, scale)
+        self.st, self.walls, self.box_min, self.box_max = scenes.dam_break_on_device(**spec)
+        self.h, self.rho0 = spec["h"], spec["rho0"]
+        self.n = self.st.n
+        self.nb = int(self.walls[0].numel())
 
 
 def viscous_dt_limit(h: float, nu: float) -> float:
@@ -204,18 +221,14 @@ class EngineRun:
     and the main-loop step (main.cu:64-75)."""
 
     def __init__(self, rank: int, scale: int, dev, precision: str, order: str = "xyz"):
-        import torch
-
         import reyn_b200 as rb
 
         self.rb = rb
         self.precision = precision
-        self.sc = sc = scene_for(rank, scale)
+        self.sc = sc = DeviceScene(rank, scale)
         self.n = sc.n
-        self.st = rb.Particles(sc.n, sc.rho0)
-        self.st.upload(sc.fluid)
-        self.bd = rb.Boundary(*(torch.tensor(sc.bdy[k], device=dev) for k in ("x", "y", "z")),
-                              None, h=sc.h, rho0=sc.rho0, mass_iters=5)
+        self.st = sc.st
+        self.bd = rb.Boundary(*sc.walls, None, h=sc.h, rho0=sc.rho0, mass_iters=5)
         self.grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h, 0.5,
                             rb.ORDER_ZORDER if order == "zorder" else rb.ORDER_XYZ)
         prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, NU)

@@ -175,6 +175,34 @@ def dam_break(counts, h: float, box, rho0: float = 1000.0, jitter: float = 0.1,
                   "seed": seed})
 
 
+def rest_mass(h: float, rho0: float, mass_kernel: str | None = None) -> float:
+    """rho0 h^3 in float32 (scene.cu:36), calibrated to the lattice density of
+    `mass_kernel` when given."""
+    hh = np.float32(h)
+    m = np.float32(np.float32(np.float32(rho0) * hh) * hh) * hh
+    if mass_kernel:
+        m = np.float32(float(m) / lattice_density_factor(mass_kernel))
+    return float(m)
+
+
+def dam_break_on_device(counts, h: float, box, rho0: float = 1000.0, jitter: float = 0.1,
+                        seed: int = 1, velocity_noise: float = 0.0,
+                        mass_kernel: str | None = None, gap: float = 1.0, stream=None):
+    """The dam_break scene generated on the GPU (reyn_scene_fluid_block and
+    reyn_scene_box_walls): the same arrays, without a host copy. Returns the
+    particle state, the wall samples as three device tensors, and the box."""
+    import reyn_b200 as rb
+    n = int(counts[0]) * int(counts[1]) * int(counts[2])
+    st = rb.Particles(n, rho0)
+    o = np.float32(gap * h)
+    rb.scene_fluid_block(st, counts, (o, o, o), h, rest_mass(h, rho0, mass_kernel), jitter,
+                         velocity_noise, seed, stream=stream)
+    box_min = np.zeros(3, np.float32)
+    box_max = np.asarray(box, np.float32)
+    walls = rb.scene_box_walls(box_min, box_max, h, stream=stream)
+    return st, walls, box_min, box_max
+
+
 def sesph_small(seed: int = 1) -> Scene:
     """SESPH dam break: 32^3 fluid particles at spacing 0.02, jitter +-0.1 h,
     unit box with Akinci walls at spacing 0.02."""
