@@ -209,6 +209,29 @@ namespace detail {
             check(reyn_solver_step(s_, st.handle(), g, bdy ? bdy->handle() : nullptr, dt, &it, s));
             return it;
         }
+        // the step with hard_enforce_bounds and the next controller's
+        // max-velocity reduction fused into its integrating kernel
+        uint32_t step_bounded(Particles& st, const reyn_grid* g, const BoundarySamples* bdy,
+            float dt, float3 bound_min, float3 bound_max, cudaStream_t s)
+        {
+            const float lo[3] = { bound_min.x, bound_min.y, bound_min.z };
+            const float hi[3] = { bound_max.x, bound_max.y, bound_max.z };
+            uint32_t it = 0;
+            check(reyn_solver_step_bounded(s_, st.handle(), g, bdy ? bdy->handle() : nullptr, dt,
+                lo, hi, &it, s));
+            return it;
+        }
+        // simple_dt_controller (cfl.cu:39-52) from the last bounded step's max |v|
+        float next_dt(Particles& st, uint32_t iter_last, float dt_last, float lambda, float h,
+            float3 g, uint32_t iter_target = 5, float change_factor = 0.01f,
+            cudaStream_t s = nullptr)
+        {
+            const float gg[3] = { g.x, g.y, g.z };
+            float dt = 0.f;
+            check(reyn_solver_next_dt(s_, st.handle(), iter_last, dt_last, lambda, h, gg,
+                iter_target, change_factor, &dt, s));
+            return dt;
+        }
         reyn_solver_buffers buffers() const
         {
             reyn_solver_buffers b {};
@@ -242,6 +265,11 @@ public:
     {
         detail::Solver::step(st, grid.grid, &bdy, dt, s);
     }
+    void step_bounded(Particles& st, const UniformGrid<R>& grid, const BoundarySamples& bdy,
+        float dt, float3 bound_min, float3 bound_max, cudaStream_t s = nullptr)
+    {
+        detail::Solver::step_bounded(st, grid.grid, &bdy, dt, bound_min, bound_max, s);
+    }
 
 private:
     static reyn_params with(reyn_params p, float3 g, float k)
@@ -268,6 +296,13 @@ public:
     {
         return detail::Solver::step(st, grid.grid, &bdy, dt, s);
     }
+    // step + hard_enforce_bounds in one pass; next_dt() then needs no pass
+    uint32_t step_bounded(Particles& st, const UniformGrid<R>& grid,
+        const BoundarySamples& bdy, float dt, float3 bound_min, float3 bound_max,
+        cudaStream_t s = nullptr)
+    {
+        return detail::Solver::step_bounded(st, grid.grid, &bdy, dt, bound_min, bound_max, s);
+    }
 };
 
 // IISPH<K,R> (IISPH.cuh:8-93): step returns the iteration count
@@ -288,6 +323,13 @@ public:
         float dt, cudaStream_t s = nullptr)
     {
         return detail::Solver::step(st, grid.grid, &bdy, dt, s);
+    }
+    // step + hard_enforce_bounds in one pass; next_dt() then needs no pass
+    uint32_t step_bounded(Particles& st, const UniformGrid<R>& grid,
+        const BoundarySamples& bdy, float dt, float3 bound_min, float3 bound_max,
+        cudaStream_t s = nullptr)
+    {
+        return detail::Solver::step_bounded(st, grid.grid, &bdy, dt, bound_min, bound_max, s);
     }
 };
 

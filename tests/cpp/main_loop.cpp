@@ -2,6 +2,8 @@
 // C++ adapters (include/reyn_b200.hpp): dt controller, grid build with
 // reorder (the particle ID carried as an extra array), IISPH step, hard
 // bounds. Reads a scene from argv[1], writes the final state to argv[2].
+// With a third argument "fused" the loop uses the fused tail (next_dt and
+// step_bounded in place of simple_dt_controller, step and hard_enforce_bounds).
 //
 // input  (little-endian): u32 N, u32 Nb, u32 steps, f32 h, rho0, nu, dt0,
 //        lambda, box_min[3], box_max[3], then N floats each of x y z vx vy vz
@@ -11,16 +13,18 @@
 #include "reyn_b200.hpp"
 
 #include <cstdio>
+#include <string>
 #include <vector>
 
 using namespace reyn;
 
 int main(int argc, char** argv)
 {
-    if (argc != 3) {
-        std::fprintf(stderr, "usage: main_loop in.bin out.bin\n");
+    if (argc != 3 && argc != 4) {
+        std::fprintf(stderr, "usage: main_loop in.bin out.bin [fused]\n");
         return 2;
     }
+    const bool fused = argc == 4 && std::string(argv[3]) == "fused";
     FILE* f = std::fopen(argv[1], "rb");
     if (!f)
         return 2;
@@ -60,10 +64,16 @@ int main(int argc, char** argv)
         std::vector<float> dt_log;
         uint32_t iters = 0;
         for (uint32_t s = 0; s < steps; ++s) {
-            dt = simple_dt_controller(iters, dt, lambda, h, state, g, 10, 0.001f);
-            const auto grid { builder.construct_and_reorder(2.f * h, state, d_id) };
-            iters = solver.step(state, grid, bdy, dt);
-            hard_enforce_bounds(state, bmin, bmax);
+            if (fused) {
+                dt = solver.next_dt(state, iters, dt, lambda, h, g, 10, 0.001f);
+                const auto grid { builder.construct_and_reorder(2.f * h, state, d_id) };
+                iters = solver.step_bounded(state, grid, bdy, dt, bmin, bmax);
+            } else {
+                dt = simple_dt_controller(iters, dt, lambda, h, state, g, 10, 0.001f);
+                const auto grid { builder.construct_and_reorder(2.f * h, state, d_id) };
+                iters = solver.step(state, grid, bdy, dt);
+                hard_enforce_bounds(state, bmin, bmax);
+            }
             iters_log.push_back(iters);
             dt_log.push_back(dt);
         }

@@ -83,3 +83,23 @@ def test_cpp_main_loop_matches_oracle(cuda, tmp_path):
         assert_close(got[k][go], fl[k][wo], 1e-6, 1e-6, k)
     for k in ("vx", "vy", "vz"):
         assert_close(got[k][go], fl[k][wo], 1e-3, 1e-3, k)
+
+
+def test_cpp_main_loop_fused_tail_is_bit_identical(cuda, tmp_path):
+    """The same C++ loop with the fused tail (next_dt + step_bounded)
+    reproduces the separate calls bit for bit."""
+    exe = compile_main_loop(str(tmp_path))
+    sc = scenes.dam_break((14, 12, 10), 0.02, (0.5, 0.5, 0.5), velocity_noise=0.02, seed=22)
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    inp = os.path.join(str(tmp_path), "in.bin")
+    write_scene(inp, sc, bm, 4, 1e-3, 0.4, 0.01)
+    res = []
+    for mode in ([], ["fused"]):
+        out = os.path.join(str(tmp_path), f"out{len(mode)}.bin")
+        subprocess.run([exe, inp, out] + mode, check=True)
+        res.append(read_out(out, sc.n))
+    (ia, da, a), (ib, db, b) = res
+    assert list(ia) == list(ib)
+    np.testing.assert_array_equal(da, db)
+    for k in a:
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
