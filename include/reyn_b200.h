@@ -134,6 +134,20 @@ int reyn_grid_create(const float bound_min[3], const float bound_max[3],
     float search_radius, float cell_ratio, reyn_cell_order order,
     reyn_grid** out);
 int reyn_grid_destroy(reyn_grid* g);
+/* (no counterpart in the reference) a grid over a batch of independent
+ * scenes that share the smoothing kernel, spacing and solver parameters.
+ * Scene s owns the particles [first[s], first[s+1]) of one reyn_particles
+ * (n_scenes + 1 host offsets) and lies in its own box scene_min/max[3s..3s+2]
+ * (host arrays; the boxes may overlap in space: scenes never see each
+ * other). Every scene is gridded over the common frame frame_min/max (which
+ * must contain every scene box) with its own range of cell keys, so one
+ * launch per phase serves every scene and a reorder keeps each scene's
+ * particles in its own index range. prefix has n_scenes * n_keys + 1
+ * entries. At most 65535 scenes. */
+int reyn_grid_create_batched(const float frame_min[3], const float frame_max[3],
+    float search_radius, float cell_ratio, reyn_cell_order order,
+    uint32_t n_scenes, const uint32_t* first, const float* scene_min,
+    const float* scene_max, reyn_grid** out);
 /* construct (uniformgrid.cu:145-156): builds prefix + sorted for n
  * positions (device arrays), particles are not moved. Within a cell the
  * indices are ascending (a stable counting sort), which is the canonical
@@ -198,6 +212,13 @@ int reyn_boundary_create(const float* bx, const float* by, const float* bz,
     const float* bm, uint32_t nb, float h, float rho0, uint32_t mass_iters,
     void* stream, reyn_boundary** out);
 int reyn_boundary_destroy(reyn_boundary* b);
+/* (no counterpart) the boundary of a batch: scene s owns samples [first[s],
+ * first[s+1]) (host offsets); Akinci masses and every boundary term use
+ * only the samples of the particle's own scene. */
+int reyn_boundary_create_batched(const float* bx, const float* by,
+    const float* bz, const float* bm, uint32_t nb, uint32_t n_scenes,
+    const uint32_t* first, float h, float rho0, uint32_t mass_iters,
+    void* stream, reyn_boundary** out);
 /* device pointers of the reordered samples and masses */
 int reyn_boundary_arrays(const reyn_boundary* b, const float** bx,
     const float** by, const float** bz, const float** bm, uint32_t* nb);
@@ -308,6 +329,21 @@ typedef struct reyn_step_stats {
     double max_density_error;
 } reyn_step_stats;
 int reyn_solver_stats(const reyn_solver* s, reyn_step_stats* out);
+
+/* (no counterpart) one step of every scene of a batched grid (after
+ * construct_and_reorder over the batch): each phase is one launch over all
+ * scenes; PCISPH/IISPH iterate per scene, a scene leaving the iteration once
+ * it meets the criterion while the others go on (its particles then sit out
+ * the remaining sweeps). bounded != 0 applies hard_enforce_bounds with each
+ * scene's own box in the integrating kernel. scene_iters (host, n_scenes
+ * entries, may be NULL) receives each scene's iteration count. One dt for
+ * all scenes. */
+int reyn_solver_step_batched(reyn_solver* s, reyn_particles* state,
+    const reyn_grid* grid, const reyn_boundary* bdy, float dt, int bounded,
+    uint32_t* scene_iters, void* stream);
+/* per-scene iterations and density errors of the last batched step */
+int reyn_solver_scene_stats(const reyn_solver* s, uint32_t n_scenes,
+    reyn_step_stats* out);
 
 /* ---- time step (src/timestep/cfl.cu) -------------------------------------- */
 /* cfl_time_step (cfl.cu:5-37); synchronises the stream */

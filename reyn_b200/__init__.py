@@ -109,6 +109,12 @@ _SIGNATURES = {
                              ctypes.POINTER(ctypes.c_uint64), _vp],
     "reyn_scene_sphere": [_f * 3, _f, _f, _vp, _vp, _vp, _u32, ctypes.POINTER(_u32), _vp],
     "reyn_scene_cull": [_vp, _vp, _f, ctypes.POINTER(_u32), _vp],
+    "reyn_grid_create_batched": [_f * 3, _f * 3, _f, _f, ctypes.c_int, _u32, _vp, _vp, _vp,
+                                 ctypes.POINTER(_vp)],
+    "reyn_boundary_create_batched": [_vp, _vp, _vp, _vp, _u32, _u32, _vp, _f, _f, _u32, _vp,
+                                     ctypes.POINTER(_vp)],
+    "reyn_solver_step_batched": [_vp, _vp, _vp, _vp, _f, ctypes.c_int, _vp, _vp],
+    "reyn_solver_scene_stats": [_vp, _u32, _vp],
     "reyn_solver_step": [_vp, _vp, _vp, _vp, _f, ctypes.POINTER(_u32), _vp],
     "reyn_solver_step_bounded": [_vp, _vp, _vp, _vp, _f, _f * 3, _f * 3, ctypes.POINTER(_u32),
                                  _vp],
@@ -240,10 +246,24 @@ class Grid:
     """UniformGridBuilder (reference uniformgrid.cuh:200-489)."""
 
     def __init__(self, bmin, bmax, search_radius: float, cell_ratio: float = 0.5,
-                 order: int = 0):
+                 order: int = 0, scene_first=None, scene_min=None, scene_max=None):
+        """With scene_first (n_scenes + 1 offsets) and per-scene boxes
+        scene_min/max (n_scenes x 3): a batched grid over the frame
+        [bmin, bmax] (reyn_grid_create_batched)."""
         h = _vp()
-        check(lib().reyn_grid_create(_f3(bmin), _f3(bmax), search_radius, cell_ratio, order,
-                                     ctypes.byref(h)))
+        self.n_scenes = 0
+        if scene_first is None:
+            check(lib().reyn_grid_create(_f3(bmin), _f3(bmax), search_radius, cell_ratio, order,
+                                         ctypes.byref(h)))
+        else:
+            first = np.ascontiguousarray(scene_first, np.uint32)
+            lo = np.ascontiguousarray(scene_min, np.float32).reshape(-1)
+            hi = np.ascontiguousarray(scene_max, np.float32).reshape(-1)
+            self.n_scenes = first.size - 1
+            check(lib().reyn_grid_create_batched(_f3(bmin), _f3(bmax), search_radius, cell_ratio,
+                                                 order, self.n_scenes, first.ctypes.data,
+                                                 lo.ctypes.data, hi.ctypes.data,
+                                                 ctypes.byref(h)))
         self.h = h
         self.r = search_radius
 
@@ -290,11 +310,21 @@ class Boundary:
     """BoundarySamples (reference scene.cuh:14-46) with Akinci masses."""
 
     def __init__(self, bx, by, bz, bm=None, h: float = 1.0, rho0: float = 1.0,
-                 mass_iters: int = 5, stream=None):
+                 mass_iters: int = 5, stream=None, scene_first=None):
+        """scene_first (n_scenes + 1 offsets): a batched boundary, scene s
+        owning samples scene_first[s] .. scene_first[s + 1] - 1."""
         hdl = _vp()
         nb = 0 if bx is None else bx.numel()
-        check(lib().reyn_boundary_create(_ptr(bx), _ptr(by), _ptr(bz), _ptr(bm), nb, h, rho0,
-                                         mass_iters, _stream(stream), ctypes.byref(hdl)))
+        if scene_first is None:
+            check(lib().reyn_boundary_create(_ptr(bx), _ptr(by), _ptr(bz), _ptr(bm), nb, h,
+                                             rho0, mass_iters, _stream(stream),
+                                             ctypes.byref(hdl)))
+        else:
+            first = np.ascontiguousarray(scene_first, np.uint32)
+            check(lib().reyn_boundary_create_batched(_ptr(bx), _ptr(by), _ptr(bz), _ptr(bm), nb,
+                                                     first.size - 1, first.ctypes.data, h, rho0,
+                                                     mass_iters, _stream(stream),
+                                                     ctypes.byref(hdl)))
         self.h = hdl
         self.nb = nb
 
@@ -370,6 +400,21 @@ class Solver:
                                                  _f3(bounds[1]), ctypes.byref(it),
                                                  _stream(stream)))
         return it.value
+
+    def step_batched(self, state: Particles, grid: Grid, bdy: Optional[Boundary], dt: float,
+                     bounded: bool = True, stream=None) -> np.ndarray:
+        """One step of every scene of a batched grid; returns per-scene
+        iteration counts."""
+        it = np.zeros(grid.n_scenes, np.uint32)
+        check(lib().reyn_solver_step_batched(self.h, state.h, grid.h, bdy.h if bdy else None, dt,
+                                             1 if bounded else 0, it.ctypes.data,
+                                             _stream(stream)))
+        return it
+
+    def scene_stats(self, n_scenes: int) -> list:
+        out = (StepStats * n_scenes)()
+        check(lib().reyn_solver_scene_stats(self.h, n_scenes, out))
+        return list(out)
 
     def next_dt(self, state: Particles, iter_last: int, dt_last: float, lam: float, h: float,
                 g, iter_target: int = 5, change: float = 0.01, stream=None) -> float:

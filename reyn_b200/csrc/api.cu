@@ -160,6 +160,40 @@ int reyn_grid_create(const float bound_min[3], const float bound_max[3], float s
     });
 }
 
+int reyn_grid_create_batched(const float frame_min[3], const float frame_max[3],
+    float search_radius, float cell_ratio, reyn_cell_order order, uint32_t n_scenes,
+    const uint32_t* first, const float* scene_min, const float* scene_max, reyn_grid** out)
+{
+    return guard([&] {
+        require(out != nullptr, "null output handle");
+        *out = nullptr;
+        check_vec3(frame_min, "frame_min must be 3 finite floats");
+        check_vec3(frame_max, "frame_max must be 3 finite floats");
+        require(first && scene_min && scene_max, "null scene arrays");
+        require(order == REYN_ORDER_XYZ || order == REYN_ORDER_ZORDER, "unknown cell order");
+        for (uint32_t k = 0; k < 3 * n_scenes; ++k)
+            require(std::isfinite(scene_min[k]) && std::isfinite(scene_max[k])
+                    && scene_min[k] <= scene_max[k],
+                "scene boxes must be finite and ordered");
+        auto g = std::make_unique<reyn_grid>();
+        g->geom = make_geom(frame_min, frame_max, search_radius, cell_ratio, order);
+        g->ratio = cell_ratio;
+        g->set_scenes(first, n_scenes, nullptr);
+        g->scene_lo.resize(3 * size_t(n_scenes));
+        g->scene_hi.resize(3 * size_t(n_scenes));
+        REYN_CUDA(cudaMemcpy(g->scene_lo.get(), scene_min, 3 * size_t(n_scenes) * sizeof(float),
+            cudaMemcpyHostToDevice));
+        REYN_CUDA(cudaMemcpy(g->scene_hi.get(), scene_max, 3 * size_t(n_scenes) * sizeof(float),
+            cudaMemcpyHostToDevice));
+        const size_t C = size_t(g->total_keys());
+        g->counts.resize(C);
+        REYN_CUDA(cudaMemset(g->counts.get(), 0, C * sizeof(uint32_t)));
+        g->prefix.resize(C + 1);
+        g->status.resize(1);
+        *out = g.release();
+    });
+}
+
 int reyn_grid_destroy(reyn_grid* g)
 {
     return guard([&] { delete g; });
@@ -255,6 +289,24 @@ int reyn_boundary_create(const float* bx, const float* by, const float* bz, cons
         require(rho0 > 0.f && std::isfinite(rho0), "rho0 must be positive and finite");
         auto b = std::make_unique<reyn_boundary>();
         boundary_build(*b, bx, by, bz, bm, nb, h, rho0, mass_iters, as_stream(stream));
+        *out = b.release();
+    });
+}
+
+int reyn_boundary_create_batched(const float* bx, const float* by, const float* bz,
+    const float* bm, uint32_t nb, uint32_t n_scenes, const uint32_t* first, float h, float rho0,
+    uint32_t mass_iters, void* stream, reyn_boundary** out)
+{
+    return guard([&] {
+        require(out != nullptr, "null output handle");
+        *out = nullptr;
+        require(rho0 > 0.f && std::isfinite(rho0), "rho0 must be positive and finite");
+        require(first != nullptr && n_scenes >= 1, "scene offsets required");
+        require(first[n_scenes] == nb, "scene offsets must end at the sample count");
+        require(nb > 0, "a batched boundary needs samples");
+        auto b = std::make_unique<reyn_boundary>();
+        boundary_build(*b, bx, by, bz, bm, nb, h, rho0, mass_iters, as_stream(stream), first,
+            n_scenes);
         *out = b.release();
     });
 }
@@ -368,6 +420,47 @@ int reyn_solver_step(reyn_solver* s, reyn_particles* state, const reyn_grid* gri
     const reyn_boundary* bdy, float dt, uint32_t* iters, void* stream)
 {
     return step_impl(s, state, grid, bdy, dt, nullptr, nullptr, iters, stream);
+}
+
+int reyn_solver_step_batched(reyn_solver* s, reyn_particles* state, const reyn_grid* grid,
+    const reyn_boundary* bdy, float dt, int bounded, uint32_t* scene_iters, void* stream)
+{
+    if (!grid || grid->n_scenes == 0) {
+        set_last_error("reyn_solver_step_batched needs a batched grid");
+        return REYN_ERR_INVALID;
+    }
+    // the per-scene boxes replace the bounds; these only switch them on
+    const float on[3] = { 0.f, 0.f, 0.f };
+    const int rc = step_impl(s, state, grid, bdy, dt, bounded ? on : nullptr,
+        bounded ? on : nullptr, nullptr, stream);
+    if (scene_iters && (rc == REYN_OK || rc == REYN_ERR_ITER_LIMIT)) {
+        const int rc2 = guard([&] {
+            REYN_CUDA(cudaMemcpy(scene_iters, s->scene_iters.get(),
+                grid->n_scenes * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        });
+        if (rc2)
+            return rc2;
+    }
+    return rc;
+}
+
+int reyn_solver_scene_stats(const reyn_solver* s, uint32_t n_scenes, reyn_step_stats* out)
+{
+    return guard([&] {
+        require(s && out, "null argument");
+        require(n_scenes == s->n_scenes && n_scenes > 0,
+            "scene count differs from the last batched step's");
+        std::vector<uint32_t> it(n_scenes);
+        std::vector<float> avg(n_scenes), mx(n_scenes);
+        REYN_CUDA(cudaMemcpy(it.data(), s->scene_iters.get(), n_scenes * sizeof(uint32_t),
+            cudaMemcpyDeviceToHost));
+        REYN_CUDA(cudaMemcpy(avg.data(), s->scene_avg.get(), n_scenes * sizeof(float),
+            cudaMemcpyDeviceToHost));
+        REYN_CUDA(cudaMemcpy(mx.data(), s->scene_max.get(), n_scenes * sizeof(float),
+            cudaMemcpyDeviceToHost));
+        for (uint32_t k = 0; k < n_scenes; ++k)
+            out[k] = reyn_step_stats { it[k], avg[k], mx[k] };
+    });
 }
 
 int reyn_solver_step_bounded(reyn_solver* s, reyn_particles* state, const reyn_grid* grid,

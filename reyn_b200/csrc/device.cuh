@@ -163,7 +163,24 @@ struct GridView {
     int order;      // REYN_ORDER_XYZ or REYN_ORDER_ZORDER
     int tx, txy;    // Z-order: 32-cell tiles along x, per xy layer
     const uint32_t* __restrict__ prefix;
+    // batched scenes: scene of each point (null for one scene); scene s's
+    // cells are keyed s * key_stride + its own key
+    const uint16_t* __restrict__ sid;
+    uint32_t key_stride;
 };
+
+__device__ __forceinline__ uint32_t scene_of(const GridView& g, uint32_t i)
+{
+    return g.sid ? uint32_t(__ldg(g.sid + i)) : 0u;
+}
+
+// the view of scene s alone (its keys start at prefix + s * key_stride)
+__device__ __forceinline__ GridView at_scene(GridView g, uint32_t s)
+{
+    g.prefix += size_t(s) * g.key_stride;
+    g.sid = nullptr;
+    return g;
+}
 
 // Z-order cell keys: cells are grouped into bricks of 4x4x4 (x fastest
 // inside a brick, so x-runs of up to 4 cells stay contiguous), bricks follow

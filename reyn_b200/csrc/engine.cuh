@@ -56,6 +56,16 @@ struct Grid {
     DevArray<float> extra_tmp; // reorder staging of caller arrays
     mutable DevArray<float4> pts_tmp; // packed positions for statistics
     uint32_t n = 0;
+    // batched scenes (n_scenes > 0): scene s owns points [first[s],
+    // first[s + 1]) in every order the grid produces (its keys are
+    // s * geom.keys() + the scene's own key, so a reorder keeps scenes
+    // contiguous); sid holds each point's scene
+    uint32_t n_scenes = 0;
+    std::vector<uint32_t> first;
+    DevArray<uint16_t> sid;
+    DevArray<float> scene_lo, scene_hi; // per-scene boxes (3 floats each), fluid grids
+    int64_t total_keys() const { return geom.keys() * int64_t(n_scenes ? n_scenes : 1); }
+    void set_scenes(const uint32_t* first, uint32_t n_scenes, cudaStream_t s);
     bool counts_dirty = false; // a build stopped between histogram and scatter
     bool reordered = false;    // last build was construct_and_reorder
     const reyn_particles* reordered_state = nullptr;
@@ -114,6 +124,13 @@ struct reyn_solver {
     const reyn_particles* p_state = nullptr;
     reyn_step_stats stats {};
     double pcisph_delta = 0.0; // k_c_pcisph template stiffness
+    // batched scenes: per-scene sweep sums, activity, iterations and errors
+    uint32_t n_scenes = 0;
+    reyn::DevArray<unsigned char> scene_stats;
+    reyn::DevArray<uint8_t> scene_active;
+    reyn::DevArray<uint32_t> scene_iters, scene_first, n_active;
+    reyn::DevArray<float> scene_avg, scene_max;
+    std::unique_ptr<reyn::PinnedArray<uint32_t>> n_active_host;
     // max |v| after the last bounded step, for the next dt controller
     reyn::DevArray<float> vmax;
     std::unique_ptr<reyn::PinnedArray<float>> vmax_host;
@@ -161,9 +178,12 @@ void neighbour_stats(const Grid& g, const float* x, const float* y,
     const float* z, const float* m, int kind, uint32_t* count, float* len2,
     float* rho, cudaStream_t s);
 
+// scene_first/n_scenes (optional): batched boundaries, scene s owning
+// samples [scene_first[s], scene_first[s + 1])
 void boundary_build(reyn_boundary& b, const float* bx, const float* by,
     const float* bz, const float* bm, uint32_t nb, float h, float rho0,
-    uint32_t mass_iters, cudaStream_t s);
+    uint32_t mass_iters, cudaStream_t s, const uint32_t* scene_first = nullptr,
+    uint32_t n_scenes = 0);
 
 // one step; with bounds (bmin and bmax not null) the step also applies
 // hard_enforce_bounds and records max |v| in sv.vmax (step tail fusion)

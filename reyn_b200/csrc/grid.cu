@@ -61,6 +61,8 @@ GridView Grid::view(float search_radius) const
     v.tx = geom.t[0];
     v.txy = geom.t[0] * geom.t[1];
     v.prefix = prefix.get();
+    v.sid = n_scenes ? sid.get() : nullptr;
+    v.key_stride = uint32_t(geom.keys());
     return v;
 }
 
@@ -94,7 +96,7 @@ __global__ void k_keys_count(uint32_t n, const float* __restrict__ x,
                              min(max(c.z, 0), g.nz - 1))
                        : make_int3(0, 0, 0);
         }
-        key = cell_key(g, c.x, c.y, c.z);
+        key = cell_key(g, c.x, c.y, c.z) + scene_of(g, i) * g.key_stride;
         keys[i] = key;
     }
     const unsigned group = __match_any_sync(0xffffffffu, key);
@@ -294,7 +296,8 @@ void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& part,
 void Grid::build(const float* x, const float* y, const float* z, uint32_t np,
     cudaStream_t s)
 {
-    const int64_t C = geom.keys();
+    const int64_t C = total_keys();
+    require(!n_scenes || np == first[n_scenes], "particle count differs from the scenes' total");
     if (counts.size() != size_t(C) || counts_dirty) {
         // the scatter returns every count to zero; only a fresh array or an
         // interrupted build needs clearing
@@ -329,6 +332,47 @@ void Grid::build(const float* x, const float* y, const float* z, uint32_t np,
             np, slots.get(), keys.get(), prefix.get(), sorted.get()));
     }
     counts_dirty = false;
+}
+
+// each point's scene from the scene offsets (binary search)
+__global__ void k_fill_sid(uint32_t n, const uint32_t* __restrict__ first, uint32_t ns,
+    uint16_t* __restrict__ sid)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    uint32_t lo = 0, hi = ns; // first[lo] <= i < first[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (first[mid] <= i)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    sid[i] = uint16_t(lo);
+}
+
+void Grid::set_scenes(const uint32_t* f, uint32_t ns, cudaStream_t s)
+{
+    require(ns >= 1 && ns <= 65535, "1 .. 65535 scenes");
+    require(f != nullptr && f[0] == 0, "scene offsets must start at 0");
+    for (uint32_t k = 0; k < ns; ++k)
+        require(f[k] <= f[k + 1], "scene offsets must not decrease");
+    require(geom.keys() * int64_t(ns) < (int64_t(1) << 32) - 1,
+        "scenes x cells exceed 32-bit keys");
+    n_scenes = ns;
+    first.assign(f, f + ns + 1);
+    const uint32_t total = first[ns];
+    sid.resize(total);
+    if (total) {
+        DevArray<uint32_t> fd(ns + 1);
+        REYN_CUDA(cudaMemcpyAsync(fd.get(), first.data(), (ns + 1) * sizeof(uint32_t),
+            cudaMemcpyHostToDevice, s));
+        REYN_KERNEL("k_fill_sid", s,
+            k_fill_sid<<<blocks_for(total, THREADS), THREADS, 0, s>>>(total, fd.get(), ns,
+            sid.get()));
+        REYN_CUDA(cudaStreamSynchronize(s));
+    }
 }
 
 void Grid::check_status(cudaStream_t s, const char* what)
@@ -489,6 +533,8 @@ __global__ void __launch_bounds__(NBR_THREADS) k_neighbour_stats(uint32_t n, Gri
     if (s >= n)
         return;
     const float4 me = pts[s];
+    const uint32_t p = owner ? owner[s] : s;
+    g = at_scene(g, scene_of(g, p)); // batched grids: the point's own scene
     int3 c = cell_of(g, me.x, me.y, me.z);
     if (!cell_inside(g, c, R) || !(isfinite(me.x) && isfinite(me.y) && isfinite(me.z))) {
         atomicOr(status, STATUS_OUT_OF_GRID);
@@ -503,7 +549,6 @@ __global__ void __launch_bounds__(NBR_THREADS) k_neighbour_stats(uint32_t n, Gri
             if (rho)
                 dens += q.w * pair_w<KIND>(kc, l2);
         });
-    const uint32_t p = owner ? owner[s] : s;
     if (count)
         count[p] = cnt;
     if (len2)
@@ -602,6 +647,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_boundary_mass(uint32_t n, GridV
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    g = at_scene(g, scene_of(g, i)); // batched boundaries: the sample's own scene
     const float4 me = pts[i];
     int3 c = clamp_cell(g, cell_of(g, me.x, me.y, me.z), R);
     float sum = 0.f;
@@ -621,6 +667,7 @@ __global__ void k_mark_near(uint32_t n, GridView g, const float4* __restrict__ p
         return;
     const float4 me = pts[i];
     const int3 c = clamp_cell(g, cell_of(g, me.x, me.y, me.z), 2);
+    near += size_t(scene_of(g, i)) * g.key_stride; // batched: the sample's scene
     for (int dz = -2; dz <= 2; ++dz)
         for (int dy = -2; dy <= 2; ++dy) {
             const int base = (c.z + dz) * g.nxny + (c.y + dy) * g.nx + c.x;
@@ -637,7 +684,8 @@ __global__ void k_unpack_mass(uint32_t n, const float4* __restrict__ pts, float*
 }
 
 void boundary_build(reyn_boundary& b, const float* bx, const float* by, const float* bz,
-    const float* bm, uint32_t nb, float h, float rho0, uint32_t mass_iters, cudaStream_t s)
+    const float* bm, uint32_t nb, float h, float rho0, uint32_t mass_iters, cudaStream_t s,
+    const uint32_t* scene_first, uint32_t n_scenes)
 {
     require(h > 0.f && std::isfinite(h), "h must be positive");
     b.nb = nb;
@@ -662,6 +710,8 @@ void boundary_build(reyn_boundary& b, const float* bx, const float* by, const fl
     // the boundary grid: support 2h over the samples' own bounds, reference
     // geometry (sample_boundary.cu:420-428)
     b.grid.geom = make_geom(lo, hi, 2.f * h, 0.5f);
+    if (n_scenes) // batched: one grid per scene, keyed scene-major
+        b.grid.set_scenes(scene_first, n_scenes, s);
     b.grid.build(bx, by, bz, nb, s);
     b.grid.check_status(s, "boundary grid");
     b.x.resize(nb);
@@ -692,7 +742,7 @@ void boundary_build(reyn_boundary& b, const float* bx, const float* by, const fl
         k_pack_positions<<<blocks_for(nb, THREADS), THREADS, 0, s>>>(
         nb, nullptr, b.x.get(), b.y.get(), b.z.get(), b.m.get(), b.pm.get()));
     b.grid.reordered = true;
-    b.near.resize(size_t(b.grid.geom.cells()));
+    b.near.resize(size_t(b.grid.total_keys()));
     b.near.zero(s);
     REYN_KERNEL("k_mark_near", s,
         k_mark_near<<<blocks_for(nb, THREADS), THREADS, 0, s>>>(nb, b.view(), b.pm.get(),

@@ -20,6 +20,7 @@
 
 #include <cmath>
 #include <type_traits>
+#include <vector>
 
 namespace reyn {
 
@@ -56,6 +57,9 @@ struct Fluid {
     const uint2* __restrict__ pmh;
     const uint2* __restrict__ acch;
     const float4* __restrict__ acc32;
+    // batched scenes: per-scene flag, 0 once the scene's iteration has
+    // converged (its particles then sit out the remaining sweeps)
+    const uint8_t* __restrict__ active;
 };
 
 // ---- mixed precision ----------------------------------------------------------
@@ -196,6 +200,32 @@ __device__ __forceinline__ int3 fluid_cell(const Fluid& f, const float4& me)
         c = clamp_cell(f.g, c, R);
     }
     return c;
+}
+
+// batched scenes: narrows the views to particle i's scene (its grid keys,
+// its boundary grid and near-flags) and returns the scene; 0 for one scene
+__device__ __forceinline__ uint32_t enter_scene(Fluid& f, uint32_t i)
+{
+    if (!f.g.sid)
+        return 0;
+    const uint32_t s = __ldg(f.g.sid + i);
+    f.g = at_scene(f.g, s);
+    return s;
+}
+
+__device__ __forceinline__ uint32_t enter_scene(Fluid& f, Bdy& b, uint32_t i)
+{
+    const uint32_t s = enter_scene(f, i);
+    if (b.n && b.g.sid) {
+        b.near += size_t(s) * b.g.key_stride;
+        b.g = at_scene(b.g, s);
+    }
+    return s;
+}
+
+__device__ __forceinline__ bool scene_live(const Fluid& f, uint32_t s)
+{
+    return !f.active || __ldg(f.active + s);
 }
 
 // the fluid neighbours j != i of particle i from the step's list (or, for a
@@ -358,6 +388,65 @@ __device__ __forceinline__ void block_accumulate(SweepStats* st, unsigned over, 
     }
 }
 
+// the same sums per scene (batched scenes, one slot per scene): a warp
+// inside one scene reduces first, a warp across a scene boundary adds per lane
+__device__ __forceinline__ void scene_accumulate(SweepStats* st, uint32_t s, bool valid,
+    unsigned over, double err, double rho, float emax)
+{
+    const uint32_t s0 = __shfl_sync(0xffffffffu, s, 0);
+    if (__all_sync(0xffffffffu, valid && s == s0)) {
+        over = warp_sum(over);
+        err = warp_sum(err);
+        rho = warp_sum(rho);
+        emax = warp_max(emax);
+        if ((threadIdx.x & 31) != 0)
+            return;
+    } else if (!valid) {
+        return;
+    }
+    SweepStats* t = st + s;
+    if (over)
+        atomicAdd(&t->over, (unsigned long long)over);
+    if (err != 0.0)
+        atomicAdd(&t->err_sum, err);
+    if (rho != 0.0)
+        atomicAdd(&t->rho_sum, rho);
+    atomic_max_nonneg(&t->err_max, emax);
+}
+
+// per-scene convergence after a sweep (batched scenes): a scene that meets
+// its criterion stops iterating; n_active counts the scenes that go on.
+// mode 0: PCISPH average density (PCISPH.cu:101); 1: IISPH average error;
+// 2: IISPH any particle above eta rho0 (IISPH.cu:246)
+__global__ void k_scene_converge(uint32_t ns, const SweepStats* __restrict__ st,
+    const uint32_t* __restrict__ first, int mode, float eta, float rho0, uint32_t iter,
+    uint8_t* __restrict__ active, uint32_t* __restrict__ iters_out,
+    float* __restrict__ avg_err, float* __restrict__ max_err, uint32_t* __restrict__ n_active)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ns || !active[s])
+        return;
+    const uint32_t cnt = first[s + 1] - first[s];
+    bool conv = true;
+    if (cnt) {
+        const SweepStats t = st[s];
+        if (mode == 0) {
+            const double a = t.rho_sum / cnt;
+            conv = !((float)a > (eta + 1.f) * rho0);
+            avg_err[s] = (float)fmax(0.0, a / rho0 - 1.0);
+        } else {
+            conv = mode == 1 ? !(t.err_sum / cnt > (double)eta * rho0) : t.over == 0;
+            avg_err[s] = (float)(t.err_sum / cnt / rho0);
+            max_err[s] = t.err_max / rho0;
+        }
+    }
+    iters_out[s] = iter;
+    if (conv)
+        active[s] = 0;
+    else
+        atomicAdd(n_active, 1u);
+}
+
 // ---- step tail ---------------------------------------------------------------
 // The reference's main loop follows every step with hard_enforce_bounds
 // (scene.cu:466-483) and starts the next with simple_dt_controller, whose CFL
@@ -368,6 +457,11 @@ __device__ __forceinline__ void block_accumulate(SweepStats* st, unsigned over, 
 struct Tail {
     float3 lo, hi;
     float* vmax; // nullptr: no bounds, no reduction (the plain step)
+    // batched scenes: each particle's scene and the scenes' boxes (3 floats
+    // each), used instead of lo/hi
+    const uint16_t* sid;
+    const float* lo_s;
+    const float* hi_s;
 };
 
 // stores the new state of particle i (bounds applied when tail.vmax is set)
@@ -378,17 +472,24 @@ __device__ __forceinline__ float store_state(const Tail& t, uint32_t i, float px
     float* __restrict__ vz)
 {
     if (t.vmax) {
+        float3 lo = t.lo, hi = t.hi;
+        if (t.sid) {
+            const uint32_t sc = __ldg(t.sid + i);
+            lo = make_float3(__ldg(t.lo_s + 3 * sc), __ldg(t.lo_s + 3 * sc + 1),
+                __ldg(t.lo_s + 3 * sc + 2));
+            hi = make_float3(__ldg(t.hi_s + 3 * sc), __ldg(t.hi_s + 3 * sc + 1),
+                __ldg(t.hi_s + 3 * sc + 2));
+        }
         // _hard_enforce_bounds, scene.cu:466-483
-        if (px <= t.lo.x || py <= t.lo.y || pz <= t.lo.z || t.hi.x <= px || t.hi.y <= py
-            || t.hi.z <= pz) {
+        if (px <= lo.x || py <= lo.y || pz <= lo.z || hi.x <= px || hi.y <= py || hi.z <= pz) {
             const float d = (float)-0.1;
             nvx = nvx * d;
             nvy = nvy * d;
             nvz = nvz * d;
         }
-        px = fmaxf(fminf(px, t.hi.x), t.lo.x);
-        py = fmaxf(fminf(py, t.hi.y), t.lo.y);
-        pz = fmaxf(fminf(pz, t.hi.z), t.lo.z);
+        px = fmaxf(fminf(px, hi.x), lo.x);
+        py = fmaxf(fminf(py, hi.y), lo.y);
+        pz = fmaxf(fminf(pz, hi.z), lo.z);
     }
     vx[i] = nvx;
     vy[i] = nvy;
@@ -433,6 +534,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bd
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    enter_scene(f, b, i);
     const float4 me = f.pm[i];
     const int3 c = fluid_cell<R>(f, me);
     uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
@@ -491,6 +593,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_nonpressure(uint32_t n, Fluid f
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    enter_scene(f, i);
     const float4 me = f.pm[i];
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
@@ -530,6 +633,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_sesph(uint32_t n, Fluid f,
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     float vn = 0.f;
     if (i < n) {
+    enter_scene(f, i);
     const float4 me = f.pm[i];
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
@@ -569,7 +673,14 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_predict(uint32_t n, Flui
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 0.0;
-    if (i < n) {
+    const bool batched = f.g.sid != nullptr;
+    uint32_t sc = 0;
+    bool live = i < n;
+    if (live) {
+        sc = enter_scene(f, i);
+        live = scene_live(f, sc);
+    }
+    if (live) {
         const float4 me = f.pm[i];
         const float4 vi = vel[i];
         const int3 c = fluid_cell<R>(f, me);
@@ -588,7 +699,10 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_predict(uint32_t n, Flui
         rho[i] = r;
         contrib = r;
     }
-    block_accumulate(stats, 0u, 0.0, contrib, 0.f);
+    if (batched)
+        scene_accumulate(stats, sc, live, 0u, 0.0, contrib, 0.f);
+    else
+        block_accumulate(stats, 0u, 0.0, contrib, 0.f);
 }
 
 // _write_pcisph_prs_acc (PCISPH.cu:21-56) + v += dt a in place
@@ -599,6 +713,8 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_pressure(uint32_t n, Flu
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
+        return;
+    if (!scene_live(f, enter_scene(f, i)))
         return;
     const float4 me = f.pm[i];
     const int3 c = fluid_cell<R>(f, me);
@@ -658,6 +774,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    enter_scene(f, i);
     const float4 me = f.pm[i];
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
@@ -708,6 +825,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    enter_scene(f, i);
     const float4 me = f.pm[i];
     const float4 vi = vel[i];
     const int3 c = fluid_cell<R>(f, me);
@@ -761,6 +879,8 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
+    if (!scene_live(f, enter_scene(f, i)))
+        return;
     const float4 me = f.pm[i];
     const int3 c = fluid_cell<R>(f, me);
     const float pi = p[i];
@@ -793,7 +913,14 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
     unsigned over = 0;
     double epos = 0.0;
     float emax = 0.f;
-    if (i < n) {
+    const bool batched = f.g.sid != nullptr;
+    uint32_t sc = 0;
+    bool live = i < n;
+    if (live) {
+        sc = enter_scene(f, i);
+        live = scene_live(f, sc);
+    }
+    if (live) {
         const float4 me = f.pm[i];
         const int3 c = fluid_cell<R>(f, me);
         const float4 ai = acc[i];
@@ -825,7 +952,10 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
         epos = err > 0.f ? (double)err : 0.0;
         emax = fmaxf(err, 0.f);
     }
-    block_accumulate(stats, over, epos, 0.0, emax);
+    if (batched)
+        scene_accumulate(stats, sc, live, over, epos, 0.0, emax);
+    else
+        block_accumulate(stats, over, epos, 0.0, emax);
 }
 
 // final _set_pressure_accelerations + integrate (IISPH.cu:248-257)
@@ -839,6 +969,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     float vn = 0.f;
     if (i < n) {
+    enter_scene(f, i);
     const float4 me = f.pm[i];
     const int3 c = fluid_cell<R>(f, me);
     const float pi = p[i];
@@ -1000,6 +1131,27 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         sv.p_epoch = st.epoch;
     }
     sv.stats = reyn_step_stats {};
+    const uint32_t ns = grid.n_scenes;
+    require(!bdy || !bdy->nb || bdy->grid.n_scenes == ns,
+        "batched grids need a boundary batched over the same scenes");
+    sv.n_scenes = ns;
+    if (ns) {
+        sv.scene_stats.resize(size_t(ns) * sizeof(SweepStats));
+        sv.scene_active.resize(ns);
+        sv.scene_iters.resize(ns);
+        sv.scene_avg.resize(ns);
+        sv.scene_max.resize(ns);
+        sv.scene_first.resize(ns + 1);
+        sv.n_active.resize(1);
+        if (!sv.n_active_host)
+            sv.n_active_host = std::make_unique<PinnedArray<uint32_t>>(1);
+        REYN_CUDA(cudaMemcpyAsync(sv.scene_first.get(), grid.first.data(),
+            (ns + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        REYN_CUDA(cudaMemsetAsync(sv.scene_active.get(), 1, ns, s));
+        sv.scene_iters.zero(s);
+        sv.scene_avg.zero(s);
+        sv.scene_max.zero(s);
+    }
     if (n == 0)
         return;
 
@@ -1013,6 +1165,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     f.pmh = nullptr;
     f.acch = nullptr;
     f.acc32 = sv.acc.get();
+    f.active = ns ? sv.scene_active.get() : nullptr;
     Bdy b {};
     if (bdy && bdy->nb) {
         b.g = bdy->view();
@@ -1032,6 +1185,11 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         tail.lo = make_float3(bmin[0], bmin[1], bmin[2]);
         tail.hi = make_float3(bmax[0], bmax[1], bmax[2]);
         tail.vmax = sv.vmax.get();
+        if (ns) { // batched: every scene's own box
+            tail.sid = grid.sid.get();
+            tail.lo_s = grid.scene_lo.get();
+            tail.hi_s = grid.scene_hi.get();
+        }
     }
     const unsigned nb = blocks_for(n, NBR_THREADS);
     const float rho0 = P.rho0;
@@ -1053,6 +1211,20 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     };
     uint32_t iters = 0;
     bool converged = true;
+    // batched scenes: per-scene sums of the current sweep, then the per-scene
+    // convergence kernel; returns whether any scene iterates on
+    SweepStats* scene_slot = reinterpret_cast<SweepStats*>(sv.scene_stats.get());
+    auto scenes_go_on = [&](int mode) {
+        REYN_CUDA(cudaMemsetAsync(sv.n_active.get(), 0, sizeof(uint32_t), s));
+        REYN_KERNEL("k_scene_converge", s,
+            k_scene_converge<<<blocks_for(ns, THREADS), THREADS, 0, s>>>(ns, scene_slot,
+            sv.scene_first.get(), mode, P.eta, rho0, iters, sv.scene_active.get(),
+            sv.scene_iters.get(), sv.scene_avg.get(), sv.scene_max.get(), sv.n_active.get()));
+        REYN_CUDA(cudaMemcpyAsync(sv.n_active_host->get(), sv.n_active.get(), sizeof(uint32_t),
+            cudaMemcpyDeviceToHost, s));
+        REYN_CUDA(cudaStreamSynchronize(s));
+        return *sv.n_active_host->get() > 0;
+    };
 
     const bool mixed = P.precision != REYN_PRECISION_FP32;
     uint2* PMH = P.precision == REYN_PRECISION_MIXED_POS16 ? sv.pmh.get() : nullptr;
@@ -1073,6 +1245,12 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 k_sesph<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), sv.bterm.get(),
                 P.k_sesph, rho0, nu10, eps, grav, dt, sv.acc.get(), X, Y, Z, VX, VY, VZ, tail));
             iters = 1;
+            if (ns) { // one pass per scene
+                const std::vector<uint32_t> ones(ns, 1u);
+                REYN_CUDA(cudaMemcpyAsync(sv.scene_iters.get(), ones.data(), ns * sizeof(uint32_t),
+                    cudaMemcpyHostToDevice, s));
+                REYN_CUDA(cudaStreamSynchronize(s));
+            }
         } else if (sv.scheme == REYN_PCISPH) {
             const float kp = (float)((sv.pcisph_delta / dt) / dt); // PCISPH.cu:65
             REYN_KERNEL("k_nonpressure", s,
@@ -1080,8 +1258,8 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 eps, grav, dt, sv.acc.get(), sv.vel2.get(), nullptr));
             float4* v = sv.vel2.get();
             for (;;) {
-                SweepStats* slot = slots + (iters % 64);
-                REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats), s));
+                SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
+                REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
                 REYN_KERNEL("k_pcisph_predict", s,
                     k_pcisph_predict<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, v, sv.bterm.get(), dt,
                     sv.rho.get(), slot));
@@ -1089,6 +1267,18 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                     k_pcisph_pressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.rho.get(),
                     sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
                 iters += 1;
+                if (ns) {
+                    const bool last = P.max_iter && iters >= P.max_iter;
+                    if (iters < P.min_iter && !last)
+                        continue;
+                    if (!scenes_go_on(0))
+                        break;
+                    if (last) {
+                        converged = false;
+                        break;
+                    }
+                    continue;
+                }
                 if (P.max_iter && iters >= P.max_iter) {
                     if (iters >= P.min_iter) {
                         readback(slot);
@@ -1134,8 +1324,8 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             // IISPH.cu:219-250: [pressure accelerations, Jacobi update]* with
             // the first accelerations computed above
             for (;;) {
-                SweepStats* slot = slots + (iters % 64);
-                REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats), s));
+                SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
+                REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
                 REYN_KERNEL("k_iisph_jacobi", s,
                     k_iisph_jacobi<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.acc.get(),
                     sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, tiny,
@@ -1143,6 +1333,16 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 iters += 1;
                 const bool last = P.max_iter && iters >= P.max_iter;
                 if (iters < P.min_iter && !last) {
+                    pacc();
+                    continue;
+                }
+                if (ns) {
+                    if (!scenes_go_on(P.convergence == REYN_CONV_AVERAGE ? 1 : 2))
+                        break;
+                    if (last) {
+                        converged = false;
+                        break;
+                    }
                     pacc();
                     continue;
                 }

@@ -203,6 +203,77 @@ def dam_break_on_device(counts, h: float, box, rho0: float = 1000.0, jitter: flo
     return st, walls, box_min, box_max
 
 
+@dataclass
+class Batch:
+    """Independent scenes sharing spacing and kernel: scene s owns fluid
+    particles first[s] .. first[s+1]-1 and wall samples bfirst[s] ..
+    bfirst[s+1]-1, in its own box [0, box_max[s]] (all boxes share the
+    origin; the frame is their union)."""
+    h: float
+    rho0: float
+    fluid: dict
+    bdy: dict
+    first: np.ndarray
+    bfirst: np.ndarray
+    box_min: np.ndarray   # (n_scenes, 3)
+    box_max: np.ndarray   # (n_scenes, 3)
+    counts: list
+
+    @property
+    def n_scenes(self) -> int:
+        return int(self.first.size - 1)
+
+    @property
+    def frame_min(self) -> np.ndarray:
+        return self.box_min.min(0)
+
+    @property
+    def frame_max(self) -> np.ndarray:
+        return self.box_max.max(0)
+
+
+def batch_counts(n_scenes: int, nmin: int, nmax: int, seed: int) -> list:
+    """Per-scene fluid cubes with particle counts drawn log-uniform from
+    [nmin, nmax] (counter-based, stream 6): cube edges of round(N^(1/3))."""
+    u = uniform01(seed, 6, np.arange(n_scenes)).astype(np.float64)
+    n = np.exp(np.log(nmin) + u * (np.log(nmax) - np.log(nmin)))
+    edge = np.maximum(2, np.rint(np.cbrt(n))).astype(int)
+    return [(int(e), int(e), int(e)) for e in edge]
+
+
+def batched_dam_breaks(counts, h: float, rho0: float = 1000.0, jitter: float = 0.05,
+                       seed: int = 4, mass_kernel: str | None = None,
+                       gap: float = 1.5) -> Batch:
+    """One dam break per entry of `counts`: the block `gap` spacings from the
+    corner of a box twice its width in x and 1.5 times in y and z."""
+    fl, bd, first, bfirst, lo, hi = [], [], [0], [0], [], []
+    for s, c in enumerate(counts):
+        ext = np.asarray(c, np.float64) * h
+        box = np.float32(np.array([2.0, 1.5, 1.5]) * ext + 2 * gap * h)
+        o = gap * h
+        f = fluid_block(c, h, (o, o, o), rho0, jitter, seed, mass_kernel=mass_kernel,
+                        first=first[-1])
+        w = box_walls((0, 0, 0), box, h)
+        fl.append(f)
+        bd.append(w)
+        first.append(first[-1] + f["x"].size)
+        bfirst.append(bfirst[-1] + w["x"].size)
+        lo.append(np.zeros(3, np.float32))
+        hi.append(box)
+    fluid = {k: np.concatenate([f[k] for f in fl]) for k in fl[0]}
+    bdy = {k: np.concatenate([w[k] for w in bd]) for k in ("x", "y", "z")}
+    return Batch(h, rho0, fluid, bdy, np.asarray(first, np.uint32), np.asarray(bfirst, np.uint32),
+                 np.asarray(lo, np.float32), np.asarray(hi, np.float32), list(counts))
+
+
+def batched_pcisph(n_scenes: int = 256, seed: int = 4, nmin: int = 2000,
+                   nmax: int = 200000) -> Batch:
+    """The batched PCISPH workload: n_scenes fluid cubes of log-uniform
+    particle counts in [nmin, nmax] at spacing 0.01, each a dam break in its
+    own closed box."""
+    return batched_dam_breaks(batch_counts(n_scenes, nmin, nmax, seed), 0.01, seed=seed)
+
+
 def sesph_small(seed: int = 1) -> Scene:
     """SESPH dam break: 32^3 fluid particles at spacing 0.02, jitter +-0.1 h,
     unit box with Akinci walls at spacing 0.02."""
