@@ -79,6 +79,11 @@ def parse_args():
                     help="all: time FP32 and mixed_pos16, then report the mixed path beside them")
     ap.add_argument("--order", choices=["xyz", "zorder"], default="xyz",
                     help="cell order of the grid the state is sorted by")
+    ap.add_argument("--workload", choices=["iisph_4m", "batched_pcisph"], default="iisph_4m",
+                    help="batched_pcisph: 256 independent PCISPH scenes (not the headline)")
+    ap.add_argument("--scenes", type=int, default=256, help="batched_pcisph: scene count")
+    ap.add_argument("--no-sequential", action="store_true",
+                    help="batched_pcisph: skip the scene-by-scene comparison run")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -530,12 +535,146 @@ def run_reference(a, world, rank):
     print(json.dumps(out), flush=True)
 
 
+# ---- batched workload ----------------------------------------------------------
+
+BATCH_DT = 2e-4
+
+
+def run_batched(a, world, rank, local):
+    """256 independent PCISPH dam breaks (cube particle counts log-uniform in
+    [2000, 200000], spacing 0.01, cubic B-spline, 1 % density tolerance,
+    fixed dt 2e-4) stepped as one batch: one grid, boundary and solver over
+    all scenes, one launch per phase. For comparison the same scenes are
+    then stepped one after another, each with its own grid, boundary and
+    solver (the same engine without batching)."""
+    import torch
+
+    import reyn_b200 as rb
+    from reyn_b200 import scenes
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    S = stream.cuda_stream
+    b = scenes.batched_pcisph(n_scenes=a.scenes, seed=4 + rank)
+    n = int(b.first[-1])
+
+    def params():
+        prm = rb.reference_params(rb.PCISPH, rb.B3, b.h, b.rho0, NU)
+        prm.eta = 0.01  # 1 % average density error
+        prm.max_iter = 100
+        return prm
+
+    st = rb.Particles(n, b.rho0)
+    st.upload(b.fluid)
+    bd = rb.Boundary(*(torch.tensor(b.bdy[k], device=dev) for k in ("x", "y", "z")), None,
+                     h=b.h, rho0=b.rho0, scene_first=b.bfirst)
+    grid = rb.Grid(b.frame_min, b.frame_max, 2 * b.h, 0.5, 0, scene_first=b.first,
+                   scene_min=b.box_min, scene_max=b.box_max)
+    sv = rb.Solver(rb.PCISPH, params(), n)
+    its = []
+
+    def step():
+        grid.construct_and_reorder(st, stream=S)
+        its.append(sv.step_batched(st, grid, bd, BATCH_DT, stream=S))
+
+    for _ in range(a.warmup):
+        step()
+    its.clear()
+    torch.cuda.synchronize()
+    gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    clocks = ClockSampler(gpu_uuid)
+    time.sleep(0.3)
+    rb.profile_reset()
+    rb.profile_enable(True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    rb.profile_enable(False)
+    prof = rb.profile_read()
+    ck_clocks = clocks.stop()
+    ms = max_over_ranks(world, e0.elapsed_time(e1))
+    value = world * n * a.steps / (ms / 1e3)
+    it = np.array(its)
+    for o in (sv, grid, bd, st):
+        o.close()
+
+    seq = None
+    if not a.no_sequential:
+        # the same scenes, each with its own grid, boundary and solver,
+        # stepped one after another
+        runs = []
+        for s in range(b.n_scenes):
+            lo, hi = int(b.first[s]), int(b.first[s + 1])
+            blo, bhi = int(b.bfirst[s]), int(b.bfirst[s + 1])
+            pst = rb.Particles(hi - lo, b.rho0)
+            pst.upload({k: v[lo:hi] for k, v in b.fluid.items()})
+            pbd = rb.Boundary(*(torch.tensor(b.bdy[k][blo:bhi], device=dev)
+                                for k in ("x", "y", "z")), None, h=b.h, rho0=b.rho0)
+            pg = rb.Grid(b.box_min[s], b.box_max[s], 2 * b.h)
+            psv = rb.Solver(rb.PCISPH, params(), hi - lo)
+            runs.append((pst, pbd, pg, psv, (b.box_min[s], b.box_max[s])))
+
+        def seq_step():
+            for pst, pbd, pg, psv, box in runs:
+                pg.construct_and_reorder(pst, stream=S)
+                psv.step(pst, pg, pbd, BATCH_DT, stream=S, bounds=box)
+
+        for _ in range(a.warmup):
+            seq_step()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(a.steps):
+            seq_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sms = max_over_ranks(world, e0.elapsed_time(e1))
+        seq = {"value": round(world * n * a.steps / (sms / 1e3), 1), "unit": UNIT,
+               "ms_per_step": round(sms / a.steps, 3),
+               "launches_per_step": "one set of phase launches per scene"}
+        for r in runs:
+            for o in r[:4]:
+                o.close()
+
+    launches = sum(v[0] for v in prof.values())
+    out = {
+        "metric": "particle-steps/s, batched PCISPH, 256 scenes", "value": round(value, 1),
+        "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": round(ms / a.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded log-uniform cube sizes, lattice + jitter, Akinci box walls)",
+        "config": {"workload": "batched_pcisph", "scenes": b.n_scenes, "particles": n,
+                   "boundary_particles": int(b.bfirst[-1]), "kernel": "B3", "h": b.h,
+                   "tolerance": "1 % average density error", "dt": BATCH_DT,
+                   "precision": "fp32 (the mixed modes are IISPH only)",
+                   "parallelism": f"replicas{world}"},
+        "clocks": ck_clocks, "gpu_launches": launches,
+        "iters_per_step_max": it.max(1).tolist(), "iters_per_step_mean":
+            [round(float(x), 2) for x in it.mean(1)],
+        "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in
+                    sorted(prof.items(), key=lambda kv: -kv[1][1])},
+        "sequential": seq,
+    }
+    if seq:
+        out["batched_over_sequential"] = round(value / seq["value"], 3)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     a = parse_args()
     world, rank, local = dist_setup()
     try:
         if a.impl == "reference":
             run_reference(a, world, rank)
+        elif a.workload == "batched_pcisph":
+            run_batched(a, world, rank, local)
         else:
             run_engine(a, world, rank, local)
     finally:

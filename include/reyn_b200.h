@@ -304,7 +304,10 @@ int reyn_solver_step_bounded(reyn_solver* s, reyn_particles* state,
     const float bound_min[3], const float bound_max[3], uint32_t* iters,
     void* stream);
 
-/* per-particle solver buffers (device, grid order of the last step) */
+/* per-particle solver buffers (device, grid order of the last step): rho
+ * the (predicted) densities, ax..az the last accelerations; p the IISPH
+ * pressure, for PCISPH the pressure term p / rho^2 of the last iteration
+ * (_eos_pcisph, PCISPH.cu:15-19); aii, sii the IISPH diagonal and source */
 typedef struct reyn_solver_buffers {
     const float *rho, *p, *aii, *sii, *ax, *ay, *az;
     uint32_t n;

@@ -669,7 +669,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_sesph(uint32_t n, Fluid f,
 template <int KIND, int R>
 __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_predict(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const float4* __restrict__ bterm, float dt,
-    float* __restrict__ rho, SweepStats* stats)
+    float* __restrict__ rho, float k, float rho0, float* __restrict__ pr, SweepStats* stats)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 0.0;
@@ -697,6 +697,9 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_predict(uint32_t n, Flui
         const float4 bt = bterm[i];
         r += bt.w + dt * fmaf(bt.x, vi.x, fmaf(bt.y, vi.y, bt.z * vi.z));
         rho[i] = r;
+        // the pressure term p / rho^2 of the next pass (_eos_pcisph,
+        // PCISPH.cu:15-19), once per particle instead of once per pair
+        pr[i] = fmaxf(0.f, k * (r - rho0)) / (r * r);
         contrib = r;
     }
     if (batched)
@@ -708,7 +711,8 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_predict(uint32_t n, Flui
 // _write_pcisph_prs_acc (PCISPH.cu:21-56) + v += dt a in place
 template <int KIND, int R>
 __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_pressure(uint32_t n, Fluid f,
-    const float* __restrict__ rho, const float4* __restrict__ bterm, float k, float rho0,
+    const float* __restrict__ rho, const float* __restrict__ pr,
+    const float4* __restrict__ bterm, float k, float rho0,
     float r0i, float dt, float4* __restrict__ acc, float4* __restrict__ vel)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -724,9 +728,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_pressure(uint32_t n, Flu
     float ax = 0.f, ay = 0.f, az = 0.f;
     for_each_listed<R>(f, i, c, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
-            const float rj = __ldg(rho + j);
-            const float pj = fmaxf(0.f, k * (rj - rho0));
-            const float s = q.w * (pri + pj / (rj * rj)) * pair_g<KIND>(f.kc, l2);
+            const float s = q.w * (pri + __ldg(pr + j)) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
             ay += s * dy;
             az += s * dz;
@@ -1262,10 +1264,10 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
                 REYN_KERNEL("k_pcisph_predict", s,
                     k_pcisph_predict<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, v, sv.bterm.get(), dt,
-                    sv.rho.get(), slot));
+                    sv.rho.get(), kp, rho0, sv.p.get(), slot));
                 REYN_KERNEL("k_pcisph_pressure", s,
                     k_pcisph_pressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.rho.get(),
-                    sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
+                    sv.p.get(), sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
                 iters += 1;
                 if (ns) {
                     const bool last = P.max_iter && iters >= P.max_iter;
