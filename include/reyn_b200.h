@@ -139,15 +139,14 @@ int reyn_grid_destroy(reyn_grid* g);
  * Scene s owns the particles [first[s], first[s+1]) of one reyn_particles
  * (n_scenes + 1 host offsets) and lies in its own box scene_min/max[3s..3s+2]
  * (host arrays; the boxes may overlap in space: scenes never see each
- * other). Every scene is gridded over the common frame frame_min/max (which
- * must contain every scene box) with its own range of cell keys, so one
- * launch per phase serves every scene and a reorder keeps each scene's
- * particles in its own index range. prefix has n_scenes * n_keys + 1
- * entries. At most 65535 scenes. */
-int reyn_grid_create_batched(const float frame_min[3], const float frame_max[3],
-    float search_radius, float cell_ratio, reyn_cell_order order,
-    uint32_t n_scenes, const uint32_t* first, const float* scene_min,
-    const float* scene_max, reyn_grid** out);
+ * other). Each scene gets the grid a reyn_grid_create over its own box
+ * would get, with its own range of cell keys after the previous scene's, so
+ * one launch per phase serves every scene and a reorder keeps each scene's
+ * particles in its own index range. The grid info's prefix covers all
+ * scenes' keys. At most 65535 scenes. */
+int reyn_grid_create_batched(float search_radius, float cell_ratio,
+    reyn_cell_order order, uint32_t n_scenes, const uint32_t* first,
+    const float* scene_min, const float* scene_max, reyn_grid** out);
 /* construct (uniformgrid.cu:145-156): builds prefix + sorted for n
  * positions (device arrays), particles are not moved. Within a cell the
  * indices are ascending (a stable counting sort), which is the canonical

@@ -109,8 +109,7 @@ _SIGNATURES = {
                              ctypes.POINTER(ctypes.c_uint64), _vp],
     "reyn_scene_sphere": [_f * 3, _f, _f, _vp, _vp, _vp, _u32, ctypes.POINTER(_u32), _vp],
     "reyn_scene_cull": [_vp, _vp, _f, ctypes.POINTER(_u32), _vp],
-    "reyn_grid_create_batched": [_f * 3, _f * 3, _f, _f, ctypes.c_int, _u32, _vp, _vp, _vp,
-                                 ctypes.POINTER(_vp)],
+    "reyn_grid_create_batched": [_f, _f, ctypes.c_int, _u32, _vp, _vp, _vp, ctypes.POINTER(_vp)],
     "reyn_boundary_create_batched": [_vp, _vp, _vp, _vp, _u32, _u32, _vp, _f, _f, _u32, _vp,
                                      ctypes.POINTER(_vp)],
     "reyn_solver_step_batched": [_vp, _vp, _vp, _vp, _f, ctypes.c_int, _vp, _vp],
@@ -248,8 +247,8 @@ class Grid:
     def __init__(self, bmin, bmax, search_radius: float, cell_ratio: float = 0.5,
                  order: int = 0, scene_first=None, scene_min=None, scene_max=None):
         """With scene_first (n_scenes + 1 offsets) and per-scene boxes
-        scene_min/max (n_scenes x 3): a batched grid over the frame
-        [bmin, bmax] (reyn_grid_create_batched)."""
+        scene_min/max (n_scenes x 3): a batched grid, each scene gridded over
+        its own box (reyn_grid_create_batched; bmin and bmax are unused)."""
         h = _vp()
         self.n_scenes = 0
         if scene_first is None:
@@ -260,10 +259,9 @@ class Grid:
             lo = np.ascontiguousarray(scene_min, np.float32).reshape(-1)
             hi = np.ascontiguousarray(scene_max, np.float32).reshape(-1)
             self.n_scenes = first.size - 1
-            check(lib().reyn_grid_create_batched(_f3(bmin), _f3(bmax), search_radius, cell_ratio,
-                                                 order, self.n_scenes, first.ctypes.data,
-                                                 lo.ctypes.data, hi.ctypes.data,
-                                                 ctypes.byref(h)))
+            check(lib().reyn_grid_create_batched(search_radius, cell_ratio, order, self.n_scenes,
+                                                 first.ctypes.data, lo.ctypes.data,
+                                                 hi.ctypes.data, ctypes.byref(h)))
         self.h = h
         self.r = search_radius
 

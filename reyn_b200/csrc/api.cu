@@ -160,25 +160,28 @@ int reyn_grid_create(const float bound_min[3], const float bound_max[3], float s
     });
 }
 
-int reyn_grid_create_batched(const float frame_min[3], const float frame_max[3],
-    float search_radius, float cell_ratio, reyn_cell_order order, uint32_t n_scenes,
-    const uint32_t* first, const float* scene_min, const float* scene_max, reyn_grid** out)
+int reyn_grid_create_batched(float search_radius, float cell_ratio, reyn_cell_order order,
+    uint32_t n_scenes, const uint32_t* first, const float* scene_min, const float* scene_max,
+    reyn_grid** out)
 {
     return guard([&] {
         require(out != nullptr, "null output handle");
         *out = nullptr;
-        check_vec3(frame_min, "frame_min must be 3 finite floats");
-        check_vec3(frame_max, "frame_max must be 3 finite floats");
         require(first && scene_min && scene_max, "null scene arrays");
+        require(n_scenes >= 1, "at least one scene");
         require(order == REYN_ORDER_XYZ || order == REYN_ORDER_ZORDER, "unknown cell order");
         for (uint32_t k = 0; k < 3 * n_scenes; ++k)
             require(std::isfinite(scene_min[k]) && std::isfinite(scene_max[k])
                     && scene_min[k] <= scene_max[k],
                 "scene boxes must be finite and ordered");
         auto g = std::make_unique<reyn_grid>();
-        g->geom = make_geom(frame_min, frame_max, search_radius, cell_ratio, order);
+        std::vector<GridGeom> geoms(n_scenes);
+        for (uint32_t k = 0; k < n_scenes; ++k) // each scene: the grid of its own box
+            geoms[k] = make_geom(scene_min + 3 * k, scene_max + 3 * k, search_radius, cell_ratio,
+                order);
+        g->geom = geoms[0];
         g->ratio = cell_ratio;
-        g->set_scenes(first, n_scenes, nullptr);
+        g->set_scenes(first, n_scenes, geoms.data(), nullptr);
         g->scene_lo.resize(3 * size_t(n_scenes));
         g->scene_hi.resize(3 * size_t(n_scenes));
         REYN_CUDA(cudaMemcpy(g->scene_lo.get(), scene_min, 3 * size_t(n_scenes) * sizeof(float),
@@ -251,7 +254,7 @@ int reyn_grid_info_get(const reyn_grid* g, reyn_grid_info* out)
         out->prefix = g->prefix.get();
         out->sorted = g->reordered ? nullptr : g->sorted.get();
         out->order = g->geom.order;
-        out->n_keys = uint32_t(g->geom.keys());
+        out->n_keys = uint32_t(g->total_keys());
     });
 }
 

@@ -163,10 +163,19 @@ struct GridView {
     int order;      // REYN_ORDER_XYZ or REYN_ORDER_ZORDER
     int tx, txy;    // Z-order: 32-cell tiles along x, per xy layer
     const uint32_t* __restrict__ prefix;
-    // batched scenes: scene of each point (null for one scene); scene s's
-    // cells are keyed s * key_stride + its own key
+    // batched scenes: scene of each point (null for one scene) and each
+    // scene's own grid geometry, whose cell keys start at its key_base
     const uint16_t* __restrict__ sid;
-    uint32_t key_stride;
+    const struct SceneGeom* __restrict__ scenes;
+    uint32_t key_base; // of the scene this view is narrowed to
+};
+
+// one scene of a batch: its grid's lower bound (with margin), cell counts
+// and the first of its cell keys
+struct SceneGeom {
+    float lox, loy, loz;
+    int nx, ny, nz, nxny, tx, txy;
+    uint32_t key_base;
 };
 
 __device__ __forceinline__ uint32_t scene_of(const GridView& g, uint32_t i)
@@ -174,11 +183,25 @@ __device__ __forceinline__ uint32_t scene_of(const GridView& g, uint32_t i)
     return g.sid ? uint32_t(__ldg(g.sid + i)) : 0u;
 }
 
-// the view of scene s alone (its keys start at prefix + s * key_stride)
+// the view of scene s alone: its geometry, and its prefix slice
 __device__ __forceinline__ GridView at_scene(GridView g, uint32_t s)
 {
-    g.prefix += size_t(s) * g.key_stride;
+    if (g.scenes) {
+        const SceneGeom q = g.scenes[s];
+        g.lox = q.lox;
+        g.loy = q.loy;
+        g.loz = q.loz;
+        g.nx = q.nx;
+        g.ny = q.ny;
+        g.nz = q.nz;
+        g.nxny = q.nxny;
+        g.tx = q.tx;
+        g.txy = q.txy;
+        g.key_base = q.key_base;
+        g.prefix += q.key_base;
+    }
     g.sid = nullptr;
+    g.scenes = nullptr;
     return g;
 }
 

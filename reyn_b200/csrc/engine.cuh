@@ -63,9 +63,14 @@ struct Grid {
     uint32_t n_scenes = 0;
     std::vector<uint32_t> first;
     DevArray<uint16_t> sid;
+    std::vector<GridGeom> scene_geom; // each scene's own grid
+    std::vector<uint32_t> key_base;   // first key of each scene (n_scenes + 1)
+    DevArray<SceneGeom> scene_tab;
     DevArray<float> scene_lo, scene_hi; // per-scene boxes (3 floats each), fluid grids
-    int64_t total_keys() const { return geom.keys() * int64_t(n_scenes ? n_scenes : 1); }
-    void set_scenes(const uint32_t* first, uint32_t n_scenes, cudaStream_t s);
+    int64_t total_keys() const { return n_scenes ? int64_t(key_base[n_scenes]) : geom.keys(); }
+    // scenes with their own geometries (n_scenes entries)
+    void set_scenes(const uint32_t* first, uint32_t n_scenes, const GridGeom* geoms,
+        cudaStream_t s);
     bool counts_dirty = false; // a build stopped between histogram and scatter
     bool reordered = false;    // last build was construct_and_reorder
     const reyn_particles* reordered_state = nullptr;

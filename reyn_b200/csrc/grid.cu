@@ -62,7 +62,8 @@ GridView Grid::view(float search_radius) const
     v.txy = geom.t[0] * geom.t[1];
     v.prefix = prefix.get();
     v.sid = n_scenes ? sid.get() : nullptr;
-    v.key_stride = uint32_t(geom.keys());
+    v.scenes = n_scenes ? scene_tab.get() : nullptr;
+    v.key_base = 0;
     return v;
 }
 
@@ -86,6 +87,7 @@ __global__ void k_keys_count(uint32_t n, const float* __restrict__ x,
     uint32_t key = 0xffffffffu;
     if (valid) {
         const float px = x[i], py = y[i], pz = z[i];
+        g = at_scene(g, scene_of(g, i)); // batched: the point's own scene grid
         int3 c = cell_of(g, px, py, pz);
         const bool finite = isfinite(px) && isfinite(py) && isfinite(pz);
         const bool inside = finite && c.x >= 0 && c.y >= 0 && c.z >= 0
@@ -96,7 +98,7 @@ __global__ void k_keys_count(uint32_t n, const float* __restrict__ x,
                              min(max(c.z, 0), g.nz - 1))
                        : make_int3(0, 0, 0);
         }
-        key = cell_key(g, c.x, c.y, c.z) + scene_of(g, i) * g.key_stride;
+        key = cell_key(g, c.x, c.y, c.z) + g.key_base;
         keys[i] = key;
     }
     const unsigned group = __match_any_sync(0xffffffffu, key);
@@ -352,24 +354,40 @@ __global__ void k_fill_sid(uint32_t n, const uint32_t* __restrict__ first, uint3
     sid[i] = uint16_t(lo);
 }
 
-void Grid::set_scenes(const uint32_t* f, uint32_t ns, cudaStream_t s)
+void Grid::set_scenes(const uint32_t* f, uint32_t ns, const GridGeom* geoms, cudaStream_t s)
 {
     require(ns >= 1 && ns <= 65535, "1 .. 65535 scenes");
     require(f != nullptr && f[0] == 0, "scene offsets must start at 0");
     for (uint32_t k = 0; k < ns; ++k)
         require(f[k] <= f[k + 1], "scene offsets must not decrease");
-    require(geom.keys() * int64_t(ns) < (int64_t(1) << 32) - 1,
-        "scenes x cells exceed 32-bit keys");
+    std::vector<SceneGeom> tab(ns);
+    key_base.assign(ns + 1, 0);
+    int64_t total = 0;
+    for (uint32_t k = 0; k < ns; ++k) {
+        const GridGeom& q = geoms[k];
+        require(q.cell == geom.cell && q.range == geom.range && q.order == geom.order,
+            "the scenes of a batch share the cell size and order");
+        tab[k] = SceneGeom { q.lo[0], q.lo[1], q.lo[2], q.n[0], q.n[1], q.n[2], q.n[0] * q.n[1],
+            q.t[0], q.t[0] * q.t[1], uint32_t(total) };
+        key_base[k] = uint32_t(total);
+        total += q.keys();
+        require(total < (int64_t(1) << 32) - 1, "the scenes' cells exceed 32-bit keys");
+    }
+    key_base[ns] = uint32_t(total);
+    scene_geom.assign(geoms, geoms + ns);
+    scene_tab.resize(ns);
+    REYN_CUDA(cudaMemcpy(scene_tab.get(), tab.data(), ns * sizeof(SceneGeom),
+        cudaMemcpyHostToDevice));
     n_scenes = ns;
     first.assign(f, f + ns + 1);
-    const uint32_t total = first[ns];
-    sid.resize(total);
-    if (total) {
+    const uint32_t np_total = first[ns];
+    sid.resize(np_total);
+    if (np_total) {
         DevArray<uint32_t> fd(ns + 1);
         REYN_CUDA(cudaMemcpyAsync(fd.get(), first.data(), (ns + 1) * sizeof(uint32_t),
             cudaMemcpyHostToDevice, s));
         REYN_KERNEL("k_fill_sid", s,
-            k_fill_sid<<<blocks_for(total, THREADS), THREADS, 0, s>>>(total, fd.get(), ns,
+            k_fill_sid<<<blocks_for(np_total, THREADS), THREADS, 0, s>>>(np_total, fd.get(), ns,
             sid.get()));
         REYN_CUDA(cudaStreamSynchronize(s));
     }
@@ -666,8 +684,9 @@ __global__ void k_mark_near(uint32_t n, GridView g, const float4* __restrict__ p
     if (i >= n)
         return;
     const float4 me = pts[i];
+    g = at_scene(g, scene_of(g, i)); // batched: the sample's own scene grid
+    near += g.key_base;
     const int3 c = clamp_cell(g, cell_of(g, me.x, me.y, me.z), 2);
-    near += size_t(scene_of(g, i)) * g.key_stride; // batched: the sample's scene
     for (int dz = -2; dz <= 2; ++dz)
         for (int dy = -2; dy <= 2; ++dy) {
             const int base = (c.z + dz) * g.nxny + (c.y + dy) * g.nx + c.x;
@@ -710,8 +729,37 @@ void boundary_build(reyn_boundary& b, const float* bx, const float* by, const fl
     // the boundary grid: support 2h over the samples' own bounds, reference
     // geometry (sample_boundary.cu:420-428)
     b.grid.geom = make_geom(lo, hi, 2.f * h, 0.5f);
-    if (n_scenes) // batched: one grid per scene, keyed scene-major
-        b.grid.set_scenes(scene_first, n_scenes, s);
+    if (n_scenes) {
+        // batched: every scene's samples get the grid a boundary of their
+        // own would get (over their own bounds), keyed scene after scene
+        DevArray<unsigned> sbox(size_t(6) * n_scenes);
+        std::vector<unsigned> sinit(size_t(6) * n_scenes);
+        for (uint32_t k = 0; k < n_scenes; ++k)
+            std::copy(init, init + 6, sinit.begin() + 6 * size_t(k));
+        REYN_CUDA(cudaMemcpyAsync(sbox.get(), sinit.data(), sinit.size() * sizeof(unsigned),
+            cudaMemcpyHostToDevice, s));
+        for (uint32_t k = 0; k < n_scenes; ++k) {
+            const uint32_t a = scene_first[k], cnt = scene_first[k + 1] - a;
+            require(cnt > 0, "every scene of a batched boundary needs samples");
+            REYN_KERNEL("k_bounds", s,
+                k_bounds<<<blocks_for(cnt, THREADS), THREADS, 0, s>>>(cnt, bx + a, by + a, bz + a,
+                sbox.get() + 6 * size_t(k)));
+        }
+        std::vector<unsigned> hsb(sinit.size());
+        REYN_CUDA(cudaMemcpyAsync(hsb.data(), sbox.get(), hsb.size() * sizeof(unsigned),
+            cudaMemcpyDeviceToHost, s));
+        REYN_CUDA(cudaStreamSynchronize(s));
+        std::vector<GridGeom> geoms(n_scenes);
+        for (uint32_t k = 0; k < n_scenes; ++k) {
+            float slo[3], shi[3];
+            for (int a = 0; a < 3; ++a) {
+                slo[a] = from_ordered_bits(hsb[6 * k + a]);
+                shi[a] = from_ordered_bits(hsb[6 * k + 3 + a]);
+            }
+            geoms[k] = make_geom(slo, shi, 2.f * h, 0.5f);
+        }
+        b.grid.set_scenes(scene_first, n_scenes, geoms.data(), s);
+    }
     b.grid.build(bx, by, bz, nb, s);
     b.grid.check_status(s, "boundary grid");
     b.x.resize(nb);

@@ -217,8 +217,8 @@ __device__ __forceinline__ uint32_t enter_scene(Fluid& f, Bdy& b, uint32_t i)
 {
     const uint32_t s = enter_scene(f, i);
     if (b.n && b.g.sid) {
-        b.near += size_t(s) * b.g.key_stride;
         b.g = at_scene(b.g, s);
+        b.near += b.g.key_base;
     }
     return s;
 }
@@ -234,9 +234,9 @@ __device__ __forceinline__ bool scene_live(const Fluid& f, uint32_t s)
 // is the neighbour's position on the FP32 path; on the mixed path with ACC it
 // is the neighbour's pressure acceleration times ACC_SCALE (from the FP16
 // record, or FP32 for a particle off the list).
-template <int R, int MIX = 0, bool ACC = false, class F>
-__device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3 c,
-    const float4& me, F&& fn)
+template <int R, int MIX = 0, bool ACC = false, bool BATCH = false, class F>
+__device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, const float4& me,
+    F&& fn)
 {
     static_assert(MIX || !ACC, "accelerations travel with the mixed records only");
     const uint32_t cnt = __ldg(f.ncount + i);
@@ -297,7 +297,15 @@ __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, int3
             fn(j, q, dx, dy, dz, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
         }
     } else {
-        for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+        // the cell traversal: the particle's (scene's) grid and cell, found
+        // only here, as the density pass already checked the positions
+        GridView g = f.g;
+        if constexpr (BATCH)
+            g = at_scene(g, scene_of(g, i));
+        int3 c = cell_of(g, me.x, me.y, me.z);
+        if (!cell_inside(g, c, R)) // flagged by the density pass already
+            c = clamp_cell(g, c, R);
+        for_each_neighbour<R>(g, c, me.x, me.y, me.z, f.pm,
             [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
                 if (j == i)
                     return;
@@ -526,7 +534,7 @@ __device__ __forceinline__ void tail_reduce(const Tail& t, float v)
 // region, so the L2 merges the scattered 4-byte stores into full lines).
 // Mixed precision: the particle's 8-byte position and velocity records are
 // written for later passes.
-template <int KIND, int R, int MIX = 0>
+template <int KIND, int R, int MIX = 0, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bdy b,
     float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm,
     uint2* __restrict__ pmh_out, uint2* __restrict__ velh_out)
@@ -534,7 +542,8 @@ __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bd
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    enter_scene(f, b, i);
+    if constexpr (BATCH)
+        enter_scene(f, b, i);
     const float4 me = f.pm[i];
     const int3 c = fluid_cell<R>(f, me);
     uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
@@ -584,7 +593,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_density(uint32_t n, Fluid f, Bd
 // write_non_prs_acc_ff (solver.cuh:40-69): gravity + artificial viscosity;
 // optionally fused with integrate_a_v_only (solver.cu:3-13) into vel_out
 // (and its FP16 copy velh_out under mixed precision)
-template <int KIND, int R, int MIX = 0>
+template <int KIND, int R, int MIX = 0, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_nonpressure(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const uint2* __restrict__ velh, float nu10, float eps,
     float3 grav, float dt, float4* __restrict__ acc, float4* __restrict__ vel_out,
@@ -593,12 +602,10 @@ __global__ void __launch_bounds__(NBR_THREADS) k_nonpressure(uint32_t n, Fluid f
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    enter_scene(f, i);
     const float4 me = f.pm[i];
     const float4 vi = vel[i];
-    const int3 c = fluid_cell<R>(f, me);
     float ax = grav.x, ay = grav.y, az = grav.z;
-    for_each_listed<R, MIX>(f, i, c, me,
+    for_each_listed<R, MIX, false, BATCH>(f, i, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float4 vj = nbr_vel<MIX>(vel, velh, j);
             const float vdx = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
@@ -623,7 +630,7 @@ __device__ __forceinline__ float eos_sesph(float rho, float k, float rho0)
 
 // _compute_accelerations (SESPH.cu:15-65) fused with integrate (solver.cu:
 // 15-32): writes the new SoA state
-template <int KIND, int R>
+template <int KIND, int R, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_sesph(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const float4* __restrict__ bterm, float k, float rho0,
     float nu10, float eps, float3 grav, float dt, float4* __restrict__ acc,
@@ -633,14 +640,12 @@ __global__ void __launch_bounds__(NBR_THREADS) k_sesph(uint32_t n, Fluid f,
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     float vn = 0.f;
     if (i < n) {
-    enter_scene(f, i);
     const float4 me = f.pm[i];
     const float4 vi = vel[i];
-    const int3 c = fluid_cell<R>(f, me);
     const float pi = eos_sesph(vi.w, k, rho0);
     const float pri = pi / (vi.w * vi.w);
     float ax = grav.x, ay = grav.y, az = grav.z;
-    for_each_listed<R>(f, i, c, me,
+    for_each_listed<R, 0, false, BATCH>(f, i, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float4 vj = __ldg(vel + j);
             const float pj = eos_sesph(vj.w, k, rho0);
@@ -666,27 +671,28 @@ __global__ void __launch_bounds__(NBR_THREADS) k_sesph(uint32_t n, Fluid f,
 
 // predict_rho (solver.cuh:71-105); the boundary part uses the cached sums:
 // sum_b m_b (W + dt grad W . v_i) = rho_b + dt g_b . v_i
-template <int KIND, int R>
+template <int KIND, int R, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_predict(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const float4* __restrict__ bterm, float dt,
     float* __restrict__ rho, float k, float rho0, float* __restrict__ pr, SweepStats* stats)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 0.0;
-    const bool batched = f.g.sid != nullptr;
+    constexpr bool batched = BATCH;
     uint32_t sc = 0;
     bool live = i < n;
     if (live) {
-        sc = enter_scene(f, i);
-        live = scene_live(f, sc);
+        if constexpr (BATCH) {
+            sc = scene_of(f.g, i);
+            live = scene_live(f, sc);
+        }
     }
     if (live) {
         const float4 me = f.pm[i];
         const float4 vi = vel[i];
-        const int3 c = fluid_cell<R>(f, me);
         // the list excludes the particle itself: its term is m_i W(0)
         float r = me.w * pair_w<KIND>(f.kc, 0.f);
-        for_each_listed<R>(f, i, c, me,
+        for_each_listed<R, 0, false, BATCH>(f, i, me,
             [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
                 const float4 vj = __ldg(vel + j);
                 float w, g;
@@ -702,14 +708,14 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_predict(uint32_t n, Flui
         pr[i] = fmaxf(0.f, k * (r - rho0)) / (r * r);
         contrib = r;
     }
-    if (batched)
+    if constexpr (batched)
         scene_accumulate(stats, sc, live, 0u, 0.0, contrib, 0.f);
     else
         block_accumulate(stats, 0u, 0.0, contrib, 0.f);
 }
 
 // _write_pcisph_prs_acc (PCISPH.cu:21-56) + v += dt a in place
-template <int KIND, int R>
+template <int KIND, int R, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_pressure(uint32_t n, Fluid f,
     const float* __restrict__ rho, const float* __restrict__ pr,
     const float4* __restrict__ bterm, float k, float rho0,
@@ -718,15 +724,16 @@ __global__ void __launch_bounds__(NBR_THREADS) k_pcisph_pressure(uint32_t n, Flu
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    if (!scene_live(f, enter_scene(f, i)))
-        return;
+    if constexpr (BATCH) {
+        if (!scene_live(f, scene_of(f.g, i)))
+            return;
+    }
     const float4 me = f.pm[i];
-    const int3 c = fluid_cell<R>(f, me);
     const float ri = rho[i];
     const float pi = fmaxf(0.f, k * (ri - rho0));
     const float pri = pi / (ri * ri);
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_listed<R>(f, i, c, me,
+    for_each_listed<R, 0, false, BATCH>(f, i, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float s = q.w * (pri + __ldg(pr + j)) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
@@ -766,7 +773,7 @@ __global__ void k_advect(uint32_t n, const float4* __restrict__ pm,
 
 // _compute_diagonal_elem_and_source_term (IISPH.cu:11-66) + warm start
 // (IISPH.cu:193-209)
-template <int KIND, int R, int MIX = 0>
+template <int KIND, int R, int MIX = 0, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const uint2* __restrict__ velh,
     const float4* __restrict__ bterm, float rho0, float dt,
@@ -776,13 +783,11 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    enter_scene(f, i);
     const float4 me = f.pm[i];
     const float4 vi = vel[i];
-    const int3 c = fluid_cell<R>(f, me);
     float gx = 0.f, gy = 0.f, gz = 0.f, vdiv = 0.f, gsq = 0.f;
     [[maybe_unused]] Kahan vk; // mixed modes: compensated divergence sum
-    for_each_listed<R, MIX>(f, i, c, me,
+    for_each_listed<R, MIX, false, BATCH>(f, i, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float4 vj = nbr_vel<MIX>(vel, velh, j);
             const float g = pair_g<KIND>(f.kc, l2);
@@ -816,7 +821,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag(uint32_t n, Fluid f,
 // carried pressure, so a_i = -(1/rho0^2)(sum m_j (p_i' + p_j') grad W_ij +
 // p_i' g_b) with p' = 0.5 p can be summed in the same neighbour loop. p_old
 // is read, p_new written (p_new = 0.5 p_old).
-template <int KIND, int R, int MIX = 0>
+template <int KIND, int R, int MIX = 0, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Fluid f,
     const float4* __restrict__ vel, const uint2* __restrict__ velh,
     const float4* __restrict__ bterm, float rho0, float dt,
@@ -827,15 +832,13 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    enter_scene(f, i);
     const float4 me = f.pm[i];
     const float4 vi = vel[i];
-    const int3 c = fluid_cell<R>(f, me);
     const float pi = p_old[i] * 0.5f;
     float gx = 0.f, gy = 0.f, gz = 0.f, vdiv = 0.f, gsq = 0.f;
     [[maybe_unused]] Kahan vk; // mixed modes: compensated divergence sum
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_listed<R, MIX>(f, i, c, me,
+    for_each_listed<R, MIX, false, BATCH>(f, i, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float4 vj = nbr_vel<MIX>(vel, velh, j);
             const float pj = __ldg(p_old + j) * 0.5f;
@@ -873,7 +876,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_diag_pacc(uint32_t n, Flu
 }
 
 // _set_pressure_accelerations (IISPH.cu:68-98)
-template <int KIND, int R, int MIX = 0>
+template <int KIND, int R, int MIX = 0, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     float4* __restrict__ acc, uint2* __restrict__ acch_out)
@@ -881,13 +884,14 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    if (!scene_live(f, enter_scene(f, i)))
-        return;
+    if constexpr (BATCH) {
+        if (!scene_live(f, scene_of(f.g, i)))
+            return;
+    }
     const float4 me = f.pm[i];
-    const int3 c = fluid_cell<R>(f, me);
     const float pi = p[i];
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_listed<R, MIX>(f, i, c, me,
+    for_each_listed<R, MIX, false, BATCH>(f, i, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float s = q.w * (pi + __ldg(p + j)) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
@@ -905,7 +909,7 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_pacc(uint32_t n, Fluid f,
 // _jacobi_update_pressures (IISPH.cu:119-162); the convergence bitmask of the
 // reference becomes a count of particles above the threshold, reduced per
 // block together with the FP64 sum of max(0, error)
-template <int KIND, int R, int MIX = 0>
+template <int KIND, int R, int MIX = 0, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid f,
     const float4* __restrict__ acc, const float4* __restrict__ bterm,
     const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
@@ -915,23 +919,24 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
     unsigned over = 0;
     double epos = 0.0;
     float emax = 0.f;
-    const bool batched = f.g.sid != nullptr;
+    constexpr bool batched = BATCH;
     uint32_t sc = 0;
     bool live = i < n;
     if (live) {
-        sc = enter_scene(f, i);
-        live = scene_live(f, sc);
+        if constexpr (BATCH) {
+            sc = scene_of(f.g, i);
+            live = scene_live(f, sc);
+        }
     }
     if (live) {
         const float4 me = f.pm[i];
-        const int3 c = fluid_cell<R>(f, me);
         const float4 ai = acc[i];
         // mixed: neighbour accelerations arrive scaled by ACC_SCALE; the own
         // one is scaled to match and the sum scaled back
         constexpr float AS = MIX ? ACC_SCALE : 1.f;
         const float3 as = make_float3(ai.x * AS, ai.y * AS, ai.z * AS);
         float sum = 0.f;
-        for_each_listed<R, MIX, (MIX != 0)>(f, i, c, me,
+        for_each_listed<R, MIX, (MIX != 0), BATCH>(f, i, me,
             [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
                 float3 aj;
                 if constexpr (MIX) {
@@ -954,14 +959,14 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_jacobi(uint32_t n, Fluid 
         epos = err > 0.f ? (double)err : 0.0;
         emax = fmaxf(err, 0.f);
     }
-    if (batched)
+    if constexpr (batched)
         scene_accumulate(stats, sc, live, over, epos, 0.0, emax);
     else
         block_accumulate(stats, over, epos, 0.0, emax);
 }
 
 // final _set_pressure_accelerations + integrate (IISPH.cu:248-257)
-template <int KIND, int R, int MIX = 0>
+template <int KIND, int R, int MIX = 0, bool BATCH = false>
 __global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     const float4* __restrict__ vel, float dt, float4* __restrict__ acc,
@@ -971,12 +976,10 @@ __global__ void __launch_bounds__(NBR_THREADS) k_iisph_final(uint32_t n, Fluid f
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     float vn = 0.f;
     if (i < n) {
-    enter_scene(f, i);
     const float4 me = f.pm[i];
-    const int3 c = fluid_cell<R>(f, me);
     const float pi = p[i];
     float ax = 0.f, ay = 0.f, az = 0.f;
-    for_each_listed<R, MIX>(f, i, c, me,
+    for_each_listed<R, MIX, false, BATCH>(f, i, me,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float s = q.w * (pi + __ldg(p + j)) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
@@ -1136,6 +1139,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     const uint32_t ns = grid.n_scenes;
     require(!bdy || !bdy->nb || bdy->grid.n_scenes == ns,
         "batched grids need a boundary batched over the same scenes");
+    require(!ns || P.precision == REYN_PRECISION_FP32, "batched scenes run in FP32");
     sv.n_scenes = ns;
     if (ns) {
         sv.scene_stats.resize(size_t(ns) * sizeof(SweepStats));
@@ -1235,16 +1239,17 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     uint2* VH2 = mixed ? sv.velh2.get() : nullptr;
     f.pmh = PMH;
     f.acch = ACH;
-    auto body = [&](auto KC, auto RC, auto MC) {
+    auto body = [&](auto KC, auto RC, auto MC, auto BC) {
         constexpr int K = decltype(KC)::value;
         constexpr int R = decltype(RC)::value;
         constexpr int MIX = decltype(MC)::value;
+        constexpr bool B = decltype(BC)::value;
         REYN_KERNEL("k_density", s,
-            k_density<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, b, sv.rho.get(), st.vel.get(),
+            k_density<K, R, MIX, B><<<nb, NBR_THREADS, 0, s>>>(n, f, b, sv.rho.get(), st.vel.get(),
             sv.bterm.get(), PMH, VH));
         if (sv.scheme == REYN_SESPH) {
             REYN_KERNEL("k_sesph", s,
-                k_sesph<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), sv.bterm.get(),
+                k_sesph<K, R, B><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), sv.bterm.get(),
                 P.k_sesph, rho0, nu10, eps, grav, dt, sv.acc.get(), X, Y, Z, VX, VY, VZ, tail));
             iters = 1;
             if (ns) { // one pass per scene
@@ -1256,17 +1261,17 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         } else if (sv.scheme == REYN_PCISPH) {
             const float kp = (float)((sv.pcisph_delta / dt) / dt); // PCISPH.cu:65
             REYN_KERNEL("k_nonpressure", s,
-                k_nonpressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), nullptr, nu10,
+                k_nonpressure<K, R, 0, B><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), nullptr, nu10,
                 eps, grav, dt, sv.acc.get(), sv.vel2.get(), nullptr));
             float4* v = sv.vel2.get();
             for (;;) {
                 SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
                 REYN_KERNEL("k_pcisph_predict", s,
-                    k_pcisph_predict<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, v, sv.bterm.get(), dt,
+                    k_pcisph_predict<K, R, B><<<nb, NBR_THREADS, 0, s>>>(n, f, v, sv.bterm.get(), dt,
                     sv.rho.get(), kp, rho0, sv.p.get(), slot));
                 REYN_KERNEL("k_pcisph_pressure", s,
-                    k_pcisph_pressure<K, R><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.rho.get(),
+                    k_pcisph_pressure<K, R, B><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.rho.get(),
                     sv.p.get(), sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
                 iters += 1;
                 if (ns) {
@@ -1301,23 +1306,23 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 VX, VY, VZ, tail));
         } else { // IISPH
             REYN_KERNEL("k_nonpressure", s,
-                k_nonpressure<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), VH, nu10,
+                k_nonpressure<K, R, MIX, B><<<nb, NBR_THREADS, 0, s>>>(n, f, st.vel.get(), VH, nu10,
                 eps, grav, dt, sv.acc.get(), sv.vel2.get(), VH2));
             const float tiny = tiny_threshold();
             auto pacc = [&] {
                 REYN_KERNEL("k_iisph_pacc", s,
-                    k_iisph_pacc<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(),
+                    k_iisph_pacc<K, R, MIX, B><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(),
                     sv.bterm.get(), r0i, sv.acc.get(), ACH));
             };
             if (P.warmstart) {
                 REYN_KERNEL("k_iisph_diag_pacc", s,
-                    k_iisph_diag_pacc<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
+                    k_iisph_diag_pacc<K, R, MIX, B><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
                     VH2, sv.bterm.get(), rho0, dt, r0i, sv.p.get(), sv.aii.get(), sv.sii.get(),
                     sv.p_tmp.get(), sv.acc.get(), ACH));
                 sv.p.swap(sv.p_tmp);
             } else {
                 REYN_KERNEL("k_iisph_diag", s,
-                    k_iisph_diag<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
+                    k_iisph_diag<K, R, MIX, B><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.vel2.get(),
                     VH2, sv.bterm.get(), rho0, dt, P.omega, P.warmstart, tiny, sv.aii.get(),
                     sv.sii.get(), sv.p.get()));
                 pacc();
@@ -1329,7 +1334,7 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
                 REYN_KERNEL("k_iisph_jacobi", s,
-                    k_iisph_jacobi<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.acc.get(),
+                    k_iisph_jacobi<K, R, MIX, B><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.acc.get(),
                     sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, tiny,
                     thr, slot));
                 iters += 1;
@@ -1363,17 +1368,19 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 pacc();
             }
             REYN_KERNEL("k_iisph_final", s,
-                k_iisph_final<K, R, MIX><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
+                k_iisph_final<K, R, MIX, B><<<nb, NBR_THREADS, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
                 r0i, sv.vel2.get(), dt, sv.acc.get(), X, Y, Z, VX, VY, VZ, tail));
         }
     };
     dispatch(P.kernel, grid.geom.range, [&](auto KC, auto RC) {
-        if (P.precision == REYN_PRECISION_MIXED_POS16)
-            body(KC, RC, std::integral_constant<int, MIX_POS16> {});
+        if (ns) // batched scenes: FP32
+            body(KC, RC, std::integral_constant<int, 0> {}, std::true_type {});
+        else if (P.precision == REYN_PRECISION_MIXED_POS16)
+            body(KC, RC, std::integral_constant<int, MIX_POS16> {}, std::false_type {});
         else if (mixed)
-            body(KC, RC, std::integral_constant<int, MIX_F16> {});
+            body(KC, RC, std::integral_constant<int, MIX_F16> {}, std::false_type {});
         else
-            body(KC, RC, std::integral_constant<int, 0> {});
+            body(KC, RC, std::integral_constant<int, 0> {}, std::false_type {});
     });
     REYN_KERNEL("k_unpack_acc", s,
         k_unpack_acc<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, sv.acc.get(), sv.ax.get(),
