@@ -69,6 +69,13 @@ template <> struct Shape<K_C2> { // w = (1-q)_+^4 (4q+1)
         const float t = fmaxf(0.f, 1.f - q);
         return t * t * t * (-20.f * q);
     }
+    // dw(q) / q: the gradient's 1/|x| cancels against q = |x| / h_bar
+    static constexpr bool kDwOverQ = true;
+    __host__ __device__ static float dw_over_q(float q)
+    {
+        const float t = fmaxf(0.f, 1.f - q);
+        return t * t * t * -20.f;
+    }
 };
 
 template <> struct Shape<K_B3> { // w = (1-q)_+^3 - 4 (1/2-q)_+^3
@@ -102,6 +109,14 @@ template <> struct Shape<K_W6> { // w = (1-q)_+^8 (32q^3 + 25q^2 + 8q + 1)
         const float t7 = t2 * t2 * t2 * t;
         return t7 * ((16.f * q * q + 7.f * q + 1.f) * (-22.f * q));
     }
+    static constexpr bool kDwOverQ = true;
+    __host__ __device__ static float dw_over_q(float q)
+    {
+        const float t = fmaxf(0.f, 1.f - q);
+        const float t2 = t * t;
+        const float t7 = t2 * t2 * t2 * t;
+        return t7 * ((16.f * q * q + 7.f * q + 1.f) * -22.f);
+    }
 };
 
 template <> struct Shape<K_COS> { // w = 4 cos(pi q) + cos(2 pi q) + 3
@@ -129,13 +144,32 @@ __device__ __forceinline__ float pair_w(const KernelConst& k, float l2)
     return k.w_scale * Shape<KIND>::w(__saturatef(len * k.h_inv));
 }
 
+template <int KIND, class = void> struct HasDwOverQ {
+    static constexpr bool value = false;
+};
+template <int KIND>
+struct HasDwOverQ<KIND, decltype(void(Shape<KIND>::kDwOverQ))> {
+    static constexpr bool value = Shape<KIND>::kDwOverQ;
+};
+
+// the gradient factor g with grad W(x) = g x. For the Wendland kernels dw(q)
+// carries a factor q, so g = dw_scale / h_bar * dw(q) / q needs no division
+// by |x|; at x = 0 it is finite and multiplies a zero vector. Otherwise the
+// reference's form dw_scale * dw(q) / |x| with its non-finite guard
+// (kernels.cuh:51-64).
 template <int KIND>
 __device__ __forceinline__ float pair_g(const KernelConst& k, float l2)
 {
     const float inv = rsqrtf(l2);
-    const float len = l2 * inv;
-    const float g = k.dw_scale * Shape<KIND>::dw(len * k.h_inv) * inv;
-    return (l2 > 0.f && isfinite(g)) ? g : 0.f;
+    if constexpr (HasDwOverQ<KIND>::value) {
+        // coincident points (l2 = 0) get the finite g at q = 0
+        const float len = l2 > 0.f ? l2 * inv : 0.f;
+        return (k.dw_scale * k.h_inv) * Shape<KIND>::dw_over_q(len * k.h_inv);
+    } else {
+        const float len = l2 * inv;
+        const float g = k.dw_scale * Shape<KIND>::dw(len * k.h_inv) * inv;
+        return (l2 > 0.f && isfinite(g)) ? g : 0.f;
+    }
 }
 
 template <int KIND>
