@@ -84,6 +84,8 @@ def parse_args():
     ap.add_argument("--scenes", type=int, default=256, help="batched_pcisph: scene count")
     ap.add_argument("--no-sequential", action="store_true",
                     help="batched_pcisph: skip the scene-by-scene comparison run")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="skip the block-size / cell-ratio autotuner (128 threads, cell r/2)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -225,7 +227,8 @@ class EngineRun:
     """The workload on the engine: one scene, its grid, boundary and solver,
     and the main-loop step (main.cu:64-75)."""
 
-    def __init__(self, rank: int, scale: int, dev, precision: str, order: str = "xyz"):
+    def __init__(self, rank: int, scale: int, dev, precision: str, order: str = "xyz",
+                 ratio: float = 0.5, block: int = 0):
         import reyn_b200 as rb
 
         self.rb = rb
@@ -234,19 +237,25 @@ class EngineRun:
         self.n = sc.n
         self.st = sc.st
         self.bd = rb.Boundary(*sc.walls, None, h=sc.h, rho0=sc.rho0, mass_iters=5)
-        self.grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h, 0.5,
+        self.grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h, ratio,
                             rb.ORDER_ZORDER if order == "zorder" else rb.ORDER_XYZ)
+        prm = self.params(rb, sc, precision)
+        prm.block_size = block
+        self.sv = rb.Solver(rb.IISPH, prm, sc.n)
+        self.dt, self.iters = DT0, 0
+        self.dt_visc = viscous_dt_limit(sc.h, NU)
+        self.log = []
+        self.limit_hits = 0
+
+    @staticmethod
+    def params(rb, sc, precision):
         prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, NU)
         prm.convergence = rb.CONV_AVERAGE
         prm.eta = 0.001
         prm.max_iter = 1000
         prm.precision = {"mixed": rb.PRECISION_MIXED, "mixed_pos16": rb.PRECISION_MIXED_POS16,
                          "fp32": rb.PRECISION_FP32}[precision]
-        self.sv = rb.Solver(rb.IISPH, prm, sc.n)
-        self.dt, self.iters = DT0, 0
-        self.dt_visc = viscous_dt_limit(sc.h, NU)
-        self.log = []
-        self.limit_hits = 0
+        return prm
 
     def step(self, S):
         rb, sc = self.rb, self.sc
@@ -336,20 +345,36 @@ def run_engine(a, world, rank, local):
     stream = torch.cuda.current_stream(dev)
     S = stream.cuda_stream
 
+    headline = "mixed" if a.precision == "all" else a.precision
+    # the autotuner (block size of the neighbour passes, cell size) on the
+    # headline configuration, from the scene's initial state
+    ratio, block, tuned = 0.5, 0, None
+    if not a.no_autotune:
+        sc = DeviceScene(rank, a.scale)
+        bd = rb.Boundary(*sc.walls, None, h=sc.h, rho0=sc.rho0, mass_iters=5)
+        best, pts = rb.autotune(rb.IISPH, EngineRun.params(rb, sc, headline), sc.st, bd,
+                                viscous_dt_limit(sc.h, NU), steps=3,
+                                bounds=(sc.box_min, sc.box_max), stream=S)
+        ratio, block = best.cell_ratio, best.block_size
+        tuned = [{"block_size": p.block_size, "cell_ratio": p.cell_ratio,
+                  "ms_per_step": round(p.ms_per_step, 3)} for p in pts]
+        bd.close()
+        sc.st.close()
+        torch.cuda.synchronize()
+
     # the plain FP32 path and the 16-bit-position variant first, on the same
     # scene, as the comparison legs
     legs = {}
     if a.precision == "all":
         for name in ("fp32", "mixed_pos16"):
-            run = EngineRun(rank, a.scale, dev, name, a.order)
+            run = EngineRun(rank, a.scale, dev, name, a.order, ratio, block)
             _, _, msl, _, clk, logl = timed_steps(run, a, world, stream, dev)
             legs[name] = leg_summary(run, a, world, msl, logl)
             legs[name]["clocks"] = clk
             run.close()
             torch.cuda.synchronize()
 
-    headline = "mixed" if a.precision == "all" else a.precision
-    run = EngineRun(rank, a.scale, dev, headline, a.order)
+    run = EngineRun(rank, a.scale, dev, headline, a.order, ratio, block)
     n = run.n
     ck, ms, ms_max, prof, ck_clocks, log = timed_steps(run, a, world, stream, dev)
     value = world * n * a.steps / (ms_max / 1e3)
@@ -422,10 +447,11 @@ def run_engine(a, world, rank, local):
                    "dt": f"min(simple_dt_controller(lambda={LAMBDA}, target 10 iters, "
                          f"0.1%/step) from {DT0}, 0.08 h^2/nu = {run.dt_visc:.2e})",
                    "precision": precision, "cell_order": a.order,
+                   "block_size": block or 128, "cell_ratio": ratio,
                    "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (state 4M x 28 B + grid 70 MB per step)"},
         "clocks": ck_clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-        "cpu_baseline": cpu,
+        "cpu_baseline": cpu, "autotune": tuned,
         "iters_per_step": [x[0] for x in log],
         "avg_density_error_per_step": [round(x[1], 7) for x in log],
         "dt_per_step": [float(f"{x[2]:.4e}") for x in log],
@@ -568,9 +594,19 @@ def run_batched(a, world, rank, local):
     st.upload(b.fluid)
     bd = rb.Boundary(*(torch.tensor(b.bdy[k], device=dev) for k in ("x", "y", "z")), None,
                      h=b.h, rho0=b.rho0, scene_first=b.bfirst)
-    grid = rb.Grid(b.frame_min, b.frame_max, 2 * b.h, 0.5, 0, scene_first=b.first,
+    tuned, ratio, block = None, 0.5, 0
+    if not a.no_autotune:
+        best, pts = rb.autotune(rb.PCISPH, params(), st, bd, BATCH_DT, steps=2,
+                                scene_first=b.first, scene_min=b.box_min, scene_max=b.box_max,
+                                stream=S)
+        ratio, block = best.cell_ratio, best.block_size
+        tuned = [{"block_size": p.block_size, "cell_ratio": p.cell_ratio,
+                  "ms_per_step": round(p.ms_per_step, 3)} for p in pts]
+    grid = rb.Grid(b.frame_min, b.frame_max, 2 * b.h, ratio, 0, scene_first=b.first,
                    scene_min=b.box_min, scene_max=b.box_max)
-    sv = rb.Solver(rb.PCISPH, params(), n)
+    prm = params()
+    prm.block_size = block
+    sv = rb.Solver(rb.PCISPH, prm, n)
     its = []
 
     def step():
@@ -617,8 +653,8 @@ def run_batched(a, world, rank, local):
             pst.upload({k: v[lo:hi] for k, v in b.fluid.items()})
             pbd = rb.Boundary(*(torch.tensor(b.bdy[k][blo:bhi], device=dev)
                                 for k in ("x", "y", "z")), None, h=b.h, rho0=b.rho0)
-            pg = rb.Grid(b.box_min[s], b.box_max[s], 2 * b.h)
-            psv = rb.Solver(rb.PCISPH, params(), hi - lo)
+            pg = rb.Grid(b.box_min[s], b.box_max[s], 2 * b.h, ratio)
+            psv = rb.Solver(rb.PCISPH, prm, hi - lo)
             runs.append((pst, pbd, pg, psv, (b.box_min[s], b.box_max[s])))
 
         def seq_step():
@@ -653,7 +689,9 @@ def run_batched(a, world, rank, local):
                    "boundary_particles": int(b.bfirst[-1]), "kernel": "B3", "h": b.h,
                    "tolerance": "1 % average density error", "dt": BATCH_DT,
                    "precision": "fp32 (the mixed modes are IISPH only)",
+                   "block_size": block or 128, "cell_ratio": ratio,
                    "parallelism": f"replicas{world}"},
+        "autotune": tuned,
         "clocks": ck_clocks, "gpu_launches": launches,
         "iters_per_step_max": it.max(1).tolist(), "iters_per_step_mean":
             [round(float(x), 2) for x in it.mean(1)],

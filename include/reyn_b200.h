@@ -267,6 +267,8 @@ typedef struct reyn_params {
     int32_t warmstart;      /* IISPH p *= 0.5 (IISPH.cuh:48) */
     reyn_convergence convergence;
     reyn_precision precision; /* REYN_PRECISION_FP32 unless set */
+    uint32_t block_size;    /* threads per block of the neighbour passes:
+                               64, 128, 256 or 512; 0 = 128 */
 } reyn_params;
 
 /* the reference's constants for `scheme` (gravity (0,-9.81,0)) */
@@ -367,6 +369,25 @@ int reyn_solver_next_dt(reyn_solver* s, reyn_particles* state,
 /* ---- bounds (src/scene/scene.cu:466-491) ---------------------------------- */
 int reyn_enforce_bounds(reyn_particles* state, const float bound_min[3],
     const float bound_max[3], void* stream);
+
+/* ---- autotuner (no counterpart in the reference) -------------------------- */
+typedef struct reyn_tune_point {
+    uint32_t block_size;  /* threads per block of the neighbour passes */
+    float cell_ratio;     /* cell size / search radius */
+    float ms_per_step;    /* grid build with reorder + solver step */
+} reyn_tune_point;
+/* Times the caller's workload for every block size in {64, 128, 256, 512}
+ * and cell ratio in {0.5, 1.0}: each from the state as it is on entry,
+ * with a fresh grid and solver, one untimed step, then `steps` timed steps.
+ * One scene: bound_min/max are its grid bounds; a batch: n_scenes > 0 with
+ * the scene arrays of reyn_grid_create_batched (bdy batched likewise). The
+ * state is restored before returning. *best is the fastest combination;
+ * points (may be NULL) receives all eight. Synchronises the stream. */
+int reyn_autotune(reyn_scheme scheme, const reyn_params* params,
+    reyn_particles* state, const reyn_boundary* bdy, const float bound_min[3],
+    const float bound_max[3], uint32_t n_scenes, const uint32_t* first,
+    const float* scene_min, const float* scene_max, float dt, uint32_t steps,
+    reyn_tune_point* best, reyn_tune_point* points, void* stream);
 
 /* ---- scene generation (src/scene/scene.cu) ------------------------------- */
 /* _init_box_kernel (scene.cu:14-37) with seeded jitter (scene.cu:232-253):

@@ -57,7 +57,11 @@ class Params(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int), ("h", _f), ("rho0", _f), ("nu", _f), ("g", _f * 3),
                 ("k_sesph", _f), ("eta", _f), ("min_iter", _u32), ("max_iter", _u32),
                 ("omega", _f), ("warmstart", ctypes.c_int32), ("convergence", ctypes.c_int),
-                ("precision", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("block_size", _u32)]
+
+
+class TunePoint(ctypes.Structure):
+    _fields_ = [("block_size", _u32), ("cell_ratio", _f), ("ms_per_step", _f)]
 
 
 class SolverBuffers(ctypes.Structure):
@@ -114,6 +118,8 @@ _SIGNATURES = {
                                      ctypes.POINTER(_vp)],
     "reyn_solver_step_batched": [_vp, _vp, _vp, _vp, _f, ctypes.c_int, _vp, _vp],
     "reyn_solver_scene_stats": [_vp, _u32, _vp],
+    "reyn_autotune": [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp, _f, _u32,
+                      _vp, _vp, _vp],
     "reyn_solver_step": [_vp, _vp, _vp, _vp, _f, ctypes.POINTER(_u32), _vp],
     "reyn_solver_step_bounded": [_vp, _vp, _vp, _vp, _f, _f * 3, _f * 3, ctypes.POINTER(_u32),
                                  _vp],
@@ -508,6 +514,26 @@ def scene_cull(state: Particles, bdy: Boundary, radius: float, stream=None) -> i
     check(lib().reyn_scene_cull(state.h, bdy.h, radius, ctypes.byref(n), _stream(stream)))
     state.n = n.value
     return n.value
+
+
+def autotune(scheme: int, params: Params, state: Particles, bdy, dt: float, steps: int = 3,
+             bounds=None, scene_first=None, scene_min=None, scene_max=None, stream=None):
+    """reyn_autotune: returns (best, all eight) as TunePoint records."""
+    best = TunePoint()
+    pts = (TunePoint * 8)()
+    if scene_first is None:
+        check(lib().reyn_autotune(scheme, ctypes.byref(params), state.h, bdy.h if bdy else None,
+                                  _f3(bounds[0]), _f3(bounds[1]), 0, None, None, None, dt, steps,
+                                  ctypes.byref(best), pts, _stream(stream)))
+    else:
+        first = np.ascontiguousarray(scene_first, np.uint32)
+        lo = np.ascontiguousarray(scene_min, np.float32).reshape(-1)
+        hi = np.ascontiguousarray(scene_max, np.float32).reshape(-1)
+        check(lib().reyn_autotune(scheme, ctypes.byref(params), state.h, bdy.h if bdy else None,
+                                  None, None, first.size - 1, first.ctypes.data, lo.ctypes.data,
+                                  hi.ctypes.data, dt, steps, ctypes.byref(best), pts,
+                                  _stream(stream)))
+    return best, list(pts)
 
 
 def profile_enable(on: bool = True) -> None:

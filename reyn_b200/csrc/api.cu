@@ -38,6 +38,9 @@ void check_params(reyn_scheme scheme, const reyn_params* p)
         "unknown precision");
     require(p->precision == REYN_PRECISION_FP32 || scheme == REYN_IISPH,
         "mixed precision is implemented for IISPH");
+    require(p->block_size == 0 || p->block_size == 64 || p->block_size == 128
+            || p->block_size == 256 || p->block_size == 512,
+        "block_size must be 0, 64, 128, 256 or 512");
 }
 
 void check_vec3(const float* v, const char* what)
@@ -362,6 +365,7 @@ int reyn_params_reference(reyn_scheme scheme, reyn_kernel kernel, float h, float
         p.warmstart = 1; // IISPH.cuh:48
         p.convergence = REYN_CONV_REFERENCE;
         p.precision = REYN_PRECISION_FP32;
+        p.block_size = 0;
         *out = p;
     });
 }

@@ -183,7 +183,8 @@ enum StatusBits : uint32_t {
 };
 
 constexpr int THREADS = 256; // threads per block of the streaming kernels
-constexpr int NBR_THREADS = 128; // threads per block of the neighbour loops
+constexpr int NBR_THREADS = 128; // default threads per block of the neighbour loops
+constexpr int NBR_MAX_THREADS = 512; // largest block size they are compiled for
 
 inline unsigned blocks_for(size_t n, int threads)
 {

@@ -337,3 +337,47 @@ def test_bounded_step_equals_step_then_bounds(cuda, scheme, kind):
     assert clamped > 0
     for k in ("x", "y", "z", "vx", "vy", "vz"):
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+@pytest.mark.parametrize("block", [64, 256, 512])
+def test_block_size_gives_the_same_step(cuda, block):
+    """The neighbour passes at any block size compute the same particles'
+    sums in the same order; only the FP64 reductions may add in another
+    order (iteration counts must agree)."""
+    import reyn_b200 as rb
+    sc = scenes.dam_break((20, 18, 16), 0.02, (0.6, 0.6, 0.6), velocity_noise=0.05, seed=5)
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    bdy = dict(sc.bdy, m=bm)
+    out = []
+    for b in (128, block):
+        prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, 0.01)
+        prm.block_size = b
+        out.append(run_engine(2, 0, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0,
+                              0.01, 1e-3, 3, params=prm))
+    assert out[0]["iters"] == out[1]["iters"]
+    compare_steps(out[1], out[0], 2, STEP_TOL, f"block {block}")
+
+
+def test_autotune_covers_the_grid_and_restores_the_state(cuda):
+    import torch
+
+    import reyn_b200 as rb
+    sc = scenes.dam_break((24, 20, 16), 0.02, (0.8, 0.6, 0.6), velocity_noise=0.05, seed=8)
+    dev = torch.device("cuda")
+    st = rb.Particles(sc.n, sc.rho0)
+    st.upload(sc.fluid)
+    bd = rb.Boundary(*(torch.tensor(sc.bdy[k], device=dev) for k in ("x", "y", "z")), None,
+                     h=sc.h, rho0=sc.rho0)
+    before = st.download()
+    prm = rb.reference_params(rb.PCISPH, rb.B3, sc.h, sc.rho0, 0.01)
+    best, pts = rb.autotune(rb.PCISPH, prm, st, bd, 1e-3, steps=2,
+                            bounds=(sc.box_min, sc.box_max))
+    after = st.download()
+    for k in before:
+        np.testing.assert_array_equal(before[k], after[k])
+    combos = {(p.block_size, p.cell_ratio) for p in pts}
+    assert combos == {(b, r) for b in (64, 128, 256, 512) for r in (0.5, 1.0)}
+    assert all(p.ms_per_step > 0 for p in pts)
+    assert best.ms_per_step == min(p.ms_per_step for p in pts)
+    for o in (bd, st):
+        o.close()
