@@ -479,6 +479,7 @@ struct Tail {
 
 // stores the new state of particle i (bounds applied when tail.vmax is set)
 // and returns |v| of what was stored
+template <bool BATCH = false>
 __device__ __forceinline__ float store_state(const Tail& t, uint32_t i, float px, float py,
     float pz, float nvx, float nvy, float nvz, float* __restrict__ x, float* __restrict__ y,
     float* __restrict__ z, float* __restrict__ vx, float* __restrict__ vy,
@@ -486,7 +487,7 @@ __device__ __forceinline__ float store_state(const Tail& t, uint32_t i, float px
 {
     if (t.vmax) {
         float3 lo = t.lo, hi = t.hi;
-        if (t.sid) {
+        if (BATCH && t.sid) {
             const uint32_t sc = __ldg(t.sid + i);
             lo = make_float3(__ldg(t.lo_s + 3 * sc), __ldg(t.lo_s + 3 * sc + 1),
                 __ldg(t.lo_s + 3 * sc + 2));
@@ -614,7 +615,8 @@ __global__ void __launch_bounds__(MB) k_nonpressure(uint32_t n, Fluid f,
         [&](uint32_t j, const float4& q, float dx, float dy, float dz, float l2) {
             const float4 vj = nbr_vel<MIX>(vel, velh, j);
             const float vdx = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
-            const float s = (nu10 * q.w / vj.w * vdx) / (l2 + eps) * pair_g<KIND>(f.kc, l2);
+            // one division per pair: (10 nu m_j v_ij.x_ij / rho_j) / (l2 + eps) g
+            const float s = (nu10 * q.w * vdx * pair_g<KIND>(f.kc, l2)) / (vj.w * (l2 + eps));
             ax += s * dx;
             ay += s * dy;
             az += s * dz;
@@ -655,7 +657,7 @@ __global__ void __launch_bounds__(MB) k_sesph(uint32_t n, Fluid f,
             const float4 vj = __ldg(vel + j);
             const float pj = eos_sesph(vj.w, k, rho0);
             const float vdx = fmaf(vi.x - vj.x, dx, fmaf(vi.y - vj.y, dy, (vi.z - vj.z) * dz));
-            const float visc = (nu10 * q.w / vj.w * vdx) / (l2 + eps);
+            const float visc = (nu10 * q.w * vdx) / (vj.w * (l2 + eps));
             const float prs = q.w * (pri + pj / (vj.w * vj.w));
             const float s = (visc - prs) * pair_g<KIND>(f.kc, l2);
             ax += s * dx;
@@ -668,7 +670,7 @@ __global__ void __launch_bounds__(MB) k_sesph(uint32_t n, Fluid f,
     az -= pri * bt.z;
     acc[i] = make_float4(ax, ay, az, 0.f);
     const float nvx = vi.x + dt * ax, nvy = vi.y + dt * ay, nvz = vi.z + dt * az;
-    vn = store_state(tail, i, me.x + dt * nvx, me.y + dt * nvy, me.z + dt * nvz, nvx, nvy, nvz,
+    vn = store_state<BATCH>(tail, i, me.x + dt * nvx, me.y + dt * nvy, me.z + dt * nvz, nvx, nvy, nvz,
         x, y, z, vx, vy, vz);
     }
     tail_reduce(tail, vn);
@@ -760,6 +762,7 @@ __global__ void __launch_bounds__(MB) k_pcisph_pressure(uint32_t n, Fluid f,
 
 // the final position update of integrate (solver.cu:15-32) when v already
 // holds v + dt a
+template <bool BATCH = false>
 __global__ void k_advect(uint32_t n, const float4* __restrict__ pm,
     const float4* __restrict__ vel, float dt, float* __restrict__ x, float* __restrict__ y,
     float* __restrict__ z, float* __restrict__ vx, float* __restrict__ vy,
@@ -770,7 +773,7 @@ __global__ void k_advect(uint32_t n, const float4* __restrict__ pm,
     if (i < n) {
         const float4 p = pm[i];
         const float4 v = vel[i];
-        vn = store_state(tail, i, p.x + dt * v.x, p.y + dt * v.y, p.z + dt * v.z, v.x, v.y, v.z,
+        vn = store_state<BATCH>(tail, i, p.x + dt * v.x, p.y + dt * v.y, p.z + dt * v.z, v.x, v.y, v.z,
             x, y, z, vx, vy, vz);
     }
     tail_reduce(tail, vn);
@@ -998,7 +1001,7 @@ __global__ void __launch_bounds__(MB) k_iisph_final(uint32_t n, Fluid f,
     acc[i] = make_float4(ax, ay, az, 0.f);
     const float4 v = vel[i];
     const float nvx = v.x + dt * ax, nvy = v.y + dt * ay, nvz = v.z + dt * az;
-    vn = store_state(tail, i, me.x + dt * nvx, me.y + dt * nvy, me.z + dt * nvz, nvx, nvy, nvz,
+    vn = store_state<BATCH>(tail, i, me.x + dt * nvx, me.y + dt * nvy, me.z + dt * nvz, nvx, nvy, nvz,
         x, y, z, vx, vy, vz);
     }
     tail_reduce(tail, vn);
@@ -1243,7 +1246,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                     break;
             }
             REYN_KERNEL("k_advect", s,
-                k_advect<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, st.pm.get(), v, dt, X, Y, Z,
+                k_advect<B><<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, st.pm.get(), v, dt, X, Y, Z,
                 VX, VY, VZ, tail));
         } else { // IISPH
             REYN_KERNEL("k_nonpressure", s,
