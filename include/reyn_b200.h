@@ -366,6 +366,16 @@ int reyn_solver_next_dt(reyn_solver* s, reyn_particles* state,
     uint32_t iter_last, float dt_last, float lambda, float h, const float g[3],
     uint32_t iter_target, float change_factor, float* dt_out, void* stream);
 
+/* ---- diagnostics (no counterpart in the reference) ------------------------ */
+typedef struct reyn_diag {
+    double mass;        /* sum m */
+    double momentum[3]; /* sum m v */
+    double kinetic;     /* sum m |v|^2 / 2 */
+} reyn_diag;
+/* global mass, momentum and kinetic energy of the state, reduced in FP64;
+ * synchronises the stream */
+int reyn_diagnostics(reyn_particles* state, reyn_diag* out, void* stream);
+
 /* ---- bounds (src/scene/scene.cu:466-491) ---------------------------------- */
 int reyn_enforce_bounds(reyn_particles* state, const float bound_min[3],
     const float bound_max[3], void* stream);

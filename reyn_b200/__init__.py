@@ -64,6 +64,11 @@ class TunePoint(ctypes.Structure):
     _fields_ = [("block_size", _u32), ("cell_ratio", _f), ("ms_per_step", _f)]
 
 
+class Diag(ctypes.Structure):
+    _fields_ = [("mass", ctypes.c_double), ("momentum", ctypes.c_double * 3),
+                ("kinetic", ctypes.c_double)]
+
+
 class SolverBuffers(ctypes.Structure):
     _fields_ = [("rho", _vp), ("p", _vp), ("aii", _vp), ("sii", _vp), ("ax", _vp), ("ay", _vp),
                 ("az", _vp), ("n", _u32)]
@@ -120,6 +125,7 @@ _SIGNATURES = {
     "reyn_solver_scene_stats": [_vp, _u32, _vp],
     "reyn_autotune": [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp, _f, _u32,
                       _vp, _vp, _vp],
+    "reyn_diagnostics": [_vp, ctypes.POINTER(Diag), _vp],
     "reyn_solver_step": [_vp, _vp, _vp, _vp, _f, ctypes.POINTER(_u32), _vp],
     "reyn_solver_step_bounded": [_vp, _vp, _vp, _vp, _f, _f * 3, _f * 3, ctypes.POINTER(_u32),
                                  _vp],
@@ -462,6 +468,13 @@ def dt_controller(state: Particles, iter_last: int, dt_last: float, lam: float, 
     check(lib().reyn_dt_controller(state.h, iter_last, dt_last, lam, h, _f3(g), iter_target,
                                    change, ctypes.byref(dt), _stream(stream)))
     return dt.value
+
+
+def diagnostics(state: Particles, stream=None) -> dict:
+    """Total mass, momentum and kinetic energy of the state (FP64 sums)."""
+    d = Diag()
+    check(lib().reyn_diagnostics(state.h, ctypes.byref(d), _stream(stream)))
+    return {"mass": d.mass, "momentum": tuple(d.momentum), "kinetic": d.kinetic}
 
 
 def enforce_bounds(state: Particles, bmin, bmax, stream=None) -> None:

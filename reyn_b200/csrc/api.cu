@@ -582,6 +582,16 @@ int reyn_solver_next_dt(reyn_solver* s, reyn_particles* state, uint32_t iter_las
     });
 }
 
+int reyn_diagnostics(reyn_particles* state, reyn_diag* out, void* stream)
+{
+    return guard([&] {
+        require(state && out, "null argument");
+        double d[5];
+        diagnostics(*state, d, as_stream(stream));
+        *out = reyn_diag { d[0], { d[1], d[2], d[3] }, d[4] };
+    });
+}
+
 int reyn_enforce_bounds(reyn_particles* state, const float bound_min[3],
     const float bound_max[3], void* stream)
 {

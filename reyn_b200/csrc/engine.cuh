@@ -204,6 +204,9 @@ float state_vmax(reyn_solver* sv, reyn_particles& st, cudaStream_t s);
 float cfl_time_step(reyn_particles& st, float lambda, float h,
     const float g[3], cudaStream_t s, reyn_solver* sv = nullptr);
 
+// total mass, momentum (3) and kinetic energy of the state, FP64
+void diagnostics(const reyn_particles& st, double out[5], cudaStream_t s);
+
 void enforce_bounds(reyn_particles& st, const float lo[3], const float hi[3],
     cudaStream_t s);
 

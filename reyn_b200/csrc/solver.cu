@@ -103,6 +103,54 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         solver_step_t<NBR_THREADS>(sv, st, grid, bdy, dt, s, bmin, bmax);
 }
 
+// ---- FP64 diagnostics ----------------------------------------------------------
+
+// sum m, sum m v, sum m |v|^2 / 2 in FP64 (per-block FP64 partials, one
+// atomic per block and quantity)
+__global__ void k_diagnostics(uint32_t n, const float* __restrict__ vx,
+    const float* __restrict__ vy, const float* __restrict__ vz, const float* __restrict__ m,
+    double* __restrict__ out)
+{
+    double acc[5] = { 0.0, 0.0, 0.0, 0.0, 0.0 };
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += gridDim.x * blockDim.x) {
+        const double mi = m[i], ux = vx[i], uy = vy[i], uz = vz[i];
+        acc[0] += mi;
+        acc[1] += mi * ux;
+        acc[2] += mi * uy;
+        acc[3] += mi * uz;
+        acc[4] += 0.5 * mi * (ux * ux + uy * uy + uz * uz);
+    }
+    __shared__ double s_acc[5][THREADS / 32];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+        const double v = warp_sum(acc[q]);
+        if ((threadIdx.x & 31) == 0)
+            s_acc[q][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double v = 0.0;
+        for (int w = 0; w < THREADS / 32; ++w)
+            v += s_acc[threadIdx.x][w];
+        atomicAdd(out + threadIdx.x, v);
+    }
+}
+
+void diagnostics(const reyn_particles& st, double out[5], cudaStream_t s)
+{
+    DevArray<double> d(5);
+    REYN_CUDA(cudaMemsetAsync(d.get(), 0, 5 * sizeof(double), s));
+    if (st.n) {
+        REYN_KERNEL("k_diagnostics", s,
+            k_diagnostics<<<std::min<unsigned>(blocks_for(st.n, THREADS), 148 * 8), THREADS, 0, s>>>(
+            st.n, st.cur[FVX].get(), st.cur[FVY].get(), st.cur[FVZ].get(), st.cur[FM].get(),
+            d.get()));
+    }
+    REYN_CUDA(cudaMemcpyAsync(out, d.get(), 5 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    REYN_CUDA(cudaStreamSynchronize(s));
+}
+
 // ---- time step and bounds ------------------------------------------------------
 
 __global__ void k_vmax(uint32_t n, const float* __restrict__ vx, const float* __restrict__ vy,

@@ -381,3 +381,17 @@ def test_autotune_covers_the_grid_and_restores_the_state(cuda):
     assert best.ms_per_step == min(p.ms_per_step for p in pts)
     for o in (bd, st):
         o.close()
+
+
+def test_fp64_diagnostics(cuda):
+    import reyn_b200 as rb
+    sc = scenes.dam_break((30, 20, 10), 0.02, (0.8, 0.6, 0.6), velocity_noise=0.5, seed=12)
+    st = rb.Particles(sc.n, sc.rho0)
+    st.upload(sc.fluid)
+    d = rb.diagnostics(st)
+    m = sc.fluid["m"].astype(np.float64)
+    v = np.stack([sc.fluid[k].astype(np.float64) for k in ("vx", "vy", "vz")], 1)
+    assert abs(d["mass"] - m.sum()) <= 1e-12 * m.sum()
+    np.testing.assert_allclose(d["momentum"], (m[:, None] * v).sum(0), rtol=1e-10, atol=1e-14)
+    assert abs(d["kinetic"] - 0.5 * (m * (v * v).sum(1)).sum()) <= 1e-10 * d["kinetic"]
+    st.close()
