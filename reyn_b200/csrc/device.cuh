@@ -299,52 +299,66 @@ __device__ __forceinline__ int3 clamp_cell(const GridView& g, int3 c, int R)
 // Each row is trimmed to the part the search sphere can reach: rows whose
 // (y, z) distance from the point exceeds r are skipped, and the x-run is cut
 // to the cells overlapping the sphere's chord at that distance. The trimming
-// is conservative by a margin of 1e-3 cells, so exactly the candidates within
-// r are still visited, in the same order; only provably empty cells are
-// skipped. Every operation is explicitly rounded (no contraction into FMAs),
-// so every kernel that walks the rows of a point gets the same runs.
+// is conservative by a margin of 1e-3 cells (far above the rounding of the
+// approximate square root used for the chord), so exactly the candidates
+// within r are still visited, in the same order; only provably empty cells
+// are skipped.
 template <int R, class Run>
 __device__ __forceinline__ void for_each_row(const GridView& g, int3 c, float xi, float yi,
     float zi, Run&& run)
 {
     constexpr float EPS = 1e-3f;
     // the point in cell units, relative to its own cell's lower corner
-    const float fx = __fsub_rn(__fmul_rn(__fsub_rn(xi, g.lox), g.inv_cell), (float)c.x);
-    const float fy = __fsub_rn(__fmul_rn(__fsub_rn(yi, g.loy), g.inv_cell), (float)c.y);
-    const float fz = __fsub_rn(__fmul_rn(__fsub_rn(zi, g.loz), g.inv_cell), (float)c.z);
-    const float rr = __fadd_rn(
-        __fmul_rn(__fmul_rn(__fmul_rn(g.r2, g.inv_cell), g.inv_cell), 1.f + EPS), EPS);
+    const float fx = (xi - g.lox) * g.inv_cell - (float)c.x;
+    const float fy = (yi - g.loy) * g.inv_cell - (float)c.y;
+    const float fz = (zi - g.loz) * g.inv_cell - (float)c.z;
+    const float rr = g.r2 * g.inv_cell * g.inv_cell * (1.f + EPS) + EPS;
 #pragma unroll 1
     for (int dz = -R; dz <= R; ++dz) {
         // distance (cells) from the point to the slab of cells at c.z + dz
-        const float gz = dz > 0 ? fmaxf(__fsub_rn((float)dz, fz), 0.f)
-                                : (dz < 0 ? fmaxf(__fsub_rn(fz, (float)(dz + 1)), 0.f) : 0.f);
-        const float gz2 = __fmul_rn(gz, gz);
+        const float gz = dz > 0 ? fmaxf((float)dz - fz, 0.f)
+                                : (dz < 0 ? fmaxf(fz - (float)(dz + 1), 0.f) : 0.f);
+        const float gz2 = gz * gz;
         if (gz2 > rr)
             continue;
         const int plane = (c.z + dz) * g.nxny;
 #pragma unroll 1
         for (int dy = -R; dy <= R; ++dy) {
-            const float gy = dy > 0 ? fmaxf(__fsub_rn((float)dy, fy), 0.f)
-                                    : (dy < 0 ? fmaxf(__fsub_rn(fy, (float)(dy + 1)), 0.f) : 0.f);
-            const float d2 = __fadd_rn(gz2, __fmul_rn(gy, gy));
+            const float gy = dy > 0 ? fmaxf((float)dy - fy, 0.f)
+                                    : (dy < 0 ? fmaxf(fy - (float)(dy + 1), 0.f) : 0.f);
+            const float d2 = fmaf(gy, gy, gz2);
             if (d2 > rr)
                 continue;
-            const float w = __fadd_rn(__fsqrt_rn(__fsub_rn(rr, d2)), EPS); // half chord, cells
-            const int x0 = max(-R, (int)floorf(__fsub_rn(fx, w)));
-            const int x1 = min(R, (int)floorf(__fadd_rn(fx, w)));
+            const float t = rr - d2;
+            const float w = (t > 0.f ? t * rsqrtf(t) : 0.f) + EPS; // half chord, cells
+            const int x0 = max(-R, (int)floorf(fx - w));
+            const int x1 = min(R, (int)floorf(fx + w));
             if (x0 > x1) // only for points clamped into the grid from outside
                 continue;
+            // one run per row, two where a Z-order row crosses a brick; one
+            // call site, so the caller's candidate loop is inlined once
+            uint32_t k0 = uint32_t(plane + (c.y + dy) * g.nx + c.x + x0);
+            int n0 = x1 - x0 + 1;
+            uint32_t k1 = 0;
+            int n1 = 0;
             if (g.order == REYN_ORDER_ZORDER) {
                 const int xa = c.x + x0, xb = c.x + x1, y = c.y + dy, z = c.z + dz;
-                if ((xa >> 2) == (xb >> 2)) {
-                    run(zorder_key(g.tx, g.txy, xa, y, z), xb - xa + 1);
-                } else {
-                    run(zorder_key(g.tx, g.txy, xa, y, z), 4 - (xa & 3));
-                    run(zorder_key(g.tx, g.txy, xb & ~3, y, z), (xb & 3) + 1);
+                k0 = zorder_key(g.tx, g.txy, xa, y, z);
+                if ((xa >> 2) != (xb >> 2)) {
+                    n0 = 4 - (xa & 3);
+                    k1 = zorder_key(g.tx, g.txy, xb & ~3, y, z);
+                    n1 = (xb & 3) + 1;
                 }
-            } else {
-                run(uint32_t(plane + (c.y + dy) * g.nx + c.x + x0), x1 - x0 + 1);
+            }
+#pragma unroll 1
+            for (int q = 0; q < 2; ++q) {
+                if (q == 1) {
+                    if (!n1)
+                        break;
+                    k0 = k1;
+                    n0 = n1;
+                }
+                run(k0, n0);
             }
         }
     }
