@@ -19,6 +19,8 @@
  *                       IISPH.cuh:51-85 (constructors and step)
  *   time step           src/timestep/cfl.cuh:13-32
  *   bounds              src/scene/scene.cu:485-491 (Scene::hard_enforce_bounds)
+ *   meshes              src/datastructure/lbvh.cuh:614-760 (LBVH),
+ *                       src/scene/sample_boundary.cu:100-439 (sampling)
  */
 #ifndef REYN_B200_H_
 #define REYN_B200_H_
@@ -432,6 +434,89 @@ int reyn_scene_sphere(const float center[3], float radius, float spacing,
  * shrinks to *n_out. Synchronises the stream. */
 int reyn_scene_cull(reyn_particles* p, const reyn_boundary* bdy, float radius,
     uint32_t* n_out, void* stream);
+
+/* ---- triangle meshes: LBVH queries, boundary sampling, fluid fill ---------
+ * src/scene/loader.{h,cpp} (Mesh, load_mesh_from_obj), sample_boundary.cuh:
+ * 13-60 (DeviceMesh, get_volume), src/datastructure/lbvh.cuh:614-760 (LBVH),
+ * src/scene/sample_boundary.cu:100-248, 299-389 (relax_sampling,
+ * uniform_sample_mesh), src/scene/scene.cu:84-139, 316-425 (InsidePredicate,
+ * Scene::from_obj's fluid fill). A mesh owns its vertices (double, as the
+ * reference stores them), its triangles and the LBVH over them. */
+typedef struct reyn_mesh reyn_mesh;
+
+typedef struct reyn_mesh_info {
+    uint32_t n_vertices;
+    uint32_t n_faces;
+    uint32_t tree_height;  /* edges from the root to the deepest leaf */
+    uint32_t reserved;
+    double bounds_min[3];  /* extent of all vertices (LBVH bounds_min/max) */
+    double bounds_max[3];
+    double area;           /* total surface area */
+    double volume;         /* |signed volume|: closed, consistently wound meshes */
+} reyn_mesh_info;
+
+/* DeviceMesh::from + LBVH(DeviceMesh*) (sample_boundary.cuh:22-30,
+ * lbvh.cuh:646-723): host vertex coordinates and host triangles (3 vertex
+ * indices each). Builds the LBVH over the faces sorted by the 30-bit Morton
+ * code of their centroids (ties by face index). Synchronises the stream. */
+int reyn_mesh_create(const double* vx, const double* vy, const double* vz,
+    uint32_t n_vertices, const uint32_t* faces, uint32_t n_faces, void* stream,
+    reyn_mesh** out);
+/* load_mesh_from_obj (loader.cpp) + reyn_mesh_create: a Wavefront OBJ file of
+ * triangles ("v" and "f" records; "o"/"g" name the shapes). Shapes whose
+ * lower-case name contains any of the n_ignore strings are skipped; with
+ * `only` != NULL only shapes whose name contains it are kept. Every vertex
+ * of the file is kept, as the reference's loader does. */
+int reyn_mesh_load_obj(const char* path, const char* const* ignore,
+    uint32_t n_ignore, const char* only, void* stream, reyn_mesh** out);
+int reyn_mesh_destroy(reyn_mesh* mesh);
+int reyn_mesh_info_get(const reyn_mesh* mesh, reyn_mesh_info* out);
+/* the LBVH in the reference's layout, device arrays (any may be NULL):
+ * order[j] = original face of leaf j (n_faces); children_l/r (n_faces - 1) in
+ * the ChildNode encoding index << 1 | (1 for an internal node) of
+ * lbvh.cuh:162-193; leaf_box (6 n_faces) and node_box (6 (n_faces - 1))
+ * floats: min xyz, max xyz. */
+int reyn_mesh_tree(const reyn_mesh* mesh, uint32_t* order, uint32_t* children_l,
+    uint32_t* children_r, float* leaf_box, float* node_box, void* stream);
+/* LBVH::project (lbvh.cuh:521-561, 726-741): each of the n points (device
+ * arrays) moves to the closest point of the mesh */
+int reyn_mesh_project(const reyn_mesh* mesh, float* x, float* y, float* z,
+    uint32_t n, void* stream);
+/* InsidePredicate (scene.cu:84-139): inside[i] = 1 when the step from point
+ * i to the closest point of the mesh runs along that face's normal
+ * (dot >= 0), i.e. i lies inside an outward-wound closed mesh. The
+ * reference's predicate returns the negation (the points its remove_if
+ * drops). */
+int reyn_mesh_inside(const reyn_mesh* mesh, const float* x, const float* y,
+    const float* z, uint32_t n, uint8_t* inside, void* stream);
+/* uniform_sample_mesh (sample_boundary.cu:299-389): ceil(area / (1.5 sqrt(3)
+ * h_bdy^2)) samples, h_bdy = h / oversampling, stratified along the summed
+ * face areas and uniform inside each triangle. The random numbers are
+ * counter-based (SplitMix64 of the seed and the sample index) instead of the
+ * reference's curand Philox. *count receives the sample count; x == NULL is
+ * a size query. */
+int reyn_mesh_sample_uniform(const reyn_mesh* mesh, float h, float oversampling,
+    uint64_t seed, float* x, float* y, float* z, uint32_t capacity,
+    uint32_t* count, void* stream);
+/* relax_sampling (sample_boundary.cu:100-166): `iters` sweeps that move every
+ * sample down the gradient of its number density (B3 at support 2 h_bdy,
+ * against the rest density of a hexagonal plane sampling), scaled by
+ * relaxation_factor h_bdy^2, then back onto the mesh. Each sweep reads the
+ * previous positions of all samples. The samples keep their order. stats
+ * (host, may be NULL) receives per sweep the max/min number-density ratio and
+ * the average number density; num_den (device, may be NULL) the number
+ * densities of the last sweep. Synchronises the stream. */
+int reyn_mesh_relax(const reyn_mesh* mesh, float* x, float* y, float* z,
+    uint32_t n, float h_bdy, float relaxation_factor, uint32_t iters,
+    float* stats, float* num_den, void* stream);
+/* Scene::from_obj's fluid volume (scene.cu:336-425): lattice points of
+ * spacing h over the mesh's bounds (x fastest), kept when inside, in lattice
+ * order, each coordinate then moved by a uniform [-jitter h, jitter h]
+ * (counter-based streams keyed by the lattice index). *count receives the
+ * number kept; x == NULL is a size query. Synchronises the stream. */
+int reyn_mesh_fill(const reyn_mesh* mesh, float h, float jitter, uint64_t seed,
+    float* x, float* y, float* z, uint32_t capacity, uint32_t* count,
+    void* stream);
 
 /* ---- launch accounting (no counterpart in the reference, which has no
  * tracing): per-kernel launch counts and CUDA-event device time ----------- */

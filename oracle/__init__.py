@@ -5,8 +5,9 @@ ctypes bindings for two checkers, never for the product:
 * ``liboracle.so`` (oracle/oracle.cpp): a host C++/OpenMP restatement of the
   reference's (reyn) SPH hot path: smoothing kernels, counting-sort uniform
   grid, ``ff_nbrs`` traversal, SESPH/PCISPH/IISPH steps, CFL, bounds, Akinci
-  boundary masses. It is the checker for the CUDA engine and the timed CPU
-  baseline.
+  boundary masses, and (oracle/mesh.cpp) the triangle-mesh path: LBVH build
+  and queries, surface sampling, relaxation and the fluid fill. It is the
+  checker for the CUDA engine and the timed CPU baseline.
 * ``_ref/libreyn_ref*.so`` (oracle/ref/): the reference's OWN sources compiled
   unmodified (kernel classes on the host; the CUDA path for a B200), used to
   pin the oracle and to generate the golden fixtures in tests/golden/.
@@ -127,6 +128,24 @@ def lib():
             ctypes.c_uint32, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, ctypes.c_float,
             ctypes.c_uint32] + [ctypes.c_void_p] * 6 + [_u32p]
         L.orc_threads.restype = ctypes.c_int
+        _d = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        mesh = [_d, _d, _d, ctypes.c_uint32, _u32p, ctypes.c_uint32]
+        vp = ctypes.c_void_p
+        L.orc_mesh_morton.argtypes = mesh + [_u32p]
+        L.orc_lbvh_build.argtypes = mesh + [vp] * 6
+        L.orc_lbvh_query.argtypes = mesh + [ctypes.c_uint32, _f32p, _f32p, _f32p, vp]
+        L.orc_project_brute.argtypes = mesh + [ctypes.c_uint32, _f32p, _f32p, _f32p]
+        L.orc_mesh_measure.argtypes = mesh + [vp, vp, vp]
+        L.orc_mesh_sample_count.argtypes = [ctypes.c_double, ctypes.c_float, ctypes.c_float]
+        L.orc_mesh_sample_count.restype = ctypes.c_uint32
+        L.orc_mesh_sample.argtypes = mesh + [ctypes.c_float, ctypes.c_float, ctypes.c_uint64,
+                                             ctypes.c_uint32, vp, vp, vp, _u32p]
+        L.orc_hex_plane_density.argtypes = [ctypes.c_float]
+        L.orc_hex_plane_density.restype = ctypes.c_float
+        L.orc_mesh_relax_sweep.argtypes = mesh + [ctypes.c_uint32, _f32p, _f32p, _f32p,
+                                                  ctypes.c_float, ctypes.c_float, _f32p]
+        L.orc_mesh_fill.argtypes = mesh + [ctypes.c_float, ctypes.c_float, ctypes.c_uint64,
+                                           ctypes.c_uint32, vp, vp, vp, _u32p]
         _lib = L
     return _lib
 
@@ -283,3 +302,106 @@ def ref_cuda():
         L.ref_last_error.restype = ctypes.c_char_p
         _ref_cuda = L
     return _ref_cuda
+
+
+# ---- triangle meshes (oracle/mesh.cpp) -------------------------------------------
+
+def _mesh_args(verts, faces):
+    v = np.ascontiguousarray(verts, np.float64).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, np.uint32).reshape(-1)
+    return (np.ascontiguousarray(v[:, 0]), np.ascontiguousarray(v[:, 1]),
+            np.ascontiguousarray(v[:, 2]), v.shape[0], f, f.size // 3)
+
+
+def _ok(rc):
+    if rc:
+        raise ValueError(f"oracle mesh call failed ({rc})")
+
+
+def mesh_morton(verts, faces) -> np.ndarray:
+    a = _mesh_args(verts, faces)
+    codes = np.zeros(a[5], np.uint32)
+    _ok(lib().orc_mesh_morton(*a, codes))
+    return codes
+
+
+def lbvh_build(verts, faces) -> dict:
+    """The LBVH of a mesh: leaf order, ChildNode-encoded children, boxes
+    (n x 6: min xyz, max xyz) and height."""
+    a = _mesh_args(verts, faces)
+    nf = a[5]
+    order = np.zeros(nf, np.uint32)
+    cl = np.zeros(max(nf - 1, 1), np.uint32)
+    cr = np.zeros(max(nf - 1, 1), np.uint32)
+    leaf = np.zeros((nf, 6), np.float32)
+    node = np.zeros((max(nf - 1, 1), 6), np.float32)
+    height = np.zeros(1, np.uint32)
+    _ok(lib().orc_lbvh_build(*a, _vp(order), _vp(cl), _vp(cr), _vp(leaf), _vp(node),
+                             _vp(height)))
+    return {"order": order, "children_l": cl[:nf - 1], "children_r": cr[:nf - 1],
+            "leaf_box": leaf, "node_box": node[:nf - 1], "height": int(height[0])}
+
+
+def lbvh_project(verts, faces, x, y, z):
+    x, y, z = f32(x).copy(), f32(y).copy(), f32(z).copy()
+    _ok(lib().orc_lbvh_query(*_mesh_args(verts, faces), x.size, x, y, z, None))
+    return x, y, z
+
+
+def lbvh_inside(verts, faces, x, y, z) -> np.ndarray:
+    x, y, z = f32(x).copy(), f32(y).copy(), f32(z).copy()
+    inside = np.zeros(x.size, np.uint8)
+    _ok(lib().orc_lbvh_query(*_mesh_args(verts, faces), x.size, x, y, z, _vp(inside)))
+    return inside
+
+
+def project_brute(verts, faces, x, y, z):
+    x, y, z = f32(x).copy(), f32(y).copy(), f32(z).copy()
+    _ok(lib().orc_project_brute(*_mesh_args(verts, faces), x.size, x, y, z))
+    return x, y, z
+
+
+def mesh_measure(verts, faces):
+    """(total area, volume, inclusive area sums)"""
+    a = _mesh_args(verts, faces)
+    area = np.zeros(1)
+    vol = np.zeros(1)
+    cdf = np.zeros(a[5])
+    _ok(lib().orc_mesh_measure(*a, _vp(area), _vp(vol), _vp(cdf)))
+    return float(area[0]), float(vol[0]), cdf
+
+
+def mesh_sample_count(area: float, h: float, oversampling: float) -> int:
+    return int(lib().orc_mesh_sample_count(area, h, oversampling))
+
+
+def mesh_sample(verts, faces, h: float, oversampling: float, seed: int):
+    a = _mesh_args(verts, faces)
+    cnt = np.zeros(1, np.uint32)
+    _ok(lib().orc_mesh_sample(*a, h, oversampling, seed, 0, None, None, None, cnt))
+    n = int(cnt[0])
+    x, y, z = (np.zeros(max(n, 1), np.float32) for _ in range(3))
+    _ok(lib().orc_mesh_sample(*a, h, oversampling, seed, n, _vp(x), _vp(y), _vp(z), cnt))
+    return x[:n], y[:n], z[:n]
+
+
+def hex_plane_density(h_bdy: float) -> float:
+    return float(lib().orc_hex_plane_density(h_bdy))
+
+
+def mesh_relax_sweep(verts, faces, x, y, z, h_bdy: float, k: float):
+    """One relaxation sweep; returns (x, y, z, number densities)."""
+    x, y, z = f32(x).copy(), f32(y).copy(), f32(z).copy()
+    nd = np.zeros(x.size, np.float32)
+    _ok(lib().orc_mesh_relax_sweep(*_mesh_args(verts, faces), x.size, x, y, z, h_bdy, k, nd))
+    return x, y, z, nd
+
+
+def mesh_fill(verts, faces, h: float, jitter: float = 0.0, seed: int = 1):
+    a = _mesh_args(verts, faces)
+    cnt = np.zeros(1, np.uint32)
+    _ok(lib().orc_mesh_fill(*a, h, jitter, seed, 0, None, None, None, cnt))
+    n = int(cnt[0])
+    x, y, z = (np.zeros(max(n, 1), np.float32) for _ in range(3))
+    _ok(lib().orc_mesh_fill(*a, h, jitter, seed, n, _vp(x), _vp(y), _vp(z), cnt))
+    return x[:n], y[:n], z[:n]

@@ -126,6 +126,79 @@ int orc_run(const orc_params* prm, uint32_t n, float* x, float* y, float* z,
 /* number of OpenMP threads the oracle uses */
 int orc_threads(void);
 
+
+/* ---- triangle meshes (scene/sample_boundary.cu, datastructure/lbvh.cuh) ----
+ * A mesh is nv double vertices (vx, vy, vz) and nf triangles (faces: 3 vertex
+ * indices each). Boxes are 6 floats (min xyz, max xyz). */
+
+/* 30-bit Morton code of each face centroid in the vertex bounds
+ * (lbvh.cuh:17-45, 204-225) */
+int orc_mesh_morton(const double* vx, const double* vy, const double* vz,
+    uint32_t nv, const uint32_t* faces, uint32_t nf, uint32_t* codes);
+
+/* the LBVH (lbvh.cuh:646-723, lbvh.cu:34-170): order[j] = original face of
+ * leaf j (faces stably sorted by code); children in the ChildNode encoding
+ * (index << 1 | 1 for an internal node, lbvh.cuh:162-193), nf - 1 each; leaf
+ * and internal boxes; height = edges from the root to the deepest leaf.
+ * Any output may be NULL. */
+int orc_lbvh_build(const double* vx, const double* vy, const double* vz,
+    uint32_t nv, const uint32_t* faces, uint32_t nf, uint32_t* order,
+    uint32_t* children_l, uint32_t* children_r, float* leaf_box,
+    float* node_box, uint32_t* height);
+
+/* LBVH queries over n points: inside == NULL projects them in place onto
+ * the closest point of the mesh (LBVH::project, lbvh.cuh:415-561); else
+ * inside[i] = 1 when the step from point i to its closest point runs along
+ * that face's normal (the negation of InsidePredicate, scene.cu:84-139,
+ * which marks the points to remove) and the points are unchanged. */
+int orc_lbvh_query(const double* vx, const double* vy, const double* vz,
+    uint32_t nv, const uint32_t* faces, uint32_t nf, uint32_t n, float* x,
+    float* y, float* z, uint8_t* inside);
+
+/* the brute-force projection of the reference's LBVH test (lbvh.cu:276-306) */
+int orc_project_brute(const double* vx, const double* vy, const double* vz,
+    uint32_t nv, const uint32_t* faces, uint32_t nf, uint32_t n, float* x,
+    float* y, float* z);
+
+/* total area, |signed volume| and (optional, nf entries) the inclusive sum of
+ * face areas (sample_boundary.cu:311-330, sample_boundary.cuh:40-60) */
+int orc_mesh_measure(const double* vx, const double* vy, const double* vz,
+    uint32_t nv, const uint32_t* faces, uint32_t nf, double* area,
+    double* volume, double* cdf);
+
+/* number of boundary samples for spacing h / oversampling
+ * (sample_boundary.cu:339-346) */
+uint32_t orc_mesh_sample_count(double area, float h, float oversampling);
+
+/* area-stratified uniform samples (sample_boundary.cu:168-248, 299-389) with
+ * the engine's counter-based random streams (SplitMix64: stream 8 the offset
+ * inside the stratum, streams 9 and 10 the barycentric pair, each in (0, 1]
+ * with 53 bits). x == NULL: count only. */
+int orc_mesh_sample(const double* vx, const double* vy, const double* vz,
+    uint32_t nv, const uint32_t* faces, uint32_t nf, float h,
+    float oversampling, uint64_t seed, uint32_t cap, float* x, float* y,
+    float* z, uint32_t* count);
+
+/* rest number density of a hexagonal plane sampling (sample_boundary.cu:78-98) */
+float orc_hex_plane_density(float h_bdy);
+
+/* one relaxation sweep (sample_boundary.cu:20-71, 134-147) over all sample
+ * pairs: number densities (out: num_den), the shift down their gradient
+ * from the old positions (the reference shifts in place while neighbours
+ * read, a data race), then the projection back onto the mesh */
+int orc_mesh_relax_sweep(const double* vx, const double* vy, const double* vz,
+    uint32_t nv, const uint32_t* faces, uint32_t nf, uint32_t n, float* x,
+    float* y, float* z, float h_bdy, float k, float* num_den);
+
+/* the fluid fill of Scene::from_obj (scene.cu:336-425): lattice points of
+ * spacing h over the mesh's float bounds (x fastest) kept when inside, in
+ * lattice order, optionally jittered by a uniform [-jitter h, jitter h] per
+ * axis (streams 0..2 keyed by the lattice index). x == NULL: count only. */
+int orc_mesh_fill(const double* vx, const double* vy, const double* vz,
+    uint32_t nv, const uint32_t* faces, uint32_t nf, float h, float jitter,
+    uint64_t seed, uint32_t cap, float* x, float* y, float* z,
+    uint32_t* count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,8 +24,10 @@
 #include "solvers/IISPH.cuh"
 #include "timestep/cfl.cuh"
 #include "scene/ply_io.cuh"
+#include "datastructure/lbvh.cuh"
 
 #include <thrust/copy.h>
+#include <thrust/host_vector.h>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -527,6 +529,101 @@ int ref_run_timed(int scheme, int kind, uint N, float* x, float* y, float* z,
         to_host(state.vx, vx, N);
         to_host(state.vy, vy, N);
         to_host(state.vz, vz, N);
+    });
+}
+
+} // extern "C"
+
+namespace {
+
+Mesh host_mesh(uint nv, const double* vx, const double* vy, const double* vz, uint nf,
+    const uint* faces)
+{
+    Mesh m;
+    m.xs.assign(vx, vx + nv);
+    m.ys.assign(vy, vy + nv);
+    m.zs.assign(vz, vz + nv);
+    m.faces.resize(nf);
+    for (uint t = 0; t < nf; ++t)
+        m.faces[t] = make_uint3(faces[3 * t], faces[3 * t + 1], faces[3 * t + 2]);
+    return m;
+}
+
+void put_boxes(const thrust::host_vector<AABB>& b, float* out)
+{
+    for (size_t i = 0; out && i < b.size(); ++i) {
+        const float v[6] = { b[i].mini.x, b[i].mini.y, b[i].mini.z, b[i].maxi.x, b[i].maxi.y,
+            b[i].maxi.z };
+        std::memcpy(out + 6 * i, v, sizeof(v));
+    }
+}
+
+} // namespace
+
+extern "C" {
+
+/// DeviceMesh::get_volume (sample_boundary.cuh:40-60) and LBVH(&mesh)
+/// (lbvh.cuh:646-723) over a host mesh: the faces as the constructor leaves
+/// them (sorted by Morton code), the children in the ChildNode encoding, the
+/// leaf and internal boxes (min xyz, max xyz) and the tree height; then
+/// LBVH::project (lbvh.cuh:726-741) of n host points, in place.
+int ref_lbvh(uint nv, const double* vx, const double* vy, const double* vz, uint nf,
+    const uint* faces, uint* faces_sorted, uint* children_l, uint* children_r, float* leaf_box,
+    float* node_box, uint* height, double* volume, uint n, float* x, float* y, float* z)
+{
+    return guarded([&] {
+        DeviceMesh dm { DeviceMesh::from(host_mesh(nv, vx, vy, vz, nf, faces)) };
+        if (volume)
+            *volume = dm.get_volume();
+        const LBVH lbvh(&dm);
+        const thrust::host_vector<uint3> fs = dm.faces.get();
+        for (uint t = 0; faces_sorted && t < nf; ++t) {
+            faces_sorted[3 * t] = fs[t].x;
+            faces_sorted[3 * t + 1] = fs[t].y;
+            faces_sorted[3 * t + 2] = fs[t].z;
+        }
+        const thrust::host_vector<ChildNode> cl = lbvh.children_l.get();
+        const thrust::host_vector<ChildNode> cr = lbvh.children_r.get();
+        for (size_t i = 0; i < cl.size(); ++i) {
+            if (children_l)
+                children_l[i] = cl[i].__i;
+            if (children_r)
+                children_r[i] = cr[i].__i;
+        }
+        put_boxes(lbvh.aabbs_leaf.get(), leaf_box);
+        put_boxes(lbvh.aabbs_internal.get(), node_box);
+        if (height)
+            *height = lbvh.get_pod().tree_height;
+        if (n) {
+            DeviceBuffer<float> xs(1), ys(1), zs(1);
+            to_dev(xs, x, n);
+            to_dev(ys, y, n);
+            to_dev(zs, z, n);
+            lbvh.project(xs, ys, zs);
+            to_host(xs, x, n);
+            to_host(ys, y, n);
+            to_host(zs, z, n);
+        }
+    });
+}
+
+/// uniform_sample_mesh (sample_boundary.cu:299-389): *count samples (curand
+/// Philox, the reference's seed), written when cap allows
+int ref_mesh_sample(uint nv, const double* vx, const double* vy, const double* vz, uint nf,
+    const uint* faces, float h, float oversampling, uint cap, float* x, float* y, float* z,
+    uint* count)
+{
+    return guarded([&] {
+        DeviceMesh dm { DeviceMesh::from(host_mesh(nv, vx, vy, vz, nf, faces)) };
+        DeviceBuffer<float> xs(1), ys(1), zs(1);
+        uniform_sample_mesh(xs, ys, zs, dm, h, oversampling);
+        const uint n = static_cast<uint>(xs.size());
+        *count = n;
+        if (x && cap >= n) {
+            to_host(xs, x, n);
+            to_host(ys, y, n);
+            to_host(zs, z, n);
+        }
     });
 }
 

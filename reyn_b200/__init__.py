@@ -79,6 +79,13 @@ class ProfileEntry(ctypes.Structure):
                 ("total_ms", ctypes.c_double)]
 
 
+class MeshInfo(ctypes.Structure):
+    _fields_ = [("n_vertices", _u32), ("n_faces", _u32), ("tree_height", _u32),
+                ("reserved", _u32), ("bounds_min", ctypes.c_double * 3),
+                ("bounds_max", ctypes.c_double * 3), ("area", ctypes.c_double),
+                ("volume", ctypes.c_double)]
+
+
 class StepStats(ctypes.Structure):
     _fields_ = [("iters", _u32), ("avg_density_error", ctypes.c_double),
                 ("max_density_error", ctypes.c_double)]
@@ -140,6 +147,19 @@ _SIGNATURES = {
     "reyn_solver_pressure_upload": [_vp, _vp, _vp, _vp],
     "reyn_grid_construct_noalloc": [_f * 3, _f * 3, _f, _f, _vp, _vp, _vp, _u32, _vp,
                                     ctypes.c_uint64, _vp, ctypes.POINTER(ctypes.c_int32), _vp],
+    "reyn_mesh_create": [_vp, _vp, _vp, _u32, _vp, _u32, _vp, ctypes.POINTER(_vp)],
+    "reyn_mesh_load_obj": [ctypes.c_char_p, ctypes.POINTER(ctypes.c_char_p), _u32,
+                           ctypes.c_char_p, _vp, ctypes.POINTER(_vp)],
+    "reyn_mesh_destroy": [_vp],
+    "reyn_mesh_info_get": [_vp, ctypes.POINTER(MeshInfo)],
+    "reyn_mesh_tree": [_vp, _vp, _vp, _vp, _vp, _vp, _vp],
+    "reyn_mesh_project": [_vp, _vp, _vp, _vp, _u32, _vp],
+    "reyn_mesh_inside": [_vp, _vp, _vp, _vp, _u32, _vp, _vp],
+    "reyn_mesh_sample_uniform": [_vp, _f, _f, ctypes.c_uint64, _vp, _vp, _vp, _u32,
+                                 ctypes.POINTER(_u32), _vp],
+    "reyn_mesh_relax": [_vp, _vp, _vp, _vp, _u32, _f, _f, _u32, _vp, _vp, _vp],
+    "reyn_mesh_fill": [_vp, _f, _f, ctypes.c_uint64, _vp, _vp, _vp, _u32, ctypes.POINTER(_u32),
+                       _vp],
     "reyn_profile_enable": [ctypes.c_int],
     "reyn_profile_reset": [],
     "reyn_profile_read": [ctypes.POINTER(ProfileEntry), _u32, ctypes.POINTER(_u32)],
@@ -353,6 +373,122 @@ class Boundary:
         check(lib().reyn_boundary_arrays(self.h, *[ctypes.byref(p) for p in ps],
                                          ctypes.byref(nb)))
         return [p.value for p in ps], nb.value
+
+
+class Mesh:
+    """A triangle mesh with its LBVH: DeviceMesh + LBVH (reference
+    sample_boundary.cuh:13-60, lbvh.cuh:614-760). verts (V, 3) and faces
+    (F, 3) are host arrays."""
+
+    def __init__(self, verts=None, faces=None, stream=None, _handle=None):
+        if _handle is None:
+            v = np.ascontiguousarray(verts, np.float64).reshape(-1, 3)
+            f = np.ascontiguousarray(faces, np.uint32).reshape(-1)
+            cols = [np.ascontiguousarray(v[:, k]) for k in range(3)]
+            hdl = _vp()
+            check(lib().reyn_mesh_create(cols[0].ctypes.data, cols[1].ctypes.data,
+                                         cols[2].ctypes.data, v.shape[0], f.ctypes.data,
+                                         f.size // 3, _stream(stream), ctypes.byref(hdl)))
+            _handle = hdl
+        self.h = _handle
+
+    @classmethod
+    def from_obj(cls, path: str, ignore=(), only=None, stream=None) -> "Mesh":
+        """load_mesh_from_obj(path, ignore, only_this_name) (loader.cpp)."""
+        ig = (ctypes.c_char_p * max(len(ignore), 1))(*[s.encode() for s in ignore])
+        hdl = _vp()
+        check(lib().reyn_mesh_load_obj(path.encode(), ig, len(ignore),
+                                       only.encode() if only else None, _stream(stream),
+                                       ctypes.byref(hdl)))
+        return cls(_handle=hdl)
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.reyn_mesh_destroy(self.h)
+        self.h = None
+
+    __del__ = close
+
+    def info(self) -> MeshInfo:
+        out = MeshInfo()
+        check(lib().reyn_mesh_info_get(self.h, ctypes.byref(out)))
+        return out
+
+    def tree(self, stream=None) -> dict:
+        """The LBVH in the reference's layout, as device tensors."""
+        import torch
+        nf = self.info().n_faces
+        ni = max(nf - 1, 0)
+        dev = "cuda"
+        order = torch.empty(nf, dtype=torch.int32, device=dev)
+        cl = torch.empty(max(ni, 1), dtype=torch.int32, device=dev)
+        cr = torch.empty(max(ni, 1), dtype=torch.int32, device=dev)
+        leaf = torch.empty((nf, 6), dtype=torch.float32, device=dev)
+        node = torch.empty((max(ni, 1), 6), dtype=torch.float32, device=dev)
+        check(lib().reyn_mesh_tree(self.h, _ptr(order), _ptr(cl), _ptr(cr), _ptr(leaf),
+                                   _ptr(node), _stream(stream)))
+        return {"order": order, "children_l": cl[:ni], "children_r": cr[:ni], "leaf_box": leaf,
+                "node_box": node[:ni]}
+
+    def project(self, x, y, z, stream=None) -> None:
+        """LBVH::project: device tensors, in place."""
+        check(lib().reyn_mesh_project(self.h, _ptr(x), _ptr(y), _ptr(z), x.numel(),
+                                      _stream(stream)))
+
+    def inside(self, x, y, z, stream=None):
+        import torch
+        flags = torch.empty(x.numel(), dtype=torch.uint8, device=x.device)
+        check(lib().reyn_mesh_inside(self.h, _ptr(x), _ptr(y), _ptr(z), x.numel(), _ptr(flags),
+                                     _stream(stream)))
+        return flags
+
+    def sample_uniform(self, h: float, oversampling: float = 2.0, seed: int = 1614201312,
+                       stream=None):
+        """uniform_sample_mesh: three device tensors."""
+        cnt = _u32()
+        check(lib().reyn_mesh_sample_uniform(self.h, h, oversampling, seed, None, None, None, 0,
+                                             ctypes.byref(cnt), None))
+        x, y, z = _device_f32(cnt.value)
+        check(lib().reyn_mesh_sample_uniform(self.h, h, oversampling, seed, _ptr(x), _ptr(y),
+                                             _ptr(z), cnt.value, ctypes.byref(cnt),
+                                             _stream(stream)))
+        return x[:cnt.value], y[:cnt.value], z[:cnt.value]
+
+    def relax(self, x, y, z, h_bdy: float, relaxation_factor: float = 1.0, iters: int = 50,
+              num_den=None, stream=None) -> np.ndarray:
+        """relax_sampling, in place; returns per sweep (max/min number-density
+        ratio, average number density)."""
+        st = np.zeros((max(iters, 1), 2), np.float32)
+        check(lib().reyn_mesh_relax(self.h, _ptr(x), _ptr(y), _ptr(z), x.numel(), h_bdy,
+                                    relaxation_factor, iters, st.ctypes.data, _ptr(num_den),
+                                    _stream(stream)))
+        return st[:iters]
+
+    def fill(self, h: float, jitter: float = 0.0, seed: int = 1, stream=None):
+        """Scene::from_obj's fluid fill: three device tensors."""
+        cnt = _u32()
+        check(lib().reyn_mesh_fill(self.h, h, jitter, seed, None, None, None, 0,
+                                   ctypes.byref(cnt), _stream(stream)))
+        x, y, z = _device_f32(cnt.value)
+        check(lib().reyn_mesh_fill(self.h, h, jitter, seed, _ptr(x), _ptr(y), _ptr(z), cnt.value,
+                                   ctypes.byref(cnt), _stream(stream)))
+        return x[:cnt.value], y[:cnt.value], z[:cnt.value]
+
+
+def sample_mesh(mesh: Mesh, h: float, rho0: float, oversampling_factor: float = 2.0,
+                relaxation_iters: int = 50, relaxation_factor: float = 1.0,
+                mass_refinement_iterations: int = 5, seed: int = 1614201312, stream=None):
+    """sample_mesh (reference sample_boundary.cu:391-439, defaults of
+    sample_boundary.cuh:160-163): uniform samples at h / oversampling_factor,
+    relaxed, then a Boundary with Akinci masses. Returns (Boundary, (x, y, z),
+    relaxation statistics)."""
+    x, y, z = mesh.sample_uniform(h, oversampling_factor, seed, stream)
+    stats = np.zeros((0, 2), np.float32)
+    if relaxation_iters > 0:
+        stats = mesh.relax(x, y, z, h / oversampling_factor, relaxation_factor,
+                           relaxation_iters, stream=stream)
+    bdy = Boundary(x, y, z, None, h, rho0, mass_refinement_iterations, stream)
+    return bdy, (x, y, z), stats
 
 
 NOALLOC_SCRATCH_WORDS = 8 * 1024 * 1024

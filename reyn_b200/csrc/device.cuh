@@ -385,6 +385,41 @@ __device__ __forceinline__ void for_each_neighbour(const GridView& g, int3 c,
     });
 }
 
+// ---- counter-based random numbers ------------------------------------------
+// Value k of stream t under seed s is SplitMix64 (Steele, Lea, Flood 2014) of
+// s + 0x9E3779B97F4A7C15 (t 2^40 + k + 1): a pure function of (s, t, k), so
+// results never depend on the launch and the host reproduces them exactly.
+
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+__host__ __device__ __forceinline__ uint64_t stream_bits(uint64_t seed, uint64_t t, uint64_t k)
+{
+    return splitmix64(seed + 0x9E3779B97F4A7C15ull * ((t << 40) + k + 1));
+}
+
+// uniform in [0, 1) from the top 24 bits (an exact float)
+__device__ __forceinline__ float uniform01(uint64_t seed, uint64_t t, uint64_t k)
+{
+    return float(uint32_t(stream_bits(seed, t, k) >> 40)) * (1.f / 16777216.f);
+}
+
+// uniform in (0, 1] from the top 53 bits (an exact double)
+__device__ __forceinline__ double uniform_open0(uint64_t seed, uint64_t t, uint64_t k)
+{
+    return double((stream_bits(seed, t, k) >> 11) + 1) * (1.0 / 9007199254740992.0);
+}
+
+// uniform in [-a, a]: (2u - 1) a, explicitly rounded
+__device__ __forceinline__ float symmetric(float u, float a)
+{
+    return __fmul_rn(__fsub_rn(__fmul_rn(2.f, u), 1.f), a);
+}
+
 // ---- reductions -------------------------------------------------------------
 
 __device__ __forceinline__ double warp_sum(double v)

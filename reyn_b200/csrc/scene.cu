@@ -18,29 +18,6 @@
 
 namespace reyn {
 
-namespace {
-
-    __host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t z)
-    {
-        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-        return z ^ (z >> 31);
-    }
-
-    // uniform in [0, 1): stream t, value k
-    __device__ __forceinline__ float uniform01(uint64_t seed, uint64_t t, uint64_t k)
-    {
-        const uint64_t z = splitmix64(seed + 0x9E3779B97F4A7C15ull * ((t << 40) + k + 1));
-        return float(uint32_t(z >> 40)) * (1.f / 16777216.f);
-    }
-
-    // uniform in [-a, a]: (2u - 1) a
-    __device__ __forceinline__ float symmetric(float u, float a)
-    {
-        return __fmul_rn(__fsub_rn(__fmul_rn(2.f, u), 1.f), a);
-    }
-
-} // namespace
 
 // lattice + jitter (_init_box_kernel, scene.cu:14-37, x fastest): particle
 // first + q of the block sits at origin + (i, j, k) h + jitter, jitter

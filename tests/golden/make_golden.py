@@ -4,6 +4,11 @@
   compiled unmodified for the host by oracle/ref/Makefile, evaluated on the
   reference's own kernel-test inputs (kernels.cu:31-52: edge cases, then
   seeded pseudo-random offsets in [0, 1.5 h]^3, h = 25). Runs without a GPU.
+* ``--mesh``: the reference's LBVH (datastructure/lbvh.cuh, compiled
+  unmodified for sm_100a) on a B200, over seeded procedural meshes
+  (reyn_b200.meshes): the sorted faces, the tree's children and boxes, its
+  height, the mesh volume, LBVH::project of seeded points, and the sample
+  counts of uniform_sample_mesh.
 * ``--device``: the reference's CUDA path (src/, compiled unmodified for
   sm_100a by oracle/ref/Makefile) on a B200: kernel values on the device, the
   uniform grid (prefix, canonicalised sorted indices, neighbour counts,
@@ -14,7 +19,7 @@
 Inputs are regenerated deterministically (numpy PCG64 seeds) and stored with
 the outputs so that the tests never need the reference at run time.
 
-Usage: python tests/golden/make_golden.py --host|--device [--out DIR]
+Usage: python tests/golden/make_golden.py --host|--device|--mesh [--out DIR]
 """
 from __future__ import annotations
 
@@ -29,7 +34,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
-from reyn_b200 import scenes  # noqa: E402
+from reyn_b200 import meshes, scenes  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
@@ -189,16 +194,77 @@ def make_device(out: str) -> None:
         print(f"wrote solver_{name}.npz iters={iters.tolist()}", flush=True)
 
 
+# mesh fixtures: (name, builder); the builders are deterministic
+MESH_CASES = [
+    ("ico3", lambda: meshes.icosphere(3, 0.7, (0.1, -0.2, 0.3))),
+    ("ico4_perturbed", lambda: (lambda v, f: (meshes.perturb(v, 0.004, 3), f))(
+        *meshes.icosphere(4, 0.7, (0.1, -0.2, 0.3)))),
+    ("box4", lambda: meshes.box((-1.0, -0.5, 0.0), (1.0, 0.5, 0.75), 4)),
+    ("torus_perturbed", lambda: (lambda v, f: (meshes.perturb(v, 0.005, 5), f))(
+        *meshes.torus(1.0, 0.3, 40, 20, (0.5, 0.5, 0.5)))),
+]
+# (h, oversampling) pairs for the sample counts
+SAMPLE_CASES = [(0.05, 2.0), (0.02, 1.0), (0.1, 3.0)]
+
+
+def make_mesh(out: str) -> None:
+    L = _ref()
+    u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+    d = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    L.ref_lbvh.argtypes = [ctypes.c_uint, d, d, d, ctypes.c_uint, u32p, u32p, u32p, u32p,
+                           oracle._f32p, oracle._f32p, u32p, d, ctypes.c_uint, oracle._f32p,
+                           oracle._f32p, oracle._f32p]
+    L.ref_mesh_sample.argtypes = [ctypes.c_uint, d, d, d, ctypes.c_uint, u32p, ctypes.c_float,
+                                  ctypes.c_float, ctypes.c_uint, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p, u32p]
+    for name, make in MESH_CASES:
+        v, f = make()
+        v = np.ascontiguousarray(v, np.float64)
+        f = np.ascontiguousarray(f, np.uint32)
+        vx, vy, vz = (np.ascontiguousarray(v[:, k]) for k in range(3))
+        nv, nf = v.shape[0], f.shape[0]
+        rng = np.random.Generator(np.random.PCG64(420))
+        lo, hi = v.min(0) - 0.2, v.max(0) + 0.2
+        q = (lo + (hi - lo) * rng.random((2000, 3))).astype(np.float32)
+        px, py, pz = (np.ascontiguousarray(q[:, k]) for k in range(3))
+        fs = np.zeros(3 * nf, np.uint32)
+        cl = np.zeros(nf - 1, np.uint32)
+        cr = np.zeros(nf - 1, np.uint32)
+        lb = np.zeros(6 * nf, np.float32)
+        nb = np.zeros(6 * (nf - 1), np.float32)
+        height = np.zeros(1, np.uint32)
+        vol = np.zeros(1, np.float64)
+        _check(L, L.ref_lbvh(nv, vx, vy, vz, nf, f.ravel(), fs, cl, cr, lb, nb, height, vol,
+                             2000, px, py, pz))
+        counts = []
+        for h, ov in SAMPLE_CASES:
+            c = np.zeros(1, np.uint32)
+            _check(L, L.ref_mesh_sample(nv, vx, vy, vz, nf, f.ravel(), h, ov, 0, None, None, None,
+                                        c))
+            counts.append(int(c[0]))
+        np.savez_compressed(os.path.join(out, f"mesh_{name}.npz"), verts=v, faces=f,
+                            faces_sorted=fs.reshape(-1, 3), children_l=cl, children_r=cr,
+                            leaf_box=lb.reshape(-1, 6), node_box=nb.reshape(-1, 6),
+                            height=height[0], volume=vol[0], points=q,
+                            projected=np.stack([px, py, pz], 1),
+                            sample_cases=np.array(SAMPLE_CASES, np.float32),
+                            sample_counts=np.array(counts, np.uint32))
+        print(f"wrote mesh_{name}.npz faces={nf} height={int(height[0])}", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     g = ap.add_mutually_exclusive_group(required=True)
     g.add_argument("--host", action="store_true")
     g.add_argument("--device", action="store_true")
+    g.add_argument("--mesh", action="store_true")
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     if a.host:
         make_host(a.out)
+    elif a.mesh:
+        make_mesh(a.out)
     else:
         make_device(a.out)
 
