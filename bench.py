@@ -79,10 +79,13 @@ def parse_args():
                     help="all: time FP32 and mixed_pos16, then report the mixed path beside them")
     ap.add_argument("--order", choices=["xyz", "zorder"], default="xyz",
                     help="cell order of the grid the state is sorted by")
-    ap.add_argument("--workload", choices=["iisph_4m", "batched_pcisph", "column_16m"],
+    ap.add_argument("--workload", choices=["iisph_4m", "batched_pcisph", "column_16m",
+                                           "mesh_lbvh"],
                     default="iisph_4m",
                     help="batched_pcisph: 256 independent PCISPH scenes; column_16m: the "
-                         "16.7M-particle column collapse onto a sphere (neither is the headline)")
+                         "16.7M-particle column collapse onto a sphere; mesh_lbvh: LBVH "
+                         "closest-point queries and boundary sampling of a 327,680-face mesh "
+                         "(none is the headline)")
     ap.add_argument("--scenes", type=int, default=256, help="batched_pcisph: scene count")
     ap.add_argument("--no-sequential", action="store_true",
                     help="batched_pcisph: skip the scene-by-scene comparison run")
@@ -816,6 +819,155 @@ def run_column(a, world, rank, local):
         obj.close()
 
 
+def mesh_workload(scale: int = 1):
+    """A closed 327,680-face mesh: a level-7 icosphere of radius 1 with its
+    vertices moved by a seeded uniform +-0.001 (a generic surface: no
+    centroid on a Morton cell boundary)."""
+    from reyn_b200 import meshes
+    v, f = meshes.icosphere(max(7 - (scale - 1), 3), 1.0, (0.0, 0.0, 0.0))
+    return meshes.perturb(v, 0.001, 21), f
+
+
+def run_mesh(a, world, rank, local):
+    """LBVH closest-point queries (LBVH::project, lbvh.cuh:726-741) of 16.7M
+    seeded uniform points in the mesh's bounding box (+10 %) against a
+    327,680-face mesh; the tree build; and sample_mesh (uniform sampling at
+    h_bdy = 0.002, 50 relaxation sweeps, Akinci masses). A step re-copies the
+    pristine points (3 device copies) and projects them."""
+    import torch
+
+    import reyn_b200 as rb
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    S = stream.cuda_stream
+    v, f = mesh_workload(a.scale)
+    torch.cuda.synchronize()
+    b0 = time.perf_counter()
+    mesh = rb.Mesh(v, f, stream=S)  # synchronises
+    build_ms = (time.perf_counter() - b0) * 1e3
+    b0 = time.perf_counter()
+    rb.Mesh(v, f, stream=S).close()  # warm: the build again, modules loaded
+    build_ms = min(build_ms, (time.perf_counter() - b0) * 1e3)
+    info = mesh.info()
+    n = (1 << 24) // (a.scale ** 3)
+    lo = np.array(info.bounds_min) - 0.1
+    hi = np.array(info.bounds_max) + 0.1
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+    pristine = [torch.rand(n, generator=g, device=dev, dtype=torch.float32) * float(hi[k] - lo[k])
+                + float(lo[k]) for k in range(3)]
+    work = [t.clone() for t in pristine]
+
+    def step():
+        for w_, p_ in zip(work, pristine):
+            w_.copy_(p_)
+        mesh.project(*work, stream=S)
+
+    for _ in range(max(a.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    clocks = ClockSampler(gpu_uuid)
+    time.sleep(0.3)
+    rb.profile_reset()
+    rb.profile_enable(True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    rb.profile_enable(False)
+    prof = rb.profile_read()
+    ck_clocks = clocks.stop()
+    ms = max_over_ranks(world, e0.elapsed_time(e1))
+    k_ms = prof.get("k_mesh_project", (0, 0.0))[1] / max(a.steps, 1)
+    peak, peak_kind = peaks()
+    algo = 24.0 * n  # 12 B read + 12 B written per query; the tree stays in L2
+    roof = {"kernel": "k_mesh_project", "bound": "hbm",
+            "achieved": round(algo / (k_ms / 1e3) / 1e9, 1) if k_ms else None,
+            "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+            "frac": round(algo / (k_ms / 1e3) / 1e9 / peak, 4) if k_ms else None,
+            "traffic": None, "bytes_per_query": 24,
+            "note": "a latency-bound stack traversal: ~log2(F) dependent 64-byte node loads "
+                    "per query from the L2-resident tree"}
+    # end to end through the public call with host buffers: pinned upload,
+    # project, download
+    e2e = None
+    if not a.no_e2e:
+        host = [p_.cpu().pin_memory() for p_ in pristine]
+        back = [torch.empty_like(h_).pin_memory() for h_ in host]
+        torch.cuda.synchronize()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        for _ in range(a.steps):
+            for w_, h_ in zip(work, host):
+                w_.copy_(h_, non_blocking=True)
+            mesh.project(*work, stream=S)
+            for b_, w_ in zip(back, work):
+                b_.copy_(w_, non_blocking=True)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        t = max_over_ranks(world, e2.elapsed_time(e3))
+        e2e = {"value": round(world * n * a.steps / (t / 1e3), 1), "unit": "queries/s",
+               "h2d_bytes_per_step": 12 * n, "d2h_bytes_per_step": 12 * n}
+    # sample_mesh: uniform samples, 50 relaxation sweeps, boundary masses
+    torch.cuda.synchronize()
+    e4 = torch.cuda.Event(enable_timing=True)
+    e5 = torch.cuda.Event(enable_timing=True)
+    e4.record(stream)
+    bdy, (sx, _, _), rstats = rb.sample_mesh(mesh, 0.004 * a.scale, 1000.0, 2.0,
+                                             relaxation_iters=50, stream=S)
+    e5.record(stream)
+    torch.cuda.synchronize()
+    sample_ms = e4.elapsed_time(e5)
+    n_samples = int(sx.numel())
+    cpu = None
+    if rank == 0 and not a.no_cpu_baseline:
+        import oracle
+        m = 2000000 // (a.scale ** 3)
+        q = [p_[:m].cpu().numpy() for p_ in pristine]
+        t0 = time.perf_counter()
+        oracle.lbvh_project(v, f, q[0][:1], q[1][:1], q[2][:1])  # tree build alone
+        tb = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        oracle.lbvh_project(v, f, *q)
+        tq = max(time.perf_counter() - t0 - tb, 1e-9)
+        cpu = {"value": round(m / tq, 1), "unit": "queries/s", "cores": oracle.threads(),
+               "kind": "port",
+               "sample": f"{m} of the {n} queries (tree build of {tb:.2f} s excluded)"}
+    out = {
+        "metric": "LBVH closest-point queries/s, 327,680-face mesh",
+        "value": round(world * n * a.steps / (ms / 1e3), 1), "unit": "queries/s",
+        "n_gpus": world, "steps": a.steps, "warmup": max(a.warmup, 3),
+        "ms_per_step": round(ms / a.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (perturbed level-7 icosphere; seeded uniform query points)",
+        "config": {"workload": "mesh_lbvh", "faces": info.n_faces, "queries": n,
+                   "tree_height": info.tree_height,
+                   "l2": "inputs (192 MB of points) larger than L2"},
+        "kernel_ms_per_step": round(k_ms, 3), "build_ms": round(build_ms, 2),
+        "sample_mesh": {"samples": n_samples, "ms": round(sample_ms, 2),
+                        "relaxation_iters": 50,
+                        "ratio_first_last": [round(float(rstats[0, 0]), 4),
+                                             round(float(rstats[-1, 0]), 4)]},
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": ck_clocks,
+        "gpu_launches": sum(v_[0] for v_ in prof.values()),
+        "kernels": {k: {"launches": v_[0], "ms": round(v_[1], 3)} for k, v_ in
+                    sorted(prof.items(), key=lambda kv: -kv[1][1])},
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    bdy.close()
+    mesh.close()
+
+
 def main():
     a = parse_args()
     world, rank, local = dist_setup()
@@ -826,6 +978,8 @@ def main():
             run_batched(a, world, rank, local)
         elif a.workload == "column_16m":
             run_column(a, world, rank, local)
+        elif a.workload == "mesh_lbvh":
+            run_mesh(a, world, rank, local)
         else:
             run_engine(a, world, rank, local)
     finally:

@@ -362,6 +362,104 @@ inline void hard_enforce_bounds(Particles& state, float3 bound_min, float3 bound
     check(reyn_enforce_bounds(state.handle(), lo, hi, s));
 }
 
+// ---- meshes (loader.h:11-20, sample_boundary.cuh:13-163, lbvh.cuh:614-760) --
+// Mesh: the reference's host mesh, double vertex components and uint3 faces
+struct Mesh {
+    std::vector<double> xs, ys, zs;
+    std::vector<uint3> faces;
+    size_t vertex_count() const { return xs.size(); }
+    size_t face_count() const { return faces.size(); }
+};
+
+// DeviceMesh together with its LBVH: reyn_mesh builds the tree at creation
+class DeviceMesh {
+public:
+    static DeviceMesh from(const Mesh& m, cudaStream_t s = nullptr)
+    {
+        std::vector<uint32_t> f(3 * m.faces.size());
+        for (size_t t = 0; t < m.faces.size(); ++t) {
+            f[3 * t] = m.faces[t].x;
+            f[3 * t + 1] = m.faces[t].y;
+            f[3 * t + 2] = m.faces[t].z;
+        }
+        reyn_mesh* h = nullptr;
+        check(reyn_mesh_create(m.xs.data(), m.ys.data(), m.zs.data(),
+            static_cast<uint32_t>(m.xs.size()), f.data(), static_cast<uint32_t>(m.faces.size()),
+            s, &h));
+        return DeviceMesh(h);
+    }
+    // load_mesh_from_obj (loader.cpp) straight into a device mesh
+    static DeviceMesh from_obj(const std::string& path, const std::vector<std::string>& ignore = {},
+        const char* only_this_name = nullptr, cudaStream_t s = nullptr)
+    {
+        std::vector<const char*> ig;
+        for (const auto& i : ignore)
+            ig.push_back(i.c_str());
+        reyn_mesh* h = nullptr;
+        check(reyn_mesh_load_obj(path.c_str(), ig.data(), static_cast<uint32_t>(ig.size()),
+            only_this_name, s, &h));
+        return DeviceMesh(h);
+    }
+    DeviceMesh(DeviceMesh&& o) noexcept : m_(std::exchange(o.m_, nullptr)) { }
+    DeviceMesh(const DeviceMesh&) = delete;
+    DeviceMesh& operator=(const DeviceMesh&) = delete;
+    ~DeviceMesh() { reyn_mesh_destroy(m_); }
+    reyn_mesh_info info() const
+    {
+        reyn_mesh_info i {};
+        check(reyn_mesh_info_get(m_, &i));
+        return i;
+    }
+    double get_volume() const { return info().volume; } // sample_boundary.cuh:40-60
+    const reyn_mesh* handle() const { return m_; }
+
+private:
+    explicit DeviceMesh(reyn_mesh* h) : m_(h) { }
+    reyn_mesh* m_ = nullptr;
+};
+
+// LBVH (lbvh.cuh:614-760) over a DeviceMesh; the tree lives in the mesh
+class LBVH {
+public:
+    explicit LBVH(const DeviceMesh* mesh) : mesh_(mesh) { }
+    // LBVH::project (lbvh.cuh:726-741): n device points, in place
+    void project(float* xs, float* ys, float* zs, uint32_t n, cudaStream_t s = nullptr) const
+    {
+        check(reyn_mesh_project(mesh_->handle(), xs, ys, zs, n, s));
+    }
+    uint32_t tree_height() const { return mesh_->info().tree_height; }
+
+private:
+    const DeviceMesh* mesh_;
+};
+
+// uniform_sample_mesh (sample_boundary.cu:299-389): the sample count for
+// spacing h / oversampling_factor; writes the samples when xs != nullptr
+inline uint32_t uniform_sample_mesh(float* xs, float* ys, float* zs, uint32_t capacity,
+    const DeviceMesh& mesh, float h, float oversampling_factor, uint64_t seed = 1614201312,
+    cudaStream_t s = nullptr)
+{
+    uint32_t n = 0;
+    check(reyn_mesh_sample_uniform(mesh.handle(), h, oversampling_factor, seed, xs, ys, zs,
+        capacity, &n, s));
+    return n;
+}
+
+// relax_sampling (sample_boundary.cu:100-166); with a debug stream, one CSV
+// line "sweep,max/min ratio,average" per sweep as the reference writes
+template <class Stream>
+void relax_sampling(float* xs, float* ys, float* zs, uint32_t n, const DeviceMesh& mesh,
+    float h_bdy, Stream* debug_stream, float relaxation_factor, uint32_t relaxation_iters,
+    cudaStream_t s = nullptr)
+{
+    std::vector<float> st(2 * static_cast<size_t>(relaxation_iters));
+    check(reyn_mesh_relax(mesh.handle(), xs, ys, zs, n, h_bdy, relaxation_factor,
+        relaxation_iters, st.data(), nullptr, s));
+    if (debug_stream)
+        for (uint32_t i = 0; i < relaxation_iters; ++i)
+            (*debug_stream) << i + 1 << "," << st[2 * i] << "," << st[2 * i + 1] << "\n";
+}
+
 } // namespace reyn
 
 #endif // REYN_B200_HPP_

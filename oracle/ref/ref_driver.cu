@@ -628,3 +628,80 @@ int ref_mesh_sample(uint nv, const double* vx, const double* vy, const double* v
 }
 
 } // extern "C"
+
+extern "C" {
+
+/// Timing of the reference's mesh path on the device (CUDA events): the
+/// LBVH constructor (lbvh.cuh:646-723) once, then `reps` times a device copy
+/// of the n pristine points followed by LBVH::project (lbvh.cuh:726-741);
+/// and sample_mesh (sample_boundary.cu:391-439) at h, oversampling 2,
+/// relax_iters sweeps, 5 mass refinements (best of two runs). ms[0] =
+/// build, ms[1] = per copy + project, ms[2] = sample_mesh, ms[3] = upload
+/// (DeviceMesh::from) + build, counts[0] = samples.
+int ref_mesh_bench(uint nv, const double* vx, const double* vy, const double* vz, uint nf,
+    const uint* faces, uint n, const float* x, const float* y, const float* z, uint reps,
+    float h, int relax_iters, float* ms, uint* counts)
+{
+    return guarded([&] {
+        cudaEvent_t e0, e1;
+        CUDA_CHECK(cudaEventCreate(&e0));
+        CUDA_CHECK(cudaEventCreate(&e1));
+        const Mesh hm = host_mesh(nv, vx, vy, vz, nf, faces);
+        {
+            // untimed first construction: module loading, allocator warm-up
+            DeviceMesh warm { DeviceMesh::from(hm) };
+            const LBVH lw(&warm);
+        }
+        {
+            CUDA_CHECK(cudaDeviceSynchronize());
+            CUDA_CHECK(cudaEventRecord(e0));
+            DeviceMesh up { DeviceMesh::from(hm) };
+            const LBVH lu(&up);
+            CUDA_CHECK(cudaEventRecord(e1));
+            CUDA_CHECK(cudaEventSynchronize(e1));
+            CUDA_CHECK(cudaEventElapsedTime(&ms[3], e0, e1));
+        }
+        DeviceMesh dm { DeviceMesh::from(hm) };
+        CUDA_CHECK(cudaDeviceSynchronize());
+        CUDA_CHECK(cudaEventRecord(e0));
+        const LBVH lbvh(&dm);
+        CUDA_CHECK(cudaEventRecord(e1));
+        CUDA_CHECK(cudaEventSynchronize(e1));
+        CUDA_CHECK(cudaEventElapsedTime(&ms[0], e0, e1));
+        DeviceBuffer<float> px(1), py(1), pz(1), wx(n), wy(n), wz(n);
+        to_dev(px, x, n);
+        to_dev(py, y, n);
+        to_dev(pz, z, n);
+        auto once = [&] {
+            thrust::copy(px.get().begin(), px.get().end(), wx.get().begin());
+            thrust::copy(py.get().begin(), py.get().end(), wy.get().begin());
+            thrust::copy(pz.get().begin(), pz.get().end(), wz.get().begin());
+            lbvh.project(wx, wy, wz);
+        };
+        once(); // warm-up
+        CUDA_CHECK(cudaDeviceSynchronize());
+        CUDA_CHECK(cudaEventRecord(e0));
+        for (uint r = 0; r < reps; ++r)
+            once();
+        CUDA_CHECK(cudaEventRecord(e1));
+        CUDA_CHECK(cudaEventSynchronize(e1));
+        CUDA_CHECK(cudaEventElapsedTime(&ms[1], e0, e1));
+        ms[1] /= float(reps > 0 ? reps : 1);
+        ms[2] = 1e30f;
+        for (int run = 0; run < 2; ++run) {
+            CUDA_CHECK(cudaDeviceSynchronize());
+            CUDA_CHECK(cudaEventRecord(e0));
+            BoundarySamples b { sample_mesh(hm, h, 1000.f, 2.f, nullptr, relax_iters, 1.f, 5) };
+            CUDA_CHECK(cudaEventRecord(e1));
+            CUDA_CHECK(cudaEventSynchronize(e1));
+            float t = 0.f;
+            CUDA_CHECK(cudaEventElapsedTime(&t, e0, e1));
+            ms[2] = std::min(ms[2], t);
+            counts[0] = static_cast<uint>(b.xs.size());
+        }
+        CUDA_CHECK(cudaEventDestroy(e0));
+        CUDA_CHECK(cudaEventDestroy(e1));
+    });
+}
+
+} // extern "C"

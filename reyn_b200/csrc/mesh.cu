@@ -254,6 +254,46 @@ namespace {
         }
     }
 
+    // 10 bits of v spread to every third bit (bit i -> bit 3i)
+    __device__ __forceinline__ uint32_t spread10(uint32_t v)
+    {
+        v &= 0x3ffu;
+        v = (v | (v << 16)) & 0x030000FFu;
+        v = (v | (v << 8)) & 0x0300F00Fu;
+        v = (v | (v << 4)) & 0x030C30C3u;
+        v = (v | (v << 2)) & 0x09249249u;
+        return v;
+    }
+
+    // Morton code of each query point in the mesh's box (clamped), for
+    // ordering only: queries sorted by it traverse similar paths in a warp
+    __global__ void k_query_keys(uint32_t n, const float* __restrict__ x,
+        const float* __restrict__ y, const float* __restrict__ z, float3 lo, float3 scale,
+        uint32_t* __restrict__ codes, uint32_t* __restrict__ ids)
+    {
+        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= n)
+            return;
+        auto q = [](float v, float l, float sc) {
+            const float t = (v - l) * sc;
+            return uint32_t(fminf(fmaxf(t, 0.f), 1023.f)); // NaN -> 0
+        };
+        codes[i] = (spread10(q(x[i], lo.x, scale.x)) << 2) | (spread10(q(y[i], lo.y, scale.y)) << 1)
+            | spread10(q(z[i], lo.z, scale.z));
+        ids[i] = i;
+    }
+
+    __global__ void k_query_gather(uint32_t n, const uint32_t* __restrict__ perm,
+        const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+        float4* __restrict__ pts)
+    {
+        const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+        if (s >= n)
+            return;
+        const uint32_t p = perm[s];
+        pts[s] = make_float4(x[p], y[p], z[p], 0.f);
+    }
+
     // ---- face areas, volume and the sampling CDF -----------------------------
     struct D3 {
         double x, y, z;
@@ -383,33 +423,21 @@ namespace {
             }
     }
 
-    // inclusive scan of n doubles; `part` holds the tile sums and must outlive
-    // the enqueued kernels
-    void inclusive_scan_d(const double* in, uint32_t n, DevArray<double>& part, double* out,
-        cudaStream_t s)
+    inline uint32_t dscan_parts(uint32_t n) { return (n + DSCAN_TILE - 1) / DSCAN_TILE; }
+
+    // inclusive scan of n doubles; `part` (dscan_parts(n) entries) holds the
+    // tile sums and must outlive the enqueued kernels
+    void inclusive_scan_d(const double* in, uint32_t n, double* part, double* out, cudaStream_t s)
     {
-        const uint32_t nparts = (n + DSCAN_TILE - 1) / DSCAN_TILE;
-        part.resize(nparts);
+        const uint32_t nparts = dscan_parts(n);
         REYN_KERNEL("k_dscan_tiles", s,
-            k_dscan_tiles<<<nparts, DSCAN_THREADS, 0, s>>>(in, n, part.get()));
-        REYN_KERNEL("k_dscan_parts", s,
-            k_dscan_parts<<<1, DSCAN_THREADS, 0, s>>>(part.get(), nparts));
+            k_dscan_tiles<<<nparts, DSCAN_THREADS, 0, s>>>(in, n, part));
+        REYN_KERNEL("k_dscan_parts", s, k_dscan_parts<<<1, DSCAN_THREADS, 0, s>>>(part, nparts));
         REYN_KERNEL("k_dscan_apply", s,
-            k_dscan_apply<<<nparts, DSCAN_THREADS, 0, s>>>(in, n, part.get(), out));
+            k_dscan_apply<<<nparts, DSCAN_THREADS, 0, s>>>(in, n, part, out));
     }
 
     // ---- Morton codes and the radix sort ----------------------------------------
-    // 10 bits of v spread to every third bit (bit i -> bit 3i)
-    __device__ __forceinline__ uint32_t spread10(uint32_t v)
-    {
-        v &= 0x3ffu;
-        v = (v | (v << 16)) & 0x030000FFu;
-        v = (v | (v << 8)) & 0x0300F00Fu;
-        v = (v | (v << 4)) & 0x030C30C3u;
-        v = (v | (v << 2)) & 0x09249249u;
-        return v;
-    }
-
     __device__ __forceinline__ uint32_t quantise(double n)
     {
         return uint32_t(__double2float_rn(fmin(fmax(__dmul_rn(n, 1024.0), 0.0), 1023.0)));
@@ -502,30 +530,58 @@ namespace {
         }
     }
 
-    // scratch of the radix sort; must outlive the enqueued kernels
-    struct SortScratch {
-        DevArray<uint32_t> k2, v2, hist, offs, part;
+    // 256-byte aligned sub-arrays of one device allocation: add() the sizes,
+    // allocate bytes, then take the pointers at the returned offsets
+    struct Carve {
+        size_t bytes = 0;
+        template <class T> size_t add(size_t n)
+        {
+            const size_t o = (bytes + 255) & ~size_t(255);
+            bytes = o + std::max<size_t>(n, 1) * sizeof(T);
+            return o;
+        }
+    };
+    template <class T> T* at(const DevArray<unsigned char>& a, size_t off)
+    {
+        return reinterpret_cast<T*>(a.get() + off);
+    }
+
+    inline uint32_t radix_tiles(uint32_t n) { return (n + RADIX_TILE - 1) / RADIX_TILE; }
+
+    // scratch of the radix sort of n pairs (all must outlive the kernels):
+    // k2, v2: n each; hist: 256 radix_tiles(n); offs: that + 1
+    struct SortBufs {
+        uint32_t *k2, *v2, *hist, *offs;
+    };
+    struct SortLayout {
+        size_t k2, v2, hist, offs;
+        SortLayout(Carve& c, uint32_t n)
+            : k2(c.add<uint32_t>(n))
+            , v2(c.add<uint32_t>(n))
+            , hist(c.add<uint32_t>(size_t(radix_tiles(n)) * 256))
+            , offs(c.add<uint32_t>(size_t(radix_tiles(n)) * 256 + 1))
+        {
+        }
+        SortBufs at(const DevArray<unsigned char>& a) const
+        {
+            return SortBufs { reyn::at<uint32_t>(a, k2), reyn::at<uint32_t>(a, v2),
+                reyn::at<uint32_t>(a, hist), reyn::at<uint32_t>(a, offs) };
+        }
     };
 
     // sorts (keys, vals) by the 32 key bits, stably; results in place
-    void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, SortScratch& w, cudaStream_t s)
+    void radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, const SortBufs& w,
+        DevArray<uint32_t>& part, cudaStream_t s)
     {
-        const uint32_t n_tiles = (n + RADIX_TILE - 1) / RADIX_TILE;
-        w.k2.resize(n);
-        w.v2.resize(n);
-        w.hist.resize(size_t(n_tiles) * 256);
-        w.offs.resize(size_t(n_tiles) * 256 + 1);
-        DevArray<uint32_t>& hist = w.hist;
-        DevArray<uint32_t>& offs = w.offs;
-        DevArray<uint32_t>& part = w.part;
-        uint32_t *ka = keys, *va = vals, *kb = w.k2.get(), *vb = w.v2.get();
+        const uint32_t n_tiles = radix_tiles(n);
+        uint32_t *ka = keys, *va = vals, *kb = w.k2, *vb = w.v2;
         for (int shift = 0; shift < 32; shift += 8) {
             REYN_KERNEL("k_radix_hist", s,
-                k_radix_hist<<<n_tiles, RADIX_THREADS, 0, s>>>(n, ka, shift, n_tiles, hist.get()));
-            exclusive_scan(hist.get(), int64_t(n_tiles) * 256, part, offs.get(), s);
+                k_radix_hist<<<n_tiles, RADIX_THREADS, 0, s>>>(n, ka, shift, n_tiles, w.hist));
+            exclusive_scan(w.hist, int64_t(n_tiles) * 256, part, w.offs, s);
             REYN_KERNEL("k_radix_scatter", s,
-                k_radix_scatter<<<n_tiles, RADIX_THREADS, 0, s>>>(n, ka, va, shift, n_tiles,
-                offs.get(), kb, vb));
+                k_radix_scatter<<<n_tiles, RADIX_THREADS, 0, s>>>(n, ka, va, shift, n_tiles, w.offs,
+                kb, vb));
             std::swap(ka, kb);
             std::swap(va, vb);
         }
@@ -899,6 +955,34 @@ namespace {
         z[o] = p.z;
     }
 
+    // scratch of a query batch in Morton order (kept by the mesh, so that
+    // the asynchronous queries never outlive it)
+    struct QueryScratch {
+        DevArray<unsigned char> buf; // codes, ids, pts, sort buffers
+        DevArray<uint32_t> part;
+        uint32_t cap = 0;
+        uint32_t *codes = nullptr, *ids = nullptr;
+        float4* pts = nullptr;
+        SortBufs sort {};
+        void reserve(uint32_t n)
+        {
+            if (n <= cap)
+                return;
+            Carve c;
+            const size_t oc = c.add<uint32_t>(n), oi = c.add<uint32_t>(n), op = c.add<float4>(n);
+            const SortLayout sl(c, n);
+            buf.resize(c.bytes);
+            codes = at<uint32_t>(buf, oc);
+            ids = at<uint32_t>(buf, oi);
+            pts = at<float4>(buf, op);
+            sort = sl.at(buf);
+            cap = n;
+        }
+    };
+
+    // below this many points a query batch runs in the caller's order
+    constexpr uint32_t QUERY_SORT_MIN = 1u << 15;
+
 } // namespace
 } // namespace reyn
 
@@ -906,25 +990,50 @@ using namespace reyn;
 
 struct reyn_mesh {
     uint32_t nv = 0, nf = 0;
-    DevArray<double> vx, vy, vz;
-    DevArray<uint32_t> faces;   // 3 per face, original order
-    DevArray<double> cdf;       // inclusive area sums, original face order
+    DevArray<unsigned char> store; // one allocation holding every array below
+    double *vx = nullptr, *vy = nullptr, *vz = nullptr;
+    uint32_t* faces = nullptr;     // 3 per face, original order
+    double* cdf = nullptr;         // inclusive area sums, original face order
     double area = 0.0, volume = 0.0;
     double lo[3] = { 0, 0, 0 }, hi[3] = { 0, 0, 0 };
     // the LBVH
-    DevArray<uint32_t> order;   // original face of each leaf
-    DevArray<uint32_t> cl, cr;  // children of each internal node
-    DevArray<Box> leaf_box, node_box;
-    DevArray<Node> nodes;
-    DevArray<float4> tri;
-    DevArray<uint32_t> status;
+    uint32_t* order = nullptr;     // original face of each leaf
+    uint32_t *cl = nullptr, *cr = nullptr; // children of each internal node
+    Box *leaf_box = nullptr, *node_box = nullptr;
+    Node* nodes = nullptr;
+    float4* tri = nullptr;
+    uint32_t* status = nullptr;
     Box root {};
     uint32_t height = 0;
+    mutable QueryScratch query;
 
-    MeshView view() const
+    void allocate()
     {
-        return MeshView { nodes.get(), tri.get(), nf - 1, root, status.get() };
+        const size_t ni = std::max<uint32_t>(nf - 1, 1);
+        Carve c;
+        const size_t o_vx = c.add<double>(nv), o_vy = c.add<double>(nv), o_vz = c.add<double>(nv);
+        const size_t o_f = c.add<uint32_t>(3 * size_t(nf)), o_cdf = c.add<double>(nf);
+        const size_t o_ord = c.add<uint32_t>(nf), o_cl = c.add<uint32_t>(ni),
+                     o_cr = c.add<uint32_t>(ni);
+        const size_t o_lb = c.add<Box>(nf), o_nb = c.add<Box>(ni), o_n = c.add<Node>(ni),
+                     o_t = c.add<float4>(3 * size_t(nf)), o_s = c.add<uint32_t>(1);
+        store.resize(c.bytes);
+        vx = at<double>(store, o_vx);
+        vy = at<double>(store, o_vy);
+        vz = at<double>(store, o_vz);
+        faces = at<uint32_t>(store, o_f);
+        cdf = at<double>(store, o_cdf);
+        order = at<uint32_t>(store, o_ord);
+        cl = at<uint32_t>(store, o_cl);
+        cr = at<uint32_t>(store, o_cr);
+        leaf_box = at<Box>(store, o_lb);
+        node_box = at<Box>(store, o_nb);
+        nodes = at<Node>(store, o_n);
+        tri = at<float4>(store, o_t);
+        status = at<uint32_t>(store, o_s);
     }
+
+    MeshView view() const { return MeshView { nodes, tri, nf - 1, root, status }; }
     int stack() const { return height + 2 <= 32 ? 32 : 64; }
 };
 
@@ -937,6 +1046,29 @@ void launch_query(const reyn_mesh& m, uint32_t n, const float4* src, const uint3
 {
     if (!n)
         return;
+    if (!src && n >= QUERY_SORT_MIN) {
+        // queries in Morton order: the lanes of a warp then walk nearly the
+        // same nodes, where random order makes each warp wait for its
+        // costliest lane; results go back to the callers' slots
+        QueryScratch& q = m.query;
+        q.reserve(n);
+        float lo[3], sc[3];
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = float(m.lo[k]);
+            const double ext = m.hi[k] - m.lo[k];
+            sc[k] = ext > 0.0 ? float(1024.0 / ext) : 0.f;
+        }
+        REYN_KERNEL("k_query_keys", s,
+            k_query_keys<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, xin, yin, zin,
+            make_float3(lo[0], lo[1], lo[2]), make_float3(sc[0], sc[1], sc[2]), q.codes,
+            q.ids));
+        radix_sort_pairs(q.codes, q.ids, n, q.sort, q.part, s);
+        REYN_KERNEL("k_query_gather", s,
+            k_query_gather<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, q.ids, xin, yin, zin,
+            q.pts));
+        src = q.pts;
+        perm = q.ids;
+    }
     const unsigned b = blocks_for(n, MESH_THREADS);
     if (m.stack() == 32)
         REYN_KERNEL(INSIDE ? "k_mesh_inside" : "k_mesh_project", s,
@@ -951,7 +1083,7 @@ void launch_query(const reyn_mesh& m, uint32_t n, const float4* src, const uint3
 void check_traversal(const reyn_mesh& m, cudaStream_t s)
 {
     uint32_t st = 0;
-    REYN_CUDA(cudaMemcpyAsync(&st, m.status.get(), sizeof(st), cudaMemcpyDeviceToHost, s));
+    REYN_CUDA(cudaMemcpyAsync(&st, m.status, sizeof(st), cudaMemcpyDeviceToHost, s));
     REYN_CUDA(cudaStreamSynchronize(s));
     if (st)
         fail(REYN_ERR_CUDA, (st & MESH_BAD_TREE) ? "LBVH traversal met a malformed tree"
@@ -961,70 +1093,68 @@ void check_traversal(const reyn_mesh& m, cudaStream_t s)
 void build_mesh(reyn_mesh& m, cudaStream_t s)
 {
     const uint32_t nf = m.nf;
+    const uint32_t ni = nf > 1 ? nf - 1 : 0;
+    // the build's temporaries, one allocation
+    Carve c;
+    const size_t o_area = c.add<double>(nf), o_vol = c.add<double>(nf), o_vsum = c.add<double>(nf);
+    const size_t o_pa = c.add<double>(dscan_parts(nf)), o_pv = c.add<double>(dscan_parts(nf));
+    const size_t o_codes = c.add<uint32_t>(nf);
+    const SortLayout sl(c, nf);
+    const size_t o_pn = c.add<uint32_t>(std::max<uint32_t>(ni, 1)), o_pl = c.add<uint32_t>(nf);
+    const size_t o_visit = c.add<uint32_t>(std::max<uint32_t>(ni, 1)), o_h = c.add<uint32_t>(1);
+    DevArray<unsigned char> tmp(c.bytes);
+    DevArray<uint32_t> part;
+    double* area = at<double>(tmp, o_area);
+    double* vol = at<double>(tmp, o_vol);
+    double* vsum = at<double>(tmp, o_vsum);
+    uint32_t* codes = at<uint32_t>(tmp, o_codes);
+    uint32_t* parent_node = at<uint32_t>(tmp, o_pn);
+    uint32_t* parent_leaf = at<uint32_t>(tmp, o_pl);
+    uint32_t* visit = at<uint32_t>(tmp, o_visit);
+    uint32_t* height = at<uint32_t>(tmp, o_h);
+    REYN_CUDA(cudaMemsetAsync(visit, 0, std::max<uint32_t>(ni, 1) * sizeof(uint32_t), s));
+    REYN_CUDA(cudaMemsetAsync(height, 0, sizeof(uint32_t), s));
+    REYN_CUDA(cudaMemsetAsync(m.status, 0, sizeof(uint32_t), s));
     // areas, volume, sampling CDF
-    {
-        DevArray<double> area(nf), vol(nf), vsum(nf), part_a, part_v;
-        m.cdf.resize(nf);
-        REYN_KERNEL("k_face_measure", s,
-            k_face_measure<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, m.vx.get(), m.vy.get(),
-            m.vz.get(), m.faces.get(), area.get(), vol.get()));
-        inclusive_scan_d(area.get(), nf, part_a, m.cdf.get(), s);
-        inclusive_scan_d(vol.get(), nf, part_v, vsum.get(), s);
-        double tot[2];
-        REYN_CUDA(cudaMemcpyAsync(&tot[0], m.cdf.get() + nf - 1, sizeof(double),
-            cudaMemcpyDeviceToHost, s));
-        REYN_CUDA(cudaMemcpyAsync(&tot[1], vsum.get() + nf - 1, sizeof(double),
-            cudaMemcpyDeviceToHost, s));
-        REYN_CUDA(cudaStreamSynchronize(s));
-        m.area = tot[0];
-        m.volume = std::fabs(tot[1]) / 6.0;
-    }
+    REYN_KERNEL("k_face_measure", s,
+        k_face_measure<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, m.vx, m.vy, m.vz, m.faces,
+        area, vol));
+    inclusive_scan_d(area, nf, at<double>(tmp, o_pa), m.cdf, s);
+    inclusive_scan_d(vol, nf, at<double>(tmp, o_pv), vsum, s);
     // Morton codes, sorted with the face ids
-    DevArray<uint32_t> codes(nf);
-    m.order.resize(nf);
     const double3 lo = make_double3(m.lo[0], m.lo[1], m.lo[2]);
     const double3 inv = make_double3(1.0 / (m.hi[0] - m.lo[0]), 1.0 / (m.hi[1] - m.lo[1]),
         1.0 / (m.hi[2] - m.lo[2]));
     REYN_KERNEL("k_morton", s,
-        k_morton<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, m.vx.get(), m.vy.get(), m.vz.get(),
-        m.faces.get(), lo, inv, codes.get(), m.order.get()));
-    SortScratch sort_scratch;
-    radix_sort_pairs(codes.get(), m.order.get(), nf, sort_scratch, s);
+        k_morton<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, m.vx, m.vy, m.vz, m.faces, lo, inv,
+        codes, m.order));
+    radix_sort_pairs(codes, m.order, nf, sl.at(tmp), part, s);
     // tree, boxes, traversal records, height
-    const uint32_t ni = nf > 1 ? nf - 1 : 0;
-    m.cl.resize(std::max<uint32_t>(ni, 1));
-    m.cr.resize(std::max<uint32_t>(ni, 1));
-    m.leaf_box.resize(nf);
-    m.node_box.resize(std::max<uint32_t>(ni, 1));
-    m.nodes.resize(std::max<uint32_t>(ni, 1));
-    m.tri.resize(3 * size_t(nf));
-    m.status.resize(1);
-    m.status.zero(s);
-    DevArray<uint32_t> parent_node(std::max<uint32_t>(ni, 1)), parent_leaf(nf),
-        visit(std::max<uint32_t>(ni, 1)), height(1);
-    visit.zero(s);
-    height.zero(s);
     if (ni)
         REYN_KERNEL("k_karras", s,
-            k_karras<<<blocks_for(ni, THREADS), THREADS, 0, s>>>(nf, codes.get(), m.cl.get(),
-            m.cr.get(), parent_node.get(), parent_leaf.get()));
+            k_karras<<<blocks_for(ni, THREADS), THREADS, 0, s>>>(nf, codes, m.cl, m.cr, parent_node,
+            parent_leaf));
     REYN_KERNEL("k_lbvh_boxes", s,
-        k_lbvh_boxes<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, m.order.get(), m.vx.get(),
-        m.vy.get(), m.vz.get(), m.faces.get(), parent_node.get(), parent_leaf.get(), m.cl.get(),
-        m.cr.get(), visit.get(), m.leaf_box.get(), m.node_box.get(), m.status.get()));
+        k_lbvh_boxes<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, m.order, m.vx, m.vy, m.vz,
+        m.faces, parent_node, parent_leaf, m.cl, m.cr, visit, m.leaf_box, m.node_box, m.status));
     REYN_KERNEL("k_lbvh_pack", s,
-        k_lbvh_pack<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, m.order.get(), m.vx.get(),
-        m.vy.get(), m.vz.get(), m.faces.get(), m.cl.get(), m.cr.get(), m.leaf_box.get(),
-        m.node_box.get(), m.nodes.get(), m.tri.get(), m.status.get()));
+        k_lbvh_pack<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, m.order, m.vx, m.vy, m.vz,
+        m.faces, m.cl, m.cr, m.leaf_box, m.node_box, m.nodes, m.tri, m.status));
     REYN_KERNEL("k_lbvh_height", s,
-        k_lbvh_height<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, parent_node.get(),
-        parent_leaf.get(), height.get()));
-    REYN_CUDA(cudaMemcpyAsync(&m.height, height.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    REYN_CUDA(cudaMemcpyAsync(&m.root, ni ? m.node_box.get() : m.leaf_box.get(), sizeof(Box),
-        cudaMemcpyDeviceToHost, s));
+        k_lbvh_height<<<blocks_for(nf, THREADS), THREADS, 0, s>>>(nf, parent_node, parent_leaf,
+        height));
+    // one readback: totals, height, root box, status
+    double tot[2];
     uint32_t st = 0;
-    REYN_CUDA(cudaMemcpyAsync(&st, m.status.get(), sizeof(st), cudaMemcpyDeviceToHost, s));
+    REYN_CUDA(cudaMemcpyAsync(&tot[0], m.cdf + nf - 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+    REYN_CUDA(cudaMemcpyAsync(&tot[1], vsum + nf - 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+    REYN_CUDA(cudaMemcpyAsync(&m.height, height, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    REYN_CUDA(cudaMemcpyAsync(&m.root, ni ? m.node_box : m.leaf_box, sizeof(Box),
+        cudaMemcpyDeviceToHost, s));
+    REYN_CUDA(cudaMemcpyAsync(&st, m.status, sizeof(st), cudaMemcpyDeviceToHost, s));
     REYN_CUDA(cudaStreamSynchronize(s));
+    m.area = tot[0];
+    m.volume = std::fabs(tot[1]) / 6.0;
     if (st)
         fail(REYN_ERR_CUDA, "LBVH construction produced a malformed tree");
     if (m.height + 2 > 64)
@@ -1129,14 +1259,11 @@ void create_mesh(const double* vx, const double* vy, const double* vz, uint32_t 
         }
     for (uint64_t i = 0; i < 3ull * nf; ++i)
         require(faces[i] < nv, "face vertex index out of range");
-    m->vx.resize(nv);
-    m->vy.resize(nv);
-    m->vz.resize(nv);
-    m->faces.resize(3 * size_t(nf));
-    REYN_CUDA(cudaMemcpyAsync(m->vx.get(), vx, nv * sizeof(double), cudaMemcpyHostToDevice, s));
-    REYN_CUDA(cudaMemcpyAsync(m->vy.get(), vy, nv * sizeof(double), cudaMemcpyHostToDevice, s));
-    REYN_CUDA(cudaMemcpyAsync(m->vz.get(), vz, nv * sizeof(double), cudaMemcpyHostToDevice, s));
-    REYN_CUDA(cudaMemcpyAsync(m->faces.get(), faces, 3 * size_t(nf) * sizeof(uint32_t),
+    m->allocate();
+    REYN_CUDA(cudaMemcpyAsync(m->vx, vx, nv * sizeof(double), cudaMemcpyHostToDevice, s));
+    REYN_CUDA(cudaMemcpyAsync(m->vy, vy, nv * sizeof(double), cudaMemcpyHostToDevice, s));
+    REYN_CUDA(cudaMemcpyAsync(m->vz, vz, nv * sizeof(double), cudaMemcpyHostToDevice, s));
+    REYN_CUDA(cudaMemcpyAsync(m->faces, faces, 3 * size_t(nf) * sizeof(uint32_t),
         cudaMemcpyHostToDevice, s));
     build_mesh(*m, s);
     *out = m.release();
@@ -1225,11 +1352,11 @@ extern "C" int reyn_mesh_tree(const reyn_mesh* mesh, uint32_t* order, uint32_t* 
             if (dst && bytes)
                 REYN_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
         };
-        copy(order, mesh->order.get(), nf * sizeof(uint32_t));
-        copy(children_l, mesh->cl.get(), ni * sizeof(uint32_t));
-        copy(children_r, mesh->cr.get(), ni * sizeof(uint32_t));
-        copy(leaf_box, mesh->leaf_box.get(), nf * sizeof(Box));
-        copy(node_box, mesh->node_box.get(), ni * sizeof(Box));
+        copy(order, mesh->order, nf * sizeof(uint32_t));
+        copy(children_l, mesh->cl, ni * sizeof(uint32_t));
+        copy(children_r, mesh->cr, ni * sizeof(uint32_t));
+        copy(leaf_box, mesh->leaf_box, nf * sizeof(Box));
+        copy(node_box, mesh->node_box, ni * sizeof(Box));
     });
 }
 
@@ -1276,9 +1403,9 @@ extern "C" int reyn_mesh_sample_uniform(const reyn_mesh* mesh, float h, float ov
         require(capacity >= n, "output arrays hold fewer samples than the mesh needs");
         const cudaStream_t s = as_stream(stream);
         REYN_KERNEL("k_mesh_sample", s,
-            k_mesh_sample<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, mesh->nf, mesh->cdf.get(),
-            mesh->area, mesh->area / double(n), seed, mesh->vx.get(), mesh->vy.get(),
-            mesh->vz.get(), mesh->faces.get(), x, y, z));
+            k_mesh_sample<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, mesh->nf, mesh->cdf,
+            mesh->area, mesh->area / double(n), seed, mesh->vx, mesh->vy,
+            mesh->vz, mesh->faces, x, y, z));
     });
 }
 
@@ -1309,13 +1436,19 @@ extern "C" int reyn_mesh_relax(const reyn_mesh* mesh, float* x, float* y, float*
         const float rho0 = hex_plane_density(h_bdy);
         const float inv2 = 1.f / (rho0 * rho0);
         const float coef = (-relaxation_factor * h_bdy) * h_bdy;
-        DevArray<float4> pts(n), moved(n);
-        DevArray<float> nd(n);
-        DevArray<unsigned> mnmx(2 * size_t(iters));
-        DevArray<double> sums(iters);
-        DevArray<uint32_t> status(1);
-        status.zero(s);
-        sums.zero(s);
+        Carve c;
+        const size_t o_pts = c.add<float4>(n), o_mv = c.add<float4>(n), o_nd = c.add<float>(n);
+        const size_t o_mm = c.add<unsigned>(2 * size_t(iters)), o_sum = c.add<double>(iters);
+        const size_t o_st = c.add<uint32_t>(1);
+        DevArray<unsigned char> tmp(c.bytes);
+        float4* pts = at<float4>(tmp, o_pts);
+        float4* moved = at<float4>(tmp, o_mv);
+        float* nd = at<float>(tmp, o_nd);
+        unsigned* mnmx = at<unsigned>(tmp, o_mm);
+        double* sums = at<double>(tmp, o_sum);
+        uint32_t* status = at<uint32_t>(tmp, o_st);
+        REYN_CUDA(cudaMemsetAsync(status, 0, sizeof(uint32_t), s));
+        REYN_CUDA(cudaMemsetAsync(sums, 0, iters * sizeof(double), s));
         {
             std::vector<unsigned> init(2 * size_t(iters));
             const float big = FLT_MAX;
@@ -1323,7 +1456,7 @@ extern "C" int reyn_mesh_relax(const reyn_mesh* mesh, float* x, float* y, float*
                 std::memcpy(&init[2 * it], &big, sizeof(float));
                 init[2 * it + 1] = 0u;
             }
-            REYN_CUDA(cudaMemcpyAsync(mnmx.get(), init.data(), init.size() * sizeof(unsigned),
+            REYN_CUDA(cudaMemcpyAsync(mnmx, init.data(), init.size() * sizeof(unsigned),
                 cudaMemcpyHostToDevice, s));
             REYN_CUDA(cudaStreamSynchronize(s)); // `init` leaves scope
         }
@@ -1333,28 +1466,28 @@ extern "C" int reyn_mesh_relax(const reyn_mesh* mesh, float* x, float* y, float*
             const GridView v = g.view(g.geom.r);
             REYN_KERNEL("k_relax_gather", s,
                 k_relax_gather<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, g.sorted.get(), x, y, z,
-                pts.get()));
+                pts));
             REYN_KERNEL("k_relax_density", s,
-                k_relax_density<1><<<b, MESH_THREADS, 0, s>>>(n, v, kc, pts.get(), nd.get(),
-                status.get()));
+                k_relax_density<1><<<b, MESH_THREADS, 0, s>>>(n, v, kc, pts, nd,
+                status));
             REYN_KERNEL("k_relax_stats", s,
-                k_relax_stats<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, nd.get(),
-                mnmx.get() + 2 * it, mnmx.get() + 2 * it + 1, sums.get() + it));
+                k_relax_stats<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, nd,
+                mnmx + 2 * it, mnmx + 2 * it + 1, sums + it));
             REYN_KERNEL("k_relax_shift", s,
-                k_relax_shift<1><<<b, MESH_THREADS, 0, s>>>(n, v, kc, pts.get(), nd.get(), inv2, coef,
-                g.sorted.get(), moved.get(), it + 1 == iters ? num_den : nullptr));
+                k_relax_shift<1><<<b, MESH_THREADS, 0, s>>>(n, v, kc, pts, nd, inv2, coef,
+                g.sorted.get(), moved, it + 1 == iters ? num_den : nullptr));
             // back onto the mesh, in grid order, results to the samples' slots
-            launch_query<false>(*mesh, n, moved.get(), g.sorted.get(), nullptr, nullptr, nullptr, x, y,
+            launch_query<false>(*mesh, n, moved, g.sorted.get(), nullptr, nullptr, nullptr, x, y,
                 z, nullptr, s);
         }
         std::vector<unsigned> mm(2 * size_t(iters));
         std::vector<double> sm(iters);
         uint32_t st = 0;
-        REYN_CUDA(cudaMemcpyAsync(mm.data(), mnmx.get(), mm.size() * sizeof(unsigned),
+        REYN_CUDA(cudaMemcpyAsync(mm.data(), mnmx, mm.size() * sizeof(unsigned),
             cudaMemcpyDeviceToHost, s));
-        REYN_CUDA(cudaMemcpyAsync(sm.data(), sums.get(), sm.size() * sizeof(double),
+        REYN_CUDA(cudaMemcpyAsync(sm.data(), sums, sm.size() * sizeof(double),
             cudaMemcpyDeviceToHost, s));
-        REYN_CUDA(cudaMemcpyAsync(&st, status.get(), sizeof(st), cudaMemcpyDeviceToHost, s));
+        REYN_CUDA(cudaMemcpyAsync(&st, status, sizeof(st), cudaMemcpyDeviceToHost, s));
         REYN_CUDA(cudaStreamSynchronize(s));
         check_traversal(*mesh, s);
         if (st)

@@ -124,7 +124,7 @@ def write_obj(path: str, shapes) -> None:
         for name, v, f in shapes:
             fh.write(f"o {name}\n")
             for p in np.asarray(v, float):
-                fh.write(f"v {p[0]!r} {p[1]!r} {p[2]!r}\n")
+                fh.write(f"v {float(p[0])!r} {float(p[1])!r} {float(p[2])!r}\n")
             for t in np.asarray(f, np.int64):
                 fh.write(f"f {t[0] + base + 1} {t[1] + base + 1} {t[2] + base + 1}\n")
             base += len(v)

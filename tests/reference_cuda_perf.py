@@ -13,8 +13,12 @@ against, not part of the product.
    benchmark scene at a fixed dt, same boundary masses. Both sides run once
    untimed first (kernel loading, buffer allocation), then the same steps
    from the same initial state are timed.
+3. (--mesh) The mesh path on bench.py's mesh_lbvh workload (327,680-face
+   perturbed icosphere): the LBVH build, a device copy plus LBVH::project of
+   16.7M seeded points, and sample_mesh at h = 0.004 with 50 relaxation
+   sweeps. Each side builds once untimed first.
 
-Usage: python tests/reference_cuda_perf.py [--iisph-steps K] [--out FILE]
+Usage: python tests/reference_cuda_perf.py [--iisph-steps K] [--mesh] [--out FILE]
 """
 from __future__ import annotations
 
@@ -148,14 +152,97 @@ def iisph_compare(steps: int, dt: float, scale: int):
             "speedup": ref["ms_per_step"] / eng["ms_per_step"]}
 
 
+def mesh_compare(reps: int, scale: int = 1) -> dict:
+    import torch
+
+    import bench
+    import reyn_b200 as rb
+    v, f = bench.mesh_workload(scale)
+    v = np.ascontiguousarray(v, np.float64)
+    f = np.ascontiguousarray(f, np.uint32)
+    n = (1 << 24) // scale ** 3
+    lo, hi = v.min(0) - 0.1, v.max(0) + 0.1
+    rng = np.random.Generator(np.random.PCG64(1234))
+    q = (lo + (hi - lo) * rng.random((n, 3))).astype(np.float32)
+    qx, qy, qz = (np.ascontiguousarray(q[:, k]) for k in range(3))
+    L = oracle.ref_cuda()
+    d = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    L.ref_mesh_bench.argtypes = [ctypes.c_uint, d, d, d, ctypes.c_uint, ctypes.c_void_p,
+                                 ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                 ctypes.c_uint, ctypes.c_float, ctypes.c_int, ctypes.c_void_p,
+                                 ctypes.c_void_p]
+    ms = np.zeros(4, np.float32)
+    cnt = np.zeros(1, np.uint32)
+    vx, vy, vz = (np.ascontiguousarray(v[:, k]) for k in range(3))
+    rc = L.ref_mesh_bench(v.shape[0], vx, vy, vz, f.shape[0], P(f), n, P(qx), P(qy), P(qz), reps,
+                          0.004 * scale, 50, P(ms), P(cnt))
+    if rc:
+        raise RuntimeError(L.ref_last_error().decode())
+    # the engine, same inputs
+    dev = torch.device("cuda")
+    stream = torch.cuda.current_stream()
+    S = stream.cuda_stream
+    rb.Mesh(v, f, stream=S).close()  # untimed first build
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    mesh = rb.Mesh(v, f, stream=S)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    e_build = ev[0].elapsed_time(ev[1])
+    pristine = [torch.from_numpy(a).to(dev) for a in (qx, qy, qz)]
+    work = [t.clone() for t in pristine]
+
+    def once():
+        for w_, p_ in zip(work, pristine):
+            w_.copy_(p_)
+        mesh.project(*work, stream=S)
+
+    once()
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for _ in range(reps):
+        once()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    e_proj = ev[0].elapsed_time(ev[1]) / reps
+    e_sample = 1e30
+    for _ in range(2):  # best of two, as on the reference side
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        bdy, (sx, _, _), _ = rb.sample_mesh(mesh, 0.004 * scale, 1000.0, 2.0,
+                                            relaxation_iters=50, stream=S)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        e_sample = min(e_sample, ev[0].elapsed_time(ev[1]))
+        bdy.close()
+    out = {"faces": int(f.shape[0]), "queries": n,
+           "reference_cuda_ms": {"build": float(ms[0]), "upload_and_build": float(ms[3]),
+                                 "copy_and_project": float(ms[1]),
+                                 "sample_mesh_50_sweeps": float(ms[2]),
+                                 "samples": int(cnt[0])},
+           "engine_ms": {"upload_and_build": e_build, "copy_and_project": e_proj,
+                         "sample_mesh_50_sweeps": e_sample, "samples": int(sx.numel())}}
+    mesh.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--iisph-steps", type=int, default=5)
     ap.add_argument("--scale", type=int, default=1)
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--mesh", action="store_true", help="only the mesh comparison")
     a = ap.parse_args()
     res = {}
+    if a.mesh:
+        res["mesh_lbvh"] = mesh_compare(max(a.reps // 4, 2), a.scale)
+        print(json.dumps(res), flush=True)
+        if a.out:
+            with open(a.out, "w") as f:
+                json.dump(res, f, indent=1)
+        return
     x, y, z, box = grid_case()
     r = 2.2
     rb_, rq = reference_grid(x, y, z, float(box), r, a.reps)

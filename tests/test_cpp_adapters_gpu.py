@@ -103,3 +103,26 @@ def test_cpp_main_loop_fused_tail_is_bit_identical(cuda, tmp_path):
     np.testing.assert_array_equal(da, db)
     for k in a:
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
+def test_cpp_mesh_adapters(cuda, tmp_path):
+    """DeviceMesh / uniform_sample_mesh / relax_sampling / LBVH::project /
+    BoundarySamples in the reference's calling pattern (tests/cpp/mesh_adapter.cpp)"""
+    exe = os.path.join(str(tmp_path), "mesh_adapter")
+    cxx = shutil.which("g++") or "g++"
+    subprocess.run([cxx, "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"),
+                    "-I/usr/local/cuda/include", os.path.join(ROOT, "tests", "cpp",
+                                                              "mesh_adapter.cpp"),
+                    "-L" + os.path.join(ROOT, "reyn_b200"), "-lreyn_b200",
+                    "-L/usr/local/cuda/lib64", "-lcudart",
+                    "-Wl,-rpath," + os.path.join(ROOT, "reyn_b200"), "-o", exe], check=True)
+    out = subprocess.run([exe, "1.0"], capture_output=True, text=True, check=True).stdout.split()
+    n = int(out[0])
+    # octahedron of "radius" 1: 8 equilateral faces of side sqrt(2)
+    area = 8 * np.sqrt(3) / 4 * 2.0
+    assert n == oracle.mesh_sample_count(area, 0.05, 2.0)
+    first, last = out[1].split(","), out[2].split(",")
+    assert first[0] == "1" and last[0] == "10"
+    assert float(last[1]) < float(first[1])       # max/min number density ratio falls
+    assert float(out[3]) < 1e-5                    # every sample on the surface
+    assert float(out[4]) == pytest.approx(4.0 / 3.0, rel=1e-12)

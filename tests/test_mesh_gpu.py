@@ -213,3 +213,38 @@ def test_size_queries_and_capacity(cuda):
                                       small.data_ptr(), 1, ctypes.byref(cnt),
                                       None) == rb.ERR_INVALID
     m.close()
+
+
+@pytest.mark.parametrize("name", ["ico3", "ico4_perturbed", "box4", "torus_perturbed"])
+def test_tree_matches_reference_fixture(cuda, name):
+    """the engine's LBVH against the reference's own (tests/golden/mesh_*.npz)"""
+    import reyn_b200 as rb
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                             f"mesh_{name}.npz"))
+    m = rb.Mesh(g["verts"], g["faces"])
+    t = {k: v.cpu().numpy() for k, v in m.tree().items()}
+    np.testing.assert_array_equal(g["faces"][t["order"]], g["faces_sorted"])
+    np.testing.assert_array_equal(t["children_l"].astype(np.uint32), g["children_l"])
+    np.testing.assert_array_equal(t["children_r"].astype(np.uint32), g["children_r"])
+    np.testing.assert_array_equal(t["leaf_box"], g["leaf_box"])
+    np.testing.assert_array_equal(t["node_box"], g["node_box"])
+    assert m.info().tree_height == int(g["height"])
+    assert m.info().volume == pytest.approx(float(g["volume"]), rel=1e-12)
+    m.close()
+
+
+@pytest.mark.parametrize("name", ["ico6_perturbed", "torus_perturbed"])
+def test_large_query_batches_match_oracle(cuda, name):
+    """batches of 2^15 points and more run in Morton order; results return to
+    the callers' slots unchanged"""
+    import reyn_b200 as rb
+    v, f = CASES[name]
+    m = rb.Mesh(v, f)
+    x, y, z = points(v, 100003, 29)
+    dx, dy, dz = dev(x, y, z)
+    np.testing.assert_array_equal(m.inside(dx, dy, dz).cpu().numpy(),
+                                  oracle.lbvh_inside(v, f, x, y, z))
+    m.project(dx, dy, dz)
+    for g, w in zip((dx, dy, dz), oracle.lbvh_project(v, f, x, y, z)):
+        np.testing.assert_array_equal(g.cpu().numpy(), w)
+    m.close()

@@ -277,3 +277,40 @@ def test_mesh_entry_points_reject_bad_arguments(tmp_path):
         rb.ERR_INVALID
     assert L.reyn_mesh_project(None, None, None, None, 0, None) == rb.ERR_INVALID
     assert L.reyn_mesh_fill(None, 0.1, 0.0, 1, None, None, None, 0, None, None) == rb.ERR_INVALID
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.mark.parametrize("name", ["ico3", "ico4_perturbed", "box4", "torus_perturbed"])
+def test_oracle_matches_reference_lbvh(name):
+    """Pinned against the reference's own LBVH (tests/golden/make_golden.py
+    --mesh ran lbvh.cuh's LBVH on a B200): the sorted faces, children, boxes
+    and height bit for bit, the volume, LBVH::project's results, and the
+    sample counts of uniform_sample_mesh."""
+    g = np.load(os.path.join(GOLDEN, f"mesh_{name}.npz"))
+    v, f = g["verts"], g["faces"]
+    t = oracle.lbvh_build(v, f)
+    np.testing.assert_array_equal(f[t["order"]], g["faces_sorted"])
+    np.testing.assert_array_equal(t["children_l"], g["children_l"])
+    np.testing.assert_array_equal(t["children_r"], g["children_r"])
+    np.testing.assert_array_equal(t["leaf_box"], g["leaf_box"])
+    np.testing.assert_array_equal(t["node_box"], g["node_box"])
+    assert t["height"] == int(g["height"])
+    area, vol, _ = oracle.mesh_measure(v, f)
+    assert vol == pytest.approx(float(g["volume"]), rel=1e-12)
+    q = g["points"]
+    a = np.stack(oracle.lbvh_project(v, f, q[:, 0], q[:, 1], q[:, 2]), 1)
+    b = g["projected"]
+    # the reference's device code may contract multiply-adds: distances agree
+    # to float rounding, points within its own test's bound (lbvh.cu:420-426)
+    a64, b64, q64 = (t.astype(np.float64) for t in (a, b, q))
+    np.testing.assert_allclose(np.sqrt(((a64 - q64) ** 2).sum(1)),
+                               np.sqrt(((b64 - q64) ** 2).sum(1)), rtol=1e-5, atol=1e-6)
+    assert np.all(((a64 - b64) ** 2).sum(1) <= 375 * F32_EPS)
+    # within 2 ulps but for near-ties between faces (same distance, another
+    # face's point): at most 0.5 % of the points
+    close = np.all(np.abs(a - b) <= 2.4e-7, 1)
+    assert np.mean(close) >= 0.995
+    for (h, ov), want in zip(g["sample_cases"], g["sample_counts"]):
+        assert oracle.mesh_sample_count(area, float(h), float(ov)) == int(want)
