@@ -401,6 +401,33 @@ int reyn_autotune(reyn_scheme scheme, const reyn_params* params,
     const float* scene_min, const float* scene_max, float dt, uint32_t steps,
     reyn_tune_point* best, reyn_tune_point* points, void* stream);
 
+/* ---- captured steps (no counterpart in the reference) -------------------- */
+typedef struct reyn_step_graph reyn_step_graph;
+/* Records one full step of the main loop at a fixed dt — construct_and_reorder
+ * of `grid` over `state`, then the solver's step, with hard bounds when
+ * bound_min/bound_max are given (for a batched grid each scene's own box; the
+ * values are then unused) — as CUDA graphs, one per buffer parity of the
+ * state. The pressure loop of PCISPH and IISPH runs as a conditional while
+ * node whose condition a kernel sets after each sweep with the plain step's
+ * stopping rule, so a launch needs no host round trip; results equal the
+ * plain calls'. The solver, state, grid and boundary must outlive the graph,
+ * and the state keeps its particle count. Synchronises. */
+int reyn_step_graph_create(reyn_solver* s, reyn_particles* state, reyn_grid* grid,
+    const reyn_boundary* bdy, float dt, const float bound_min[3],
+    const float bound_max[3], reyn_step_graph** out);
+/* one step: the graph launch on `stream` plus the host bookkeeping of the plain
+ * calls (no synchronisation); plain steps may be interleaved */
+int reyn_step_graph_launch(reyn_step_graph* g, void* stream);
+/* the last launched step's sweeps and density errors (synchronises the
+ * stream); returns the status the plain calls would have returned for it
+ * (REYN_ERR_ITER_LIMIT, REYN_ERR_OUT_OF_BOUNDS, REYN_ERR_NONFINITE) */
+int reyn_step_graph_stats(reyn_step_graph* g, reyn_step_stats* out,
+    void* stream);
+/* kernels per step outside the pressure loop, and per sweep inside it */
+int reyn_step_graph_info(const reyn_step_graph* g, uint32_t* step_kernels,
+    uint32_t* sweep_kernels);
+int reyn_step_graph_destroy(reyn_step_graph* g);
+
 /* ---- scene generation (src/scene/scene.cu) ------------------------------- */
 /* _init_box_kernel (scene.cu:14-37) with seeded jitter (scene.cu:232-253):
  * particles first .. first + nx*ny*nz - 1 of the state become a lattice of

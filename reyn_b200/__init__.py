@@ -160,6 +160,12 @@ _SIGNATURES = {
     "reyn_mesh_relax": [_vp, _vp, _vp, _vp, _u32, _f, _f, _u32, _vp, _vp, _vp],
     "reyn_mesh_fill": [_vp, _f, _f, ctypes.c_uint64, _vp, _vp, _vp, _u32, ctypes.POINTER(_u32),
                        _vp],
+    "reyn_step_graph_create": [_vp, _vp, _vp, _vp, _f, ctypes.POINTER(_f), ctypes.POINTER(_f),
+                               ctypes.POINTER(_vp)],
+    "reyn_step_graph_launch": [_vp, _vp],
+    "reyn_step_graph_stats": [_vp, ctypes.POINTER(StepStats), _vp],
+    "reyn_step_graph_info": [_vp, ctypes.POINTER(_u32), ctypes.POINTER(_u32)],
+    "reyn_step_graph_destroy": [_vp],
     "reyn_profile_enable": [ctypes.c_int],
     "reyn_profile_reset": [],
     "reyn_profile_read": [ctypes.POINTER(ProfileEntry), _u32, ctypes.POINTER(_u32)],
@@ -373,6 +379,43 @@ class Boundary:
         check(lib().reyn_boundary_arrays(self.h, *[ctypes.byref(p) for p in ps],
                                          ctypes.byref(nb)))
         return [p.value for p in ps], nb.value
+
+
+class StepGraph:
+    """One full step (construct_and_reorder + the solver step, bounded when
+    `bounds` is given; a batched grid uses its scenes' boxes) captured as CUDA
+    graphs at a fixed dt; launch() replays it."""
+
+    def __init__(self, solver: "Solver", state: Particles, grid: Grid, bdy, dt: float,
+                 bounds=None):
+        hdl = _vp()
+        lo = _f3(bounds[0]) if bounds is not None else None
+        hi = _f3(bounds[1]) if bounds is not None else None
+        check(lib().reyn_step_graph_create(solver.h, state.h, grid.h, bdy.h if bdy else None, dt,
+                                           lo, hi, ctypes.byref(hdl)))
+        self.h = hdl
+
+    def launch(self, stream=None) -> None:
+        check(lib().reyn_step_graph_launch(self.h, _stream(stream)))
+
+    def stats(self, stream=None) -> StepStats:
+        """The last launch's sweeps and errors; raises as the plain step would."""
+        out = StepStats()
+        check(lib().reyn_step_graph_stats(self.h, ctypes.byref(out), _stream(stream)))
+        return out
+
+    def info(self):
+        """(kernels per step outside the pressure loop, kernels per sweep)"""
+        a, b = _u32(), _u32()
+        check(lib().reyn_step_graph_info(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.reyn_step_graph_destroy(self.h)
+        self.h = None
+
+    __del__ = close
 
 
 class Mesh:

@@ -9,6 +9,34 @@
 #include <memory>
 #include <vector>
 
+namespace reyn {
+
+// statistics of a captured step, kept on the device
+struct GraphStats {
+    uint32_t iters;       // sweeps of the pressure loop
+    uint32_t unconverged; // 1: stopped by max_iter before converging
+    double avg_err;       // last average density error (relative)
+    double max_err;       // last maximum density error (IISPH)
+};
+
+// the capture of one step (reyn_step_graph): the loop bodies are captured on
+// `body`; kernel names go to top_names / body_names instead of the launch
+// counters
+struct GraphCtx {
+    cudaStream_t body = nullptr;
+    GraphStats* stats = nullptr; // device
+    uint32_t* gate = nullptr;    // device: IISPH pressure-pass gate
+    std::vector<const char*> top_names, body_names;
+};
+
+// while sink is non-null, REYN_KERNEL appends each launch's name to it
+// instead of counting and timing it (this thread only)
+void profile_record(std::vector<const char*>* sink);
+// adds `times` launches of each named kernel to the launch counters
+void profile_count(const std::vector<const char*>& names, uint64_t times);
+
+} // namespace reyn
+
 // C-ABI handle types are the engine classes themselves
 struct reyn_particles;
 struct reyn_grid;
@@ -143,6 +171,8 @@ struct reyn_solver {
     const reyn_particles* vmax_state = nullptr;
     uint64_t vmax_version = 0;
     bool vmax_valid = false;
+    // non-null while a step of this solver is being captured into a graph
+    reyn::GraphCtx* graph = nullptr;
     ~reyn_solver()
     {
         if (vmax_ready)
@@ -174,6 +204,12 @@ void pack_state(reyn_particles& st, cudaStream_t s);
 
 void reorder_state(reyn_particles& st, Grid& g, float* const* extra,
     uint32_t n_extra, cudaStream_t s);
+
+// the solver's per-particle buffers for n particles (allocated once)
+void ensure_buffers(reyn_solver& sv, uint32_t n);
+
+// bytes of one scene's (or one sweep's) convergence sums, an upper bound
+constexpr size_t SWEEP_STATS_BYTES = 64;
 
 void kernel_eval(int kind, float h_bar, const float* dx, const float* dy,
     const float* dz, uint32_t n, float* w, float* gx, float* gy, float* gz,

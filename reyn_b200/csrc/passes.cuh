@@ -431,12 +431,21 @@ __device__ __forceinline__ void scene_accumulate(SweepStats* st, uint32_t s, boo
 // its criterion stops iterating; n_active counts the scenes that go on.
 // mode 0: PCISPH average density (PCISPH.cu:101); 1: IISPH average error;
 // 2: IISPH any particle above eta rho0 (IISPH.cu:246)
+// In a captured step the sweep count lives on the device (iter_dev: sweeps
+// finished before this one) and the kernel does nothing before min_iter, as
+// the host loop does not call it then.
 __global__ void k_scene_converge(uint32_t ns, const SweepStats* __restrict__ st,
     const uint32_t* __restrict__ first, int mode, float eta, float rho0, uint32_t iter,
     uint8_t* __restrict__ active, uint32_t* __restrict__ iters_out,
-    float* __restrict__ avg_err, float* __restrict__ max_err, uint32_t* __restrict__ n_active)
+    float* __restrict__ avg_err, float* __restrict__ max_err, uint32_t* __restrict__ n_active,
+    const uint32_t* __restrict__ iter_dev, uint32_t min_iter, uint32_t max_iter)
 {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (iter_dev) {
+        iter = *iter_dev + 1;
+        if (iter < min_iter && !(max_iter && iter >= max_iter))
+            return;
+    }
     if (s >= ns || !active[s])
         return;
     const uint32_t cnt = first[s + 1] - first[s];
@@ -458,6 +467,66 @@ __global__ void k_scene_converge(uint32_t ns, const SweepStats* __restrict__ st,
         active[s] = 0;
     else
         atomicAdd(n_active, 1u);
+}
+
+// ---- captured steps: the iteration decision on the device ------------------
+// After each sweep of a captured step: counts the sweep, applies the host
+// loop's stopping rule (min_iter, max_iter, the scheme's criterion on this
+// sweep's sums, or for a batch whether any scene goes on), records the step
+// statistics and sets the while node's condition and the pressure-pass gate.
+// scheme: REYN_PCISPH or REYN_IISPH; conv_any: IISPH's any-particle rule.
+__global__ void k_graph_decide(int scheme, int conv_any, const SweepStats* __restrict__ slot,
+    uint32_t n, float eta, float rho0, uint32_t min_iter, uint32_t max_iter,
+    const uint32_t* __restrict__ n_active, GraphStats* gs, uint32_t* gate,
+    cudaGraphConditionalHandle h)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    const uint32_t it = gs->iters + 1;
+    gs->iters = it;
+    const bool last = max_iter && it >= max_iter;
+    bool go;
+    if (it < min_iter && !last) {
+        go = true;
+    } else if (n_active) { // a batch (IISPH.cu / PCISPH.cu loops per scene)
+        const bool any = *n_active > 0;
+        go = any && !last;
+        if (any && last)
+            gs->unconverged = 1;
+    } else if (scheme == REYN_IISPH) {
+        const SweepStats t = *slot;
+        gs->avg_err = t.err_sum / n / rho0;
+        gs->max_err = t.err_max / rho0;
+        const bool more = conv_any ? t.over > 0 : t.err_sum / n > (double)eta * rho0;
+        go = more && !last;
+        if (more && last)
+            gs->unconverged = 1;
+    } else { // PCISPH (PCISPH.cu:95-102)
+        const SweepStats t = *slot;
+        const float avg = (float)(t.rho_sum / n);
+        if (last) {
+            if (it >= min_iter && !(avg <= (eta + 1.f) * rho0))
+                gs->unconverged = 1;
+            go = false;
+        } else {
+            gs->avg_err = fmax(0.0, t.rho_sum / n / rho0 - 1.0);
+            go = avg > (eta + 1.f) * rho0;
+        }
+    }
+    if (gate)
+        *gate = go ? 1u : 0u;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+}
+
+// a captured SESPH step: one pass, for the statistics and every scene
+__global__ void k_graph_single_pass(GraphStats* gs, uint32_t* __restrict__ scene_iters,
+    uint32_t ns)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0)
+        gs->iters = 1;
+    if (s < ns)
+        scene_iters[s] = 1;
 }
 
 // ---- step tail ---------------------------------------------------------------
@@ -887,10 +956,12 @@ __global__ void __launch_bounds__(MB) k_iisph_diag_pacc(uint32_t n, Fluid f,
 template <int KIND, int R, int MIX = 0, bool BATCH = false, int MB = NBR_THREADS>
 __global__ void __launch_bounds__(MB) k_iisph_pacc(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
-    float4* __restrict__ acc, uint2* __restrict__ acch_out)
+    float4* __restrict__ acc, uint2* __restrict__ acch_out, const uint32_t* __restrict__ gate)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
+    // a captured step's loop body: the first sweep uses the accelerations of
+    // the pass before the loop
+    if (i >= n || (gate && !*gate))
         return;
     if constexpr (BATCH) {
         if (!scene_live(f, scene_of(f.g, i)))
@@ -1047,8 +1118,6 @@ template <class F> void dispatch(int kind, int range, F&& f)
 } // namespace
 
 double pcisph_template_delta(int kind, float h);
-void ensure_buffers(reyn_solver& sv, uint32_t n);
-
 template <int MB>
 void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     const reyn_boundary* bdy, float dt, cudaStream_t s, const float* bmin, const float* bmax)
@@ -1079,6 +1148,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         sv.p_epoch = st.epoch;
     }
     sv.stats = reyn_step_stats {};
+    GraphCtx* const gx = sv.graph; // non-null: this step is being captured
     const uint32_t ns = grid.n_scenes;
     require(!bdy || !bdy->nb || bdy->grid.n_scenes == ns,
         "batched grids need a boundary batched over the same scenes");
@@ -1094,8 +1164,9 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         sv.n_active.resize(1);
         if (!sv.n_active_host)
             sv.n_active_host = std::make_unique<PinnedArray<uint32_t>>(1);
-        REYN_CUDA(cudaMemcpyAsync(sv.scene_first.get(), grid.first.data(),
-            (ns + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        if (!gx) // a capture uploads the offsets before it starts
+            REYN_CUDA(cudaMemcpyAsync(sv.scene_first.get(), grid.first.data(),
+                (ns + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
         REYN_CUDA(cudaMemsetAsync(sv.scene_active.get(), 1, ns, s));
         sv.scene_iters.zero(s);
         sv.scene_avg.zero(s);
@@ -1169,11 +1240,56 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         REYN_KERNEL("k_scene_converge", s,
             k_scene_converge<<<blocks_for(ns, THREADS), THREADS, 0, s>>>(ns, scene_slot,
             sv.scene_first.get(), mode, P.eta, rho0, iters, sv.scene_active.get(),
-            sv.scene_iters.get(), sv.scene_avg.get(), sv.scene_max.get(), sv.n_active.get()));
+            sv.scene_iters.get(), sv.scene_avg.get(), sv.scene_max.get(), sv.n_active.get(),
+            nullptr, 0, 0));
         REYN_CUDA(cudaMemcpyAsync(sv.n_active_host->get(), sv.n_active.get(), sizeof(uint32_t),
             cudaMemcpyDeviceToHost, s));
         REYN_CUDA(cudaStreamSynchronize(s));
         return *sv.n_active_host->get() > 0;
+    };
+    // a captured step's sweep loop: a while node after the work captured so
+    // far on s; `sweep(stream, handle)` enqueues one sweep and its decision
+    // on the body stream
+    auto graph_loop = [&](auto&& sweep) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        REYN_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd));
+        require(cs == cudaStreamCaptureStatusActive, "no capture in progress");
+        cudaGraphConditionalHandle h;
+        REYN_CUDA(cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        REYN_CUDA(cudaGraphAddNode(&node, cg, deps, nd, &cp));
+        REYN_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1,
+            cudaStreamSetCaptureDependencies));
+        const cudaStream_t bst = gx->body;
+        REYN_CUDA(cudaStreamBeginCaptureToGraph(bst, cp.conditional.phGraph_out[0], nullptr,
+            nullptr, 0, cudaStreamCaptureModeRelaxed));
+        profile_record(&gx->body_names);
+        sweep(bst, h);
+        profile_record(&gx->top_names);
+        cudaGraph_t body_out = nullptr;
+        REYN_CUDA(cudaStreamEndCapture(bst, &body_out));
+    };
+    auto decide = [&](cudaStream_t q, cudaGraphConditionalHandle h, const SweepStats* slot) {
+        REYN_KERNEL("k_graph_decide", q,
+            k_graph_decide<<<1, 32, 0, q>>>(int(sv.scheme), P.convergence != REYN_CONV_AVERAGE,
+            slot, n, P.eta, rho0, P.min_iter, P.max_iter, ns ? sv.n_active.get() : nullptr,
+            gx->stats, sv.scheme == REYN_IISPH ? gx->gate : nullptr, h));
+    };
+    auto scene_converge_dev = [&](cudaStream_t q, int mode) {
+        REYN_CUDA(cudaMemsetAsync(sv.n_active.get(), 0, sizeof(uint32_t), q));
+        REYN_KERNEL("k_scene_converge", q,
+            k_scene_converge<<<blocks_for(ns, THREADS), THREADS, 0, q>>>(ns, scene_slot,
+            sv.scene_first.get(), mode, P.eta, rho0, 0, sv.scene_active.get(),
+            sv.scene_iters.get(), sv.scene_avg.get(), sv.scene_max.get(), sv.n_active.get(),
+            &gx->stats->iters, P.min_iter, P.max_iter));
     };
 
     const bool mixed = P.precision != REYN_PRECISION_FP32;
@@ -1196,7 +1312,11 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 k_sesph<K, R, B, MB><<<nb, bs, 0, s>>>(n, f, st.vel.get(), sv.bterm.get(),
                 P.k_sesph, rho0, nu10, eps, grav, dt, sv.acc.get(), X, Y, Z, VX, VY, VZ, tail));
             iters = 1;
-            if (ns) { // one pass per scene
+            if (gx) {
+                REYN_KERNEL("k_graph_single_pass", s,
+                    k_graph_single_pass<<<blocks_for(std::max<uint32_t>(ns, 1), THREADS), THREADS,
+                    0, s>>>(gx->stats, ns ? sv.scene_iters.get() : nullptr, ns));
+            } else if (ns) { // one pass per scene
                 const std::vector<uint32_t> ones(ns, 1u);
                 REYN_CUDA(cudaMemcpyAsync(sv.scene_iters.get(), ones.data(), ns * sizeof(uint32_t),
                     cudaMemcpyHostToDevice, s));
@@ -1208,7 +1328,22 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 k_nonpressure<K, R, 0, B, MB><<<nb, bs, 0, s>>>(n, f, st.vel.get(), nullptr, nu10,
                 eps, grav, dt, sv.acc.get(), sv.vel2.get(), nullptr));
             float4* v = sv.vel2.get();
-            for (;;) {
+            if (gx) {
+                graph_loop([&](cudaStream_t q, cudaGraphConditionalHandle h) {
+                    SweepStats* slot = ns ? scene_slot : slots;
+                    REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), q));
+                    REYN_KERNEL("k_pcisph_predict", q,
+                        k_pcisph_predict<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, v, sv.bterm.get(), dt,
+                        sv.rho.get(), kp, rho0, sv.p.get(), slot));
+                    REYN_KERNEL("k_pcisph_pressure", q,
+                        k_pcisph_pressure<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, sv.rho.get(),
+                        sv.p.get(), sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
+                    if (ns)
+                        scene_converge_dev(q, 0);
+                    decide(q, h, slot);
+                });
+            }
+            for (; !gx;) {
                 SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
                 REYN_KERNEL("k_pcisph_predict", s,
@@ -1256,7 +1391,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             auto pacc = [&] {
                 REYN_KERNEL("k_iisph_pacc", s,
                     k_iisph_pacc<K, R, MIX, B, MB><<<nb, bs, 0, s>>>(n, f, sv.p.get(),
-                    sv.bterm.get(), r0i, sv.acc.get(), ACH));
+                    sv.bterm.get(), r0i, sv.acc.get(), ACH, nullptr));
             };
             if (P.warmstart) {
                 REYN_KERNEL("k_iisph_diag_pacc", s,
@@ -1272,9 +1407,28 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 pacc();
             }
             const float thr = P.eta * rho0;
+            if (gx) {
+                // the loop body: [gated pressure accelerations, Jacobi update,
+                // decision]; the gate is closed for the first sweep
+                REYN_CUDA(cudaMemsetAsync(gx->gate, 0, sizeof(uint32_t), s));
+                graph_loop([&](cudaStream_t q, cudaGraphConditionalHandle h) {
+                    SweepStats* slot = ns ? scene_slot : slots;
+                    REYN_KERNEL("k_iisph_pacc", q,
+                        k_iisph_pacc<K, R, MIX, B, MB><<<nb, bs, 0, q>>>(n, f, sv.p.get(),
+                        sv.bterm.get(), r0i, sv.acc.get(), ACH, gx->gate));
+                    REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), q));
+                    REYN_KERNEL("k_iisph_jacobi", q,
+                        k_iisph_jacobi<K, R, MIX, B, MB><<<nb, bs, 0, q>>>(n, f, sv.acc.get(),
+                        sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, tiny,
+                        thr, slot));
+                    if (ns)
+                        scene_converge_dev(q, P.convergence == REYN_CONV_AVERAGE ? 1 : 2);
+                    decide(q, h, slot);
+                });
+            }
             // IISPH.cu:219-250: [pressure accelerations, Jacobi update]* with
             // the first accelerations computed above
-            for (;;) {
+            for (; !gx;) {
                 SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
                 REYN_KERNEL("k_iisph_jacobi", s,
@@ -1332,9 +1486,11 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     st.packed_valid = false; // positions moved: the packed copy is stale
     st.version += 1;
     if (tail.vmax) {
-        REYN_CUDA(cudaMemcpyAsync(sv.vmax_host->get(), tail.vmax, sizeof(float),
-            cudaMemcpyDeviceToHost, s));
-        REYN_CUDA(cudaEventRecord(sv.vmax_ready, s));
+        if (!gx) { // a captured step records these after each launch
+            REYN_CUDA(cudaMemcpyAsync(sv.vmax_host->get(), tail.vmax, sizeof(float),
+                cudaMemcpyDeviceToHost, s));
+            REYN_CUDA(cudaEventRecord(sv.vmax_ready, s));
+        }
         sv.vmax_state = &st;
         sv.vmax_version = st.version;
         sv.vmax_valid = true;

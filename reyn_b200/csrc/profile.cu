@@ -73,12 +73,19 @@ Registry& reg()
 }
 
 thread_local int t_open = -1; // index into pending of the open scope
+thread_local std::vector<const char*>* t_sink = nullptr; // capture: names only
 
 } // namespace
+
+void profile_record(std::vector<const char*>* sink) { t_sink = sink; }
 
 ProfScope::ProfScope(const char* name, cudaStream_t s)
     : s_(s)
 {
+    if (t_sink) { // captured into a graph: the replay counts it
+        t_sink->push_back(name);
+        return;
+    }
     Registry& r = reg();
     std::lock_guard<std::mutex> lock(r.mu);
     const int k = r.id(name);
@@ -99,6 +106,17 @@ ProfScope::~ProfScope()
     std::lock_guard<std::mutex> lock(r.mu);
     if (slot_ < (int)r.pending.size())
         cudaEventRecord(r.pending[slot_].b, s_);
+}
+
+// counts `times` launches of each named kernel (graph replays)
+void profile_count(const std::vector<const char*>& names, uint64_t times)
+{
+    if (!times)
+        return;
+    Registry& r = reg();
+    std::lock_guard<std::mutex> lock(r.mu);
+    for (const char* n : names)
+        r.launches[r.id(n)] += times;
 }
 
 } // namespace reyn
