@@ -627,6 +627,7 @@ def run_batched(a, world, rank, local):
         step()
     its.clear()
     torch.cuda.synchronize()
+    start = st.download()  # the graph leg starts from the same state
     gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
     clocks = ClockSampler(gpu_uuid)
     time.sleep(0.3)
@@ -648,6 +649,33 @@ def run_batched(a, world, rank, local):
     ms = max_over_ranks(world, e0.elapsed_time(e1))
     value = world * n * a.steps / (ms / 1e3)
     it = np.array(its)
+
+    # the same steps from the same state as CUDA-graph replays: one launch per
+    # step, the pressure loop in a device-side while node, no host round trip
+    st.upload(start)
+    torch.cuda.synchronize()
+    graph = rb.StepGraph(sv, st, grid, bd, BATCH_DT, bounds=((0, 0, 0), (0, 0, 0)))
+    for _ in range(a.warmup):
+        graph.launch(stream=S)
+    graph.stats(stream=S)
+    st.upload(start)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0.record(stream)
+    for _ in range(a.steps):
+        graph.launch(stream=S)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    gms = max_over_ranks(world, e0.elapsed_time(e1))
+    g_last = graph.stats(stream=S)
+    g_step_k, g_sweep_k = graph.info()
+    graph_leg = {"value": round(world * n * a.steps / (gms / 1e3), 1), "unit": UNIT,
+                 "ms_per_step": round(gms / a.steps, 3),
+                 "kernels_per_step": g_step_k, "kernels_per_sweep": g_sweep_k,
+                 "last_step_sweeps": g_last.iters,
+                 "note": "same scenes, state and dt; graph launches back to back"}
+    graph.close()
     for o in (sv, grid, bd, st):
         o.close()
 
@@ -708,6 +736,8 @@ def run_batched(a, world, rank, local):
         "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in
                     sorted(prof.items(), key=lambda kv: -kv[1][1])},
         "sequential": seq,
+        "graph": graph_leg,
+        "graph_over_plain": round(graph_leg["value"] / value, 3),
     }
     if seq:
         out["batched_over_sequential"] = round(value / seq["value"], 3)

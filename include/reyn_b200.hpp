@@ -159,6 +159,8 @@ public:
         return i;
     }
 
+    reyn_grid* handle() { return g_; }
+
 private:
     reyn_grid* g_ = nullptr;
 };
@@ -244,6 +246,7 @@ namespace detail {
             check(reyn_solver_stats(s_, &t));
             return t;
         }
+        reyn_solver* handle() { return s_; }
 
     private:
         reyn_solver* s_ = nullptr;
@@ -361,6 +364,35 @@ inline void hard_enforce_bounds(Particles& state, float3 bound_min, float3 bound
     const float hi[3] = { bound_max.x, bound_max.y, bound_max.z };
     check(reyn_enforce_bounds(state.handle(), lo, hi, s));
 }
+
+// ---- captured steps (no counterpart in the reference) --------------------------
+// the loop body `construct_and_reorder(2h, state); step(...); hard bounds` at a
+// fixed dt as CUDA graphs (reyn_step_graph_*): launch() replays one step
+class StepGraph {
+public:
+    StepGraph(detail::Solver& solver, Particles& state, UniformGridBuilder& builder,
+        const BoundarySamples* bdy, float dt, float3 bound_min, float3 bound_max)
+    {
+        const float lo[3] = { bound_min.x, bound_min.y, bound_min.z };
+        const float hi[3] = { bound_max.x, bound_max.y, bound_max.z };
+        check(reyn_step_graph_create(solver.handle(), state.handle(), builder.handle(),
+            bdy ? bdy->handle() : nullptr, dt, lo, hi, &g_));
+    }
+    ~StepGraph() { reyn_step_graph_destroy(g_); }
+    StepGraph(const StepGraph&) = delete;
+    StepGraph& operator=(const StepGraph&) = delete;
+    void launch(cudaStream_t s = nullptr) { check(reyn_step_graph_launch(g_, s)); }
+    // sweeps of the last launched step, as IISPH::step / PCISPH::step return
+    uint32_t iterations(cudaStream_t s = nullptr)
+    {
+        reyn_step_stats t {};
+        check(reyn_step_graph_stats(g_, &t, s));
+        return t.iters;
+    }
+
+private:
+    reyn_step_graph* g_ = nullptr;
+};
 
 // ---- meshes (loader.h:11-20, sample_boundary.cuh:13-163, lbvh.cuh:614-760) --
 // Mesh: the reference's host mesh, double vertex components and uint3 faces

@@ -3,7 +3,9 @@
 // reorder (the particle ID carried as an extra array), IISPH step, hard
 // bounds. Reads a scene from argv[1], writes the final state to argv[2].
 // With a third argument "fused" the loop uses the fused tail (next_dt and
-// step_bounded in place of simple_dt_controller, step and hard_enforce_bounds).
+// step_bounded in place of simple_dt_controller, step and hard_enforce_bounds);
+// "fixed" keeps dt fixed (no controller; the id array is not reordered) and
+// "graph" runs that fixed-dt loop as replays of a StepGraph.
 //
 // input  (little-endian): u32 N, u32 Nb, u32 steps, f32 h, rho0, nu, dt0,
 //        lambda, box_min[3], box_max[3], then N floats each of x y z vx vy vz
@@ -24,7 +26,8 @@ int main(int argc, char** argv)
         std::fprintf(stderr, "usage: main_loop in.bin out.bin [fused]\n");
         return 2;
     }
-    const bool fused = argc == 4 && std::string(argv[3]) == "fused";
+    const std::string mode = argc == 4 ? std::string(argv[3]) : std::string();
+    const bool fused = mode == "fused";
     FILE* f = std::fopen(argv[1], "rb");
     if (!f)
         return 2;
@@ -63,8 +66,19 @@ int main(int argc, char** argv)
         std::vector<uint32_t> iters_log;
         std::vector<float> dt_log;
         uint32_t iters = 0;
-        for (uint32_t s = 0; s < steps; ++s) {
-            if (fused) {
+        if (mode == "graph") {
+            StepGraph graph(solver, state, builder, &bdy, dt, bmin, bmax);
+            for (uint32_t s = 0; s < steps; ++s) {
+                graph.launch();
+                iters_log.push_back(graph.iterations());
+                dt_log.push_back(dt);
+            }
+        }
+        for (uint32_t s = 0; s < steps && mode != "graph"; ++s) {
+            if (mode == "fixed") {
+                const auto grid { builder.construct_and_reorder(2.f * h, state) };
+                iters = solver.step_bounded(state, grid, bdy, dt, bmin, bmax);
+            } else if (fused) {
                 dt = solver.next_dt(state, iters, dt, lambda, h, g, 10, 0.001f);
                 const auto grid { builder.construct_and_reorder(2.f * h, state, d_id) };
                 iters = solver.step_bounded(state, grid, bdy, dt, bmin, bmax);

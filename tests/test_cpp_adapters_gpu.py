@@ -105,6 +105,25 @@ def test_cpp_main_loop_fused_tail_is_bit_identical(cuda, tmp_path):
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
 
 
+def test_cpp_step_graph_is_bit_identical(cuda, tmp_path):
+    """The fixed-dt loop as StepGraph replays reproduces the plain calls bit
+    for bit, with the same sweep counts."""
+    exe = compile_main_loop(str(tmp_path))
+    sc = scenes.dam_break((14, 12, 10), 0.02, (0.5, 0.5, 0.5), velocity_noise=0.02, seed=23)
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    inp = os.path.join(str(tmp_path), "in.bin")
+    write_scene(inp, sc, bm, 4, 1e-3, 0.4, 0.01)
+    res = []
+    for mode in ("fixed", "graph"):
+        out = os.path.join(str(tmp_path), f"out_{mode}.bin")
+        subprocess.run([exe, inp, out, mode], check=True)
+        res.append(read_out(out, sc.n))
+    (ia, _, a), (ib, _, b) = res
+    assert list(ia) == list(ib) and min(ia) >= 3
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+
+
 def test_cpp_mesh_adapters(cuda, tmp_path):
     """DeviceMesh / uniform_sample_mesh / relax_sampling / LBVH::project /
     BoundarySamples in the reference's calling pattern (tests/cpp/mesh_adapter.cpp)"""
