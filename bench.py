@@ -849,6 +849,20 @@ def run_column(a, world, rank, local):
         obj.close()
 
 
+def mesh_traffic(n_queries: int):
+    """DRAM bytes of one k_mesh_query launch over n queries, from the
+    committed ncu summary (profiles/k_mesh_query_mesh_lbvh.txt, captured at
+    2M queries; the traffic grows with the query count)."""
+    path = os.path.join(ROOT, "profiles", "k_mesh_query_mesh_lbvh.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_query:"):
+                return float(line.split(":", 1)[1].split()[0]) * n_queries
+    except OSError:
+        pass
+    return None
+
+
 def mesh_workload(scale: int = 1):
     """A closed 327,680-face mesh: a level-7 icosphere of radius 1 with its
     vertices moved by a seeded uniform +-0.001 (a generic surface: no
@@ -923,7 +937,7 @@ def run_mesh(a, world, rank, local):
             "achieved": round(algo / (k_ms / 1e3) / 1e9, 1) if k_ms else None,
             "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
             "frac": round(algo / (k_ms / 1e3) / 1e9 / peak, 4) if k_ms else None,
-            "traffic": None, "bytes_per_query": 24,
+            "traffic": mesh_traffic(n), "bytes_per_query": 24,
             "note": "a latency-bound stack traversal: ~log2(F) dependent 64-byte node loads "
                     "per query from the L2-resident tree"}
     # end to end through the public call with host buffers: pinned upload,
