@@ -264,7 +264,9 @@ typedef struct reyn_params {
     float k_sesph;          /* SESPH stiffness (SESPH.cuh:50: 500) */
     float eta;              /* tolerance (PCISPH 0.001, IISPH 0.005) */
     uint32_t min_iter;      /* 3 (PCISPH.cuh:38, IISPH.cuh:43) */
-    uint32_t max_iter;      /* 0 = unbounded, as the reference */
+    uint32_t max_iter;      /* 0 = unbounded, as the reference (a safety bound of
+                             * 100000 sweeps still ends a step that cannot
+                             * converge, with REYN_ERR_ITER_LIMIT) */
     float omega;            /* IISPH Jacobi weight (0.5, IISPH.cuh:45) */
     int32_t warmstart;      /* IISPH p *= 0.5 (IISPH.cuh:48) */
     reyn_convergence convergence;

@@ -1123,6 +1123,11 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     const reyn_boundary* bdy, float dt, cudaStream_t s, const float* bmin, const float* bmax)
 {
     const reyn_params& P = sv.prm;
+    // max_iter 0 is unbounded as in the reference; a hard bound still ends a
+    // loop that cannot converge (a non-finite state), far above any sweep
+    // count a converging step needs
+    constexpr uint32_t SWEEP_SAFETY_LIMIT = 100000;
+    const uint32_t max_it = P.max_iter ? P.max_iter : SWEEP_SAFETY_LIMIT;
     const uint32_t n = st.n;
     sv.vmax_valid = false;
     require(n == sv.n, "particle count differs from the solver's");
@@ -1280,7 +1285,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     auto decide = [&](cudaStream_t q, cudaGraphConditionalHandle h, const SweepStats* slot) {
         REYN_KERNEL("k_graph_decide", q,
             k_graph_decide<<<1, 32, 0, q>>>(int(sv.scheme), P.convergence != REYN_CONV_AVERAGE,
-            slot, n, P.eta, rho0, P.min_iter, P.max_iter, ns ? sv.n_active.get() : nullptr,
+            slot, n, P.eta, rho0, P.min_iter, max_it, ns ? sv.n_active.get() : nullptr,
             gx->stats, sv.scheme == REYN_IISPH ? gx->gate : nullptr, h));
     };
     auto scene_converge_dev = [&](cudaStream_t q, int mode) {
@@ -1289,7 +1294,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             k_scene_converge<<<blocks_for(ns, THREADS), THREADS, 0, q>>>(ns, scene_slot,
             sv.scene_first.get(), mode, P.eta, rho0, 0, sv.scene_active.get(),
             sv.scene_iters.get(), sv.scene_avg.get(), sv.scene_max.get(), sv.n_active.get(),
-            &gx->stats->iters, P.min_iter, P.max_iter));
+            &gx->stats->iters, P.min_iter, max_it));
     };
 
     const bool mixed = P.precision != REYN_PRECISION_FP32;
@@ -1354,7 +1359,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                     sv.p.get(), sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
                 iters += 1;
                 if (ns) {
-                    const bool last = P.max_iter && iters >= P.max_iter;
+                    const bool last = max_it && iters >= max_it;
                     if (iters < P.min_iter && !last)
                         continue;
                     if (!scenes_go_on(0))
@@ -1365,7 +1370,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                     }
                     continue;
                 }
-                if (P.max_iter && iters >= P.max_iter) {
+                if (max_it && iters >= max_it) {
                     if (iters >= P.min_iter) {
                         readback(slot);
                         converged = (float)(host.rho_sum / n) <= (P.eta + 1.f) * rho0;
@@ -1436,7 +1441,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                     sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, tiny,
                     thr, slot));
                 iters += 1;
-                const bool last = P.max_iter && iters >= P.max_iter;
+                const bool last = max_it && iters >= max_it;
                 if (iters < P.min_iter && !last) {
                     pacc();
                     continue;
