@@ -140,19 +140,24 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(kernel: str, precision: str):
-    """DRAM bytes per launch of `kernel` on this workload, from the committed
-    ncu summary (profiles/<kernel>_iisph_4m[_mixed].txt, line
-    'traffic_bytes_per_launch:')."""
+def profile_field(kernel: str, precision: str, key: str):
+    """A numeric field of the committed ncu summary of `kernel` on this
+    workload (profiles/<kernel>_iisph_4m[_mixed].txt, line '<key>: value')."""
     suffix = "" if precision == "fp32" else "_" + precision
     path = os.path.join(ROOT, "profiles", f"{kernel}_iisph_4m{suffix}.txt")
     try:
         for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":", 1)[1])
-    except OSError:
+            if line.startswith(key + ":"):
+                return float(line.split(":", 1)[1].split()[0])
+    except (OSError, ValueError):
         pass
     return None
+
+
+def profile_traffic(kernel: str, precision: str):
+    """DRAM bytes per launch of `kernel` on this workload, from its committed
+    ncu summary (line 'traffic_bytes_per_launch:')."""
+    return profile_field(kernel, precision, "traffic_bytes_per_launch")
 
 
 class ClockSampler:
@@ -401,6 +406,9 @@ def run_engine(a, world, rank, local):
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": profile_traffic(dom_name, headline), "peak_source": peak_kind,
+                # the unit these passes are bound by (ncu, committed summary)
+                "l1tex_throughput_pct": profile_field(dom_name, headline,
+                                                      "l1tex_throughput_pct"),
                 "alg_bytes_per_launch": alg, "ms_per_launch": round(per_launch_s * 1e3, 4),
                 "share_of_step": round(dom_ms / ms, 4)}
     kernels = {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in
