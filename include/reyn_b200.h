@@ -534,7 +534,9 @@ int reyn_mesh_sample_uniform(const reyn_mesh* mesh, float h, float oversampling,
  * previous positions of all samples. The samples keep their order. stats
  * (host, may be NULL) receives per sweep the max/min number-density ratio and
  * the average number density; num_den (device, may be NULL) the number
- * densities of the last sweep. Synchronises the stream. */
+ * densities of the last sweep. The mesh keeps the relaxation's grid (cell
+ * 2 h_bdy over its box) and scratch for the next call until it is
+ * destroyed. Synchronises the stream. */
 int reyn_mesh_relax(const reyn_mesh* mesh, float* x, float* y, float* z,
     uint32_t n, float h_bdy, float relaxation_factor, uint32_t iters,
     float* stats, float* num_den, void* stream);

@@ -1006,6 +1006,13 @@ struct reyn_mesh {
     Box root {};
     uint32_t height = 0;
     mutable QueryScratch query;
+    // the relaxation's uniform grid (rebuilt for another spacing) and its
+    // scratch, kept for the next call: a surface's grid spans the mesh's box
+    // at cell 2 h_bdy and can take a gigabyte, whose allocation would
+    // otherwise dominate a call
+    mutable std::unique_ptr<Grid> relax_grid;
+    mutable float relax_r = 0.f;
+    mutable DevArray<unsigned char> relax_tmp;
 
     void allocate()
     {
@@ -1423,15 +1430,21 @@ extern "C" int reyn_mesh_relax(const reyn_mesh* mesh, float* x, float* y, float*
         const cudaStream_t s = as_stream(stream);
         // a grid of cell 2 h_bdy over the mesh bounds: projected samples lie
         // inside them, and the grid adds its own 2r margin
-        Grid g;
-        float bmin[3], bmax[3];
-        for (int k = 0; k < 3; ++k) {
-            bmin[k] = float(mesh->lo[k]);
-            bmax[k] = float(mesh->hi[k]);
+        if (!mesh->relax_grid || mesh->relax_r != 2.f * h_bdy) {
+            auto ng = std::make_unique<Grid>();
+            float bmin[3], bmax[3];
+            for (int k = 0; k < 3; ++k) {
+                bmin[k] = float(mesh->lo[k]);
+                bmax[k] = float(mesh->hi[k]);
+            }
+            ng->geom = make_geom(bmin, bmax, 2.f * h_bdy, 1.0f);
+            ng->ratio = 1.0f;
+            require(ng->geom.range == 1, "unexpected relaxation grid range");
+            mesh->relax_grid.reset(); // the old grid's memory first
+            mesh->relax_grid = std::move(ng);
+            mesh->relax_r = 2.f * h_bdy;
         }
-        g.geom = make_geom(bmin, bmax, 2.f * h_bdy, 1.0f);
-        g.ratio = 1.0f;
-        require(g.geom.range == 1, "unexpected relaxation grid range");
+        Grid& g = *mesh->relax_grid;
         const KernelConst kc = make_kernel(K_B3, 2.f * h_bdy);
         const float rho0 = hex_plane_density(h_bdy);
         const float inv2 = 1.f / (rho0 * rho0);
@@ -1440,7 +1453,8 @@ extern "C" int reyn_mesh_relax(const reyn_mesh* mesh, float* x, float* y, float*
         const size_t o_pts = c.add<float4>(n), o_mv = c.add<float4>(n), o_nd = c.add<float>(n);
         const size_t o_mm = c.add<unsigned>(2 * size_t(iters)), o_sum = c.add<double>(iters);
         const size_t o_st = c.add<uint32_t>(1);
-        DevArray<unsigned char> tmp(c.bytes);
+        DevArray<unsigned char>& tmp = mesh->relax_tmp;
+        tmp.resize(c.bytes);
         float4* pts = at<float4>(tmp, o_pts);
         float4* moved = at<float4>(tmp, o_mv);
         float* nd = at<float>(tmp, o_nd);
