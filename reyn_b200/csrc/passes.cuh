@@ -1157,7 +1157,6 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     const uint32_t ns = grid.n_scenes;
     require(!bdy || !bdy->nb || bdy->grid.n_scenes == ns,
         "batched grids need a boundary batched over the same scenes");
-    require(!ns || P.precision == REYN_PRECISION_FP32, "batched scenes run in FP32");
     sv.n_scenes = ns;
     if (ns) {
         sv.scene_stats.resize(size_t(ns) * sizeof(SweepStats));
@@ -1476,7 +1475,14 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         }
     };
     dispatch(P.kernel, grid.geom.range, [&](auto KC, auto RC) {
-        if (ns) // batched scenes: FP32
+        // batched scenes: the records of the mixed modes use each scene's own
+        // grid origin (the cell size is shared), and neighbours never cross
+        // scenes, so every mode runs batched
+        if (ns && P.precision == REYN_PRECISION_MIXED_POS16)
+            body(KC, RC, std::integral_constant<int, MIX_POS16> {}, std::true_type {});
+        else if (ns && mixed)
+            body(KC, RC, std::integral_constant<int, MIX_F16> {}, std::true_type {});
+        else if (ns)
             body(KC, RC, std::integral_constant<int, 0> {}, std::true_type {});
         else if (P.precision == REYN_PRECISION_MIXED_POS16)
             body(KC, RC, std::integral_constant<int, MIX_POS16> {}, std::false_type {});

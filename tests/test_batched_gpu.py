@@ -18,14 +18,15 @@ def _small_batch(seed=11):
     return scenes.batched_dam_breaks(counts, 0.02, seed=seed)
 
 
-def _params(rb, scheme, kind, h):
+def _params(rb, scheme, kind, h, precision=0):
     prm = rb.reference_params(scheme, kind, h, 1000.0, 0.01)
     if scheme == rb.SESPH:
         prm.k_sesph = 1000.0
+    prm.precision = precision
     return prm
 
 
-def _run_batched(batch, scheme, kind, steps, dt):
+def _run_batched(batch, scheme, kind, steps, dt, precision=0):
     import torch
 
     import reyn_b200 as rb
@@ -38,7 +39,7 @@ def _run_batched(batch, scheme, kind, steps, dt):
                      h=batch.h, rho0=batch.rho0, scene_first=batch.bfirst)
     grid = rb.Grid(batch.frame_min, batch.frame_max, 2 * batch.h, 0.5, 0,
                    scene_first=batch.first, scene_min=batch.box_min, scene_max=batch.box_max)
-    sv = rb.Solver(scheme, _params(rb, scheme, kind, batch.h), n)
+    sv = rb.Solver(scheme, _params(rb, scheme, kind, batch.h, precision), n)
     its = []
     for _ in range(steps):
         grid.construct_and_reorder(st, [ids])
@@ -53,7 +54,7 @@ def _run_batched(batch, scheme, kind, steps, dt):
     return out, np.array(its)
 
 
-def _run_alone(batch, s, scheme, kind, steps, dt):
+def _run_alone(batch, s, scheme, kind, steps, dt, precision=0):
     import torch
 
     import reyn_b200 as rb
@@ -67,7 +68,7 @@ def _run_alone(batch, s, scheme, kind, steps, dt):
     bd = rb.Boundary(*(torch.tensor(batch.bdy[k][c:d], device=dev) for k in ("x", "y", "z")),
                      None, h=batch.h, rho0=batch.rho0)
     grid = rb.Grid(batch.box_min[s], batch.box_max[s], 2 * batch.h)
-    sv = rb.Solver(scheme, _params(rb, scheme, kind, batch.h), b - a)
+    sv = rb.Solver(scheme, _params(rb, scheme, kind, batch.h, precision), b - a)
     its = []
     for _ in range(steps):
         grid.construct_and_reorder(st, [ids])
@@ -96,6 +97,24 @@ def test_batch_matches_scenes_alone(cuda, scheme, kind, steps, dt):
         want, wits = _run_alone(batch, s, scheme, kind, steps, dt)
         assert list(its[:, s]) == list(wits), (s, its[:, s], wits)
         compare_steps(mine, want, scheme, tol, f"scene {s}")
+
+
+@pytest.mark.parametrize("precision", [1, 2])
+def test_mixed_precision_batch_matches_scenes_alone(cuda, precision):
+    """IISPH in MIXED (1) and MIXED_POS16 (2): each scene of the batch reads
+    the same 16-bit records as when stepped alone (its own grid origin, the
+    shared cell size and mass reference), so the per-scene results agree as
+    in FP32"""
+    batch = _small_batch()
+    steps, dt = 3, 1e-3
+    got, its = _run_batched(batch, 2, 0, steps, dt, precision)
+    tol = {k: (r * steps * 10, a * steps * 10) for k, (r, a) in STEP_TOL.items()}
+    for s in range(batch.n_scenes):
+        a, b = int(batch.first[s]), int(batch.first[s + 1])
+        mine = {k: v[a:b] for k, v in got.items()}
+        want, wits = _run_alone(batch, s, 2, 0, steps, dt, precision)
+        assert list(its[:, s]) == list(wits), (s, its[:, s], wits)
+        compare_steps(mine, want, 2, tol, f"scene {s}")
 
 
 def test_batched_scene_stats_and_errors(cuda):
