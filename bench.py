@@ -79,14 +79,17 @@ def parse_args():
                     help="all: time FP32 and mixed_pos16, then report the mixed path beside them")
     ap.add_argument("--order", choices=["xyz", "zorder"], default="xyz",
                     help="cell order of the grid the state is sorted by")
-    ap.add_argument("--workload", choices=["iisph_4m", "batched_pcisph", "column_16m",
-                                           "mesh_lbvh"],
+    ap.add_argument("--workload", choices=["iisph_4m", "batched_pcisph", "batched_iisph",
+                                           "column_16m", "mesh_lbvh"],
                     default="iisph_4m",
-                    help="batched_pcisph: 256 independent PCISPH scenes; column_16m: the "
+                    help="batched_pcisph: 256 independent PCISPH scenes; batched_iisph: "
+                         "about 4M particles of independent IISPH scenes in FP32 and the "
+                         "mixed modes; column_16m: the "
                          "16.7M-particle column collapse onto a sphere; mesh_lbvh: LBVH "
                          "closest-point queries and boundary sampling of a 327,680-face mesh "
                          "(none is the headline)")
-    ap.add_argument("--scenes", type=int, default=256, help="batched_pcisph: scene count")
+    ap.add_argument("--scenes", type=int, default=0,
+                    help="batched workloads: scene count (0: 256 for PCISPH, 96 for IISPH)")
     ap.add_argument("--no-sequential", action="store_true",
                     help="batched_pcisph: skip the scene-by-scene comparison run")
     ap.add_argument("--no-autotune", action="store_true",
@@ -603,7 +606,7 @@ def run_batched(a, world, rank, local):
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream(dev)
     S = stream.cuda_stream
-    b = scenes.batched_pcisph(n_scenes=a.scenes, seed=4 + rank)
+    b = scenes.batched_pcisph(n_scenes=a.scenes or 256, seed=4 + rank)
     n = int(b.first[-1])
 
     def params():
@@ -753,6 +756,127 @@ def run_batched(a, world, rank, local):
     }
     if seq:
         out["batched_over_sequential"] = round(value / seq["value"], 3)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_batched_iisph(a, world, rank, local):
+    """Batched IISPH: independent dam breaks (96 cubes of log-uniform particle
+    counts in [2000, 200000] at spacing 0.01, about 4M particles, Wendland C2
+    masses), 0.1 % average density error, fixed dt 2e-4. The same batch from
+    the same start is stepped in FP32, MIXED and MIXED_POS16 (one launch per
+    phase for all scenes); the fastest is the headline, and a CUDA-graph leg
+    replays its step."""
+    import torch
+
+    import reyn_b200 as rb
+    from reyn_b200 import scenes
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    S = stream.cuda_stream
+    ns = a.scenes or 96
+    counts = scenes.batch_counts(ns, 2000, 200000, 4 + rank)
+    b = scenes.batched_dam_breaks(counts, 0.01, seed=4 + rank, mass_kernel="C2")
+    n = int(b.first[-1])
+    st = rb.Particles(n, b.rho0)
+    st.upload(b.fluid)
+    bd = rb.Boundary(*(torch.tensor(b.bdy[k], device=dev) for k in ("x", "y", "z")), None,
+                     h=b.h, rho0=b.rho0, scene_first=b.bfirst)
+    grid = rb.Grid(b.frame_min, b.frame_max, 2 * b.h, 0.5, 0, scene_first=b.first,
+                   scene_min=b.box_min, scene_max=b.box_max)
+
+    def params(precision):
+        prm = rb.reference_params(rb.IISPH, rb.C2, b.h, b.rho0, NU)
+        prm.convergence = rb.CONV_AVERAGE
+        prm.eta = 0.001
+        prm.max_iter = 1000
+        prm.precision = precision
+        return prm
+
+    modes = (("fp32", rb.PRECISION_FP32), ("mixed", rb.PRECISION_MIXED),
+             ("mixed_pos16", rb.PRECISION_MIXED_POS16))
+    legs = {}
+    gpu_uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for name, prec in modes:
+        st.upload(b.fluid)
+        sv = rb.Solver(rb.IISPH, params(prec), n)
+        its = []
+
+        def step():
+            grid.construct_and_reorder(st, stream=S)
+            its.append(sv.step_batched(st, grid, bd, BATCH_DT, stream=S))
+
+        for _ in range(a.warmup):
+            step()
+        its.clear()
+        torch.cuda.synchronize()
+        clocks = ClockSampler(gpu_uuid)
+        time.sleep(0.3)
+        rb.profile_reset()
+        rb.profile_enable(True)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(a.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        rb.profile_enable(False)
+        prof = rb.profile_read()
+        ck = clocks.stop()
+        ms = max_over_ranks(world, e0.elapsed_time(e1))
+        it = np.array(its)
+        legs[name] = {"value": round(world * n * a.steps / (ms / 1e3), 1), "unit": UNIT,
+                      "ms_per_step": round(ms / a.steps, 3), "clocks": ck,
+                      "gpu_launches": sum(v[0] for v in prof.values()),
+                      "iters_per_step_max": it.max(1).tolist(),
+                      "iters_per_step_mean": [round(float(x), 2) for x in it.mean(1)],
+                      "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in
+                                  sorted(prof.items(), key=lambda kv: -kv[1][1])}}
+        sv.close()
+    head = max(legs, key=lambda k: legs[k]["value"])
+    # the headline mode's step as CUDA-graph replays, from the same start
+    st.upload(b.fluid)
+    sv = rb.Solver(rb.IISPH, params(dict(modes)[head]), n)
+    graph = rb.StepGraph(sv, st, grid, bd, BATCH_DT, bounds=((0, 0, 0), (0, 0, 0)))
+    for _ in range(a.warmup):
+        graph.launch(stream=S)
+    graph.stats(stream=S)
+    torch.cuda.synchronize()
+    barrier(world)
+    e0.record(stream)
+    for _ in range(a.steps):
+        graph.launch(stream=S)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    gms = max_over_ranks(world, e0.elapsed_time(e1))
+    graph.close()
+    sv.close()
+    for o in (grid, bd, st):
+        o.close()
+    top = legs[head]
+    out = {
+        "metric": f"particle-steps/s, batched IISPH, {ns} scenes",
+        "value": top["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": top["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded log-uniform cube sizes, lattice + jitter, Akinci box walls)",
+        "config": {"workload": "batched_iisph", "scenes": ns, "particles": n,
+                   "boundary_particles": int(b.bfirst[-1]), "kernel": "C2", "h": b.h,
+                   "tolerance": "0.1 % average density error", "dt": BATCH_DT,
+                   "headline_precision": head, "parallelism": f"replicas{world}"},
+        "clocks": top["clocks"], "gpu_launches": top["gpu_launches"],
+        "legs": legs,
+        "mixed_over_fp32": round(legs["mixed"]["value"] / legs["fp32"]["value"], 3),
+        "mixed_pos16_over_fp32": round(legs["mixed_pos16"]["value"] / legs["fp32"]["value"], 3),
+        "graph": {"precision": head, "ms_per_step": round(gms / a.steps, 3),
+                  "value": round(world * n * a.steps / (gms / 1e3), 1)},
+    }
     if rank == 0:
         print(json.dumps(out), flush=True)
 
@@ -1032,6 +1156,8 @@ def main():
             run_reference(a, world, rank)
         elif a.workload == "batched_pcisph":
             run_batched(a, world, rank, local)
+        elif a.workload == "batched_iisph":
+            run_batched_iisph(a, world, rank, local)
         elif a.workload == "column_16m":
             run_column(a, world, rank, local)
         elif a.workload == "mesh_lbvh":
