@@ -2,9 +2,11 @@
 
 The error reference for the engine's precision modes: the same algorithm as
 the FP32 oracle (oracle.cpp, which follows the reference's IISPH.cu), carried
-out in double precision with numpy over explicit pair lists (scipy's k-d tree
-finds the pairs; the summation order differs from any grid traversal, which
-FP64 makes irrelevant at the tolerances the tests use). Both the FP32 engine
+out in double precision over explicit pair lists: scipy's k-d tree finds the
+pairs on the host, and the arithmetic runs in torch float64 on the host or,
+for large scenes, on a GPU (`device="cuda"`). The summation order differs
+from any grid traversal, which FP64 makes irrelevant at the tolerances the
+tests use. Both the FP32 engine
 and the mixed-precision engine are measured against it, so the cost of FP16
 storage is stated as an error against the exact arithmetic rather than
 against another FP32 result.
@@ -32,91 +34,105 @@ _ALPHA = {C2: 21.0 / 2.0 / np.pi, B3: 16.0 / np.pi, W6: 1365.0 / 64.0 / np.pi,
 
 def _w(kind: int, q):
     """kernels.cuh:78-165, w(q) on [0, 1]."""
-    t1 = np.maximum(0.0, 1.0 - q)
+    import torch
+    t1 = torch.clamp_min(1.0 - q, 0.0)
     if kind == C2:
         return t1 ** 4 * (4.0 * q + 1.0)
     if kind == B3:
-        t2 = np.clip(0.5 - q, 0.0, 1.0)
+        t2 = torch.clamp(0.5 - q, 0.0, 1.0)
         return t1 ** 3 - 4.0 * t2 ** 3
     if kind == W6:
         return t1 ** 8 * (32.0 * q ** 3 + 25.0 * q * q + 8.0 * q + 1.0)
-    s = np.pi * np.minimum(1.0, q)
-    return 4.0 * np.cos(s) + np.cos(2.0 * s) + 3.0
+    s = np.pi * torch.clamp_max(q, 1.0)
+    return 4.0 * torch.cos(s) + torch.cos(2.0 * s) + 3.0
 
 
 def _dw(kind: int, q):
     """kernels.cuh:78-165, dw/dq on [0, 1]."""
-    t1 = np.maximum(0.0, 1.0 - q)
+    import torch
+    t1 = torch.clamp_min(1.0 - q, 0.0)
     if kind == C2:
         return t1 ** 3 * (-20.0 * q)
     if kind == B3:
-        t2 = np.clip(0.5 - q, 0.0, 1.0)
+        t2 = torch.clamp(0.5 - q, 0.0, 1.0)
         return -3.0 * t1 * t1 + 12.0 * t2 * t2
     if kind == W6:
         return t1 ** 7 * (16.0 * q * q + 7.0 * q + 1.0) * (-22.0 * q)
-    s = np.pi * np.minimum(1.0, q)
-    return -4.0 * np.pi * np.sin(s) - 2.0 * np.pi * np.sin(2.0 * s)
+    s = np.pi * torch.clamp_max(q, 1.0)
+    return -4.0 * np.pi * torch.sin(s) - 2.0 * np.pi * torch.sin(2.0 * s)
 
 
 class _Pairs:
     """All pairs (i, j) with |x_i - x_j| < r, i from `a`, j from `b`, with the
-    kernel value and the gradient factor: grad W_ij = gf * x_ij."""
+    kernel value and the gradient factor: grad W_ij = gf * x_ij. a, b: (N, 3)
+    float64 tensors; the pairs are found on the host."""
 
-    def __init__(self, kind: int, hbar: float, a: np.ndarray, b: np.ndarray, same: bool):
-        ta = cKDTree(a)
-        tb = ta if same else cKDTree(b)
+    def __init__(self, kind: int, hbar: float, a, b, same: bool):
+        import torch
+        an = a.cpu().numpy()
+        ta = cKDTree(an)
+        tb = ta if same else cKDTree(b.cpu().numpy())
         sp = ta.sparse_distance_matrix(tb, hbar, output_type="ndarray")
         # for a tree against itself the pairs include i == j (distance 0)
-        i, j = sp["i"].astype(np.int64), sp["j"].astype(np.int64)
+        dev = a.device
+        i = torch.from_numpy(sp["i"].astype(np.int64)).to(dev)
+        j = torch.from_numpy(sp["j"].astype(np.int64)).to(dev)
+        del sp
         x = a[i] - b[j]
-        r = np.sqrt((x * x).sum(1))
-        q = np.minimum(r / hbar, 1.0)
+        r = torch.sqrt((x * x).sum(1))
+        q = torch.clamp_max(r / hbar, 1.0)
         alpha = _ALPHA[kind]
         self.i, self.j, self.x, self.r2 = i, j, x, r * r
         self.w = alpha / hbar ** 3 * _w(kind, q)
-        with np.errstate(divide="ignore", invalid="ignore"):
-            gf = alpha / hbar ** 4 * _dw(kind, q) / r
-        self.gf = np.where(np.isfinite(gf), gf, 0.0)
+        gf = alpha / hbar ** 4 * _dw(kind, q) / r
+        self.gf = torch.where(torch.isfinite(gf), gf, torch.zeros_like(gf))
         self.n = a.shape[0]
 
     def sum(self, v):
         """sum over j of v (per pair, scalar or (P, 3)) into i."""
-        if v.ndim == 1:
-            return np.bincount(self.i, weights=v, minlength=self.n)
-        return np.stack([np.bincount(self.i, weights=v[:, c], minlength=self.n)
-                         for c in range(v.shape[1])], 1)
+        import torch
+        if v.dim() == 1:
+            return torch.bincount(self.i, weights=v, minlength=self.n)
+        return torch.stack([torch.bincount(self.i, weights=v[:, c], minlength=self.n)
+                            for c in range(v.shape[1])], 1)
 
 
 def iisph_run(kind: int, fluid: dict, bdy: dict, box_min, box_max, h: float, rho0: float,
               nu: float, g, dt: float, steps: int, iters: int, omega: float = 0.5,
-              warmstart: bool = True, p=None):
+              warmstart: bool = True, p=None, device: str = "cpu"):
     """`steps` IISPH steps with exactly `iters` Jacobi sweeps each (the
     convergence test is left out, so that every precision runs the same
     arithmetic). fluid: x, y, z, vx, vy, vz, m (any order); bdy: x, y, z, m.
-    Returns dict of float64 arrays in the input order: x, y, z, vx, vy, vz,
-    rho, p, aii, sii."""
-    X = np.stack([np.asarray(fluid[k], np.float64) for k in ("x", "y", "z")], 1)
-    V = np.stack([np.asarray(fluid[k], np.float64) for k in ("vx", "vy", "vz")], 1)
-    m = np.asarray(fluid["m"], np.float64)
-    B = np.stack([np.asarray(bdy[k], np.float64) for k in ("x", "y", "z")], 1)
-    mb = np.asarray(bdy["m"], np.float64)
-    n = m.size
-    P = np.zeros(n) if p is None else np.asarray(p, np.float64).copy()
-    lo = np.asarray(box_min, np.float64)
-    hi = np.asarray(box_max, np.float64)
-    grav = np.asarray(g, np.float64)
+    Returns dict of float64 numpy arrays in the input order: x, y, z, vx, vy,
+    vz, rho, p, aii, sii."""
+    import torch
+    f64 = torch.float64
+
+    def t(a):
+        return torch.as_tensor(np.asarray(a, np.float64), dtype=f64, device=device)
+
+    X = torch.stack([t(fluid[k]) for k in ("x", "y", "z")], 1)
+    V = torch.stack([t(fluid[k]) for k in ("vx", "vy", "vz")], 1)
+    m = t(fluid["m"])
+    B = torch.stack([t(bdy[k]) for k in ("x", "y", "z")], 1)
+    mb = t(bdy["m"])
+    n = m.numel()
+    P = torch.zeros(n, dtype=f64, device=device) if p is None else t(p).clone()
+    lo = t(box_min)
+    hi = t(box_max)
+    grav = t(g)
     hbar = 2.0 * h
     r0i = 1.0 / (rho0 * rho0)
     rho = aii = sii = None
     for _ in range(steps):
         F = _Pairs(kind, hbar, X, X, True)
-        Bp = _Pairs(kind, hbar, X, B, False) if mb.size else None
+        Bp = _Pairs(kind, hbar, X, B, False) if mb.numel() else None
         mj = m[F.j]
         # densities (solver.cuh:18-38)
         rho = F.sum(mj * F.w)
-        gb = np.zeros((n, 3))
+        gb = torch.zeros((n, 3), dtype=f64, device=device)
         if Bp is not None:
-            rho += Bp.sum(mb[Bp.j] * Bp.w)
+            rho = rho + Bp.sum(mb[Bp.j] * Bp.w)
             gb = Bp.sum((mb[Bp.j] * Bp.gf)[:, None] * Bp.x)
         # gravity + artificial viscosity (solver.cuh:40-69), then v*
         vij = V[F.i] - V[F.j]
@@ -134,16 +150,15 @@ def iisph_run(kind: int, fluid: dict, bdy: dict, box_min, box_max, h: float, rho
         sii = (rho0 - rho) / dt - (vdiv + (V * gb).sum(1))
 
         def jacobi(Ap):  # IISPH.cu:108-117
-            small = np.abs(aii) < 1e-6
-            with np.errstate(divide="ignore", invalid="ignore"):
-                d = np.maximum(0.0, omega * (sii - Ap) / aii)
-            return np.where(small, 0.0, d)
+            small = torch.abs(aii) < 1e-6
+            d = torch.clamp_min(omega * (sii - Ap) / aii, 0.0)
+            return torch.where(small, torch.zeros_like(d), d)
 
         def pacc(P):  # IISPH.cu:68-98
             sp = mj * (P[F.i] + P[F.j]) * F.gf
             return -r0i * (F.sum(sp[:, None] * F.x) + P[:, None] * gb)
 
-        P = 0.5 * P if warmstart else jacobi(np.zeros(n))
+        P = 0.5 * P if warmstart else jacobi(torch.zeros(n, dtype=f64, device=device))
         for _ in range(iters):  # IISPH.cu:119-162
             A = pacc(P)
             aij = A[F.i] - A[F.j]
@@ -155,7 +170,9 @@ def iisph_run(kind: int, fluid: dict, bdy: dict, box_min, box_max, h: float, rho
         X = X + dt * V
         # hard_enforce_bounds (scene.cu:466-483)
         touch = ((X <= lo) | (X >= hi)).any(1)
-        V[touch] *= -0.1
-        X = np.clip(X, lo, hi)
-    return {"x": X[:, 0], "y": X[:, 1], "z": X[:, 2], "vx": V[:, 0], "vy": V[:, 1],
-            "vz": V[:, 2], "rho": rho, "p": P, "aii": aii, "sii": sii}
+        V = torch.where(touch[:, None], V * -0.1, V)
+        X = torch.minimum(torch.maximum(X, lo), hi)
+        del F, Bp
+    out = {"x": X[:, 0], "y": X[:, 1], "z": X[:, 2], "vx": V[:, 0], "vy": V[:, 1],
+           "vz": V[:, 2], "rho": rho, "p": P, "aii": aii, "sii": sii}
+    return {k: v.cpu().numpy() for k, v in out.items()}
