@@ -288,11 +288,16 @@ int reyn_solver_create(reyn_scheme scheme, const reyn_params* params,
 int reyn_solver_destroy(reyn_solver* s);
 
 /* Solver::step(state, grid, bdy, dt) on a grid built by
- * construct_and_reorder over `state`. IISPH's pressure is carried across
- * steps and re-permuted with the grid's permutation automatically (the
- * reference passes it as an extra reorder buffer, main.cu:68). iters (may
- * be NULL) receives the iteration count (1 for SESPH); it synchronises the
- * stream for PCISPH/IISPH. */
+ * construct_and_reorder over `state` (the solvers' Resort::yes form), or by
+ * reyn_grid_construct over `state`'s own position arrays (reyn_particles_soa;
+ * Resort::no, IISPH.cu:264-266): the particles then keep the caller's order,
+ * the step runs on a copy gathered into grid order and positions,
+ * velocities and the solver buffers are scattered back (not batched grids,
+ * not inside a step graph). IISPH's pressure is carried across steps in the
+ * state's order and re-permuted with the grid's permutation automatically
+ * (the reference passes it as an extra reorder buffer, main.cu:68). iters
+ * (may be NULL) receives the iteration count (1 for SESPH); it synchronises
+ * the stream for PCISPH/IISPH. */
 int reyn_solver_step(reyn_solver* s, reyn_particles* state,
     const reyn_grid* grid, const reyn_boundary* bdy, float dt,
     uint32_t* iters, void* stream);
@@ -309,7 +314,8 @@ int reyn_solver_step_bounded(reyn_solver* s, reyn_particles* state,
     const float bound_min[3], const float bound_max[3], uint32_t* iters,
     void* stream);
 
-/* per-particle solver buffers (device, grid order of the last step): rho
+/* per-particle solver buffers (device, in the particle order of the last
+ * step's state: grid order after construct_and_reorder): rho
  * the (predicted) densities, ax..az the last accelerations; p the IISPH
  * pressure, for PCISPH the pressure term p / rho^2 of the last iteration
  * (_eos_pcisph, PCISPH.cu:15-19); aii, sii the IISPH diagonal and source */

@@ -133,6 +133,16 @@ public:
         return { info(), g_ };
     }
 
+    // construct over a state's own positions: a solver step on the result
+    // keeps the caller's particle order (the solvers' Resort::no form)
+    UniformGrid<Resort::no> construct(float search_radius, Particles& state,
+        cudaStream_t s = nullptr)
+    {
+        reyn_soa v {};
+        check(reyn_particles_soa(state.handle(), &v));
+        return construct(search_radius, v.xx, v.xy, v.xz, v.n, s);
+    }
+
     // construct_and_reorder (uniformgrid.cuh:477-483): the state and any
     // extra device arrays of n floats are permuted into grid order
     template <class... Extra>
@@ -255,8 +265,6 @@ namespace detail {
 
 // SESPH<K,R> (SESPH.cuh:11-68): step returns nothing, like the reference
 template <class K, Resort R = Resort::yes> class SESPH : public detail::Solver {
-    static_assert(R == Resort::yes, "the engine's solvers run on reordered state");
-
 public:
     SESPH(K W, uint32_t N, float nu, float h, float rho0,
         float3 g = make_float3(0.f, -9.81f, 0.f), float k = 500.f)
@@ -287,8 +295,6 @@ private:
 
 // PCISPH<K,R> (PCISPH.cuh:8-111): step returns the iteration count
 template <class K, Resort R = Resort::yes> class PCISPH : public detail::Solver {
-    static_assert(R == Resort::yes, "the engine's solvers run on reordered state");
-
 public:
     PCISPH(K W, uint32_t N, float nu, float h, float rho0)
         : detail::Solver(REYN_PCISPH, detail::params(REYN_PCISPH, W, nu, h, rho0), N)
@@ -310,8 +316,6 @@ public:
 
 // IISPH<K,R> (IISPH.cuh:8-93): step returns the iteration count
 template <class K, Resort R = Resort::yes> class IISPH : public detail::Solver {
-    static_assert(R == Resort::yes, "the engine's solvers run on reordered state");
-
 public:
     IISPH(K W, uint32_t N, float nu, float h, float rho0)
         : detail::Solver(REYN_IISPH, detail::params(REYN_IISPH, W, nu, h, rho0), N)

@@ -315,6 +315,13 @@ class Grid:
         check(lib().reyn_grid_construct(self.h, self.r, _ptr(x), _ptr(y), _ptr(z), x.numel(),
                                         _stream(stream)))
 
+    def construct_state(self, state: Particles, stream=None):
+        """construct over the state's own positions: a solver step on this
+        grid keeps the caller's particle order (Resort::no)."""
+        v = state.soa()
+        check(lib().reyn_grid_construct(self.h, self.r, v.xx, v.xy, v.xz, v.n,
+                                        _stream(stream)))
+
     def construct_and_reorder(self, state: Particles, extra: Sequence = (), stream=None):
         ptrs = (_vp * max(len(extra), 1))(*[_ptr(t) for t in extra])
         check(lib().reyn_grid_construct_and_reorder(self.h, self.r, state.h, ptrs, len(extra),

@@ -103,6 +103,7 @@ struct Grid {
     bool reordered = false;    // last build was construct_and_reorder
     const reyn_particles* reordered_state = nullptr;
     uint64_t reorder_epoch = 0; // state epoch produced by that reorder
+    const float* built_pos[3] = { nullptr, nullptr, nullptr }; // positions of the last build
 
     GridView view(float search_radius) const;
     // counting-sort build over positions: keys, counts, prefix, canonical
@@ -173,6 +174,10 @@ struct reyn_solver {
     bool vmax_valid = false;
     // non-null while a step of this solver is being captured into a graph
     reyn::GraphCtx* graph = nullptr;
+    // a step on a grid built by construct (the reference's Resort::no): the
+    // state gathered into grid order, stepped there and scattered back
+    std::unique_ptr<reyn_particles> shadow;
+    std::array<reyn::DevArray<float>, 7> shadow_out; // buffers scattered back
     ~reyn_solver()
     {
         if (vmax_ready)

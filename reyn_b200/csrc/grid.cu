@@ -317,6 +317,9 @@ void Grid::build(const float* x, const float* y, const float* z, uint32_t np,
     sorted.resize(np);
     reordered = false;
     reordered_state = nullptr;
+    built_pos[0] = x;
+    built_pos[1] = y;
+    built_pos[2] = z;
     const GridView g = view(geom.r);
     counts_dirty = true;
     if (np) {

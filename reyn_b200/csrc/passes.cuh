@@ -1132,10 +1132,12 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     sv.vmax_valid = false;
     require(n == sv.n, "particle count differs from the solver's");
     require(dt > 0.f && std::isfinite(dt), "dt must be positive and finite");
-    if (!(grid.reordered && grid.reordered_state == &st && grid.reorder_epoch == st.epoch
+    // the solver's own copy in grid order (a step on a construct-built grid)
+    const bool shadow = &st == sv.shadow.get() && grid.n == n;
+    if (!shadow && !(grid.reordered && grid.reordered_state == &st && grid.reorder_epoch == st.epoch
             && grid.n == n))
         fail(REYN_ERR_NOT_READY,
-            "the grid must come from construct_and_reorder over this particle state");
+            "the grid must come from construct_and_reorder or construct over this particle state");
     ensure_buffers(sv, n);
     if (!st.packed_valid)
         pack_state(st, s);

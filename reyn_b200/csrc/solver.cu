@@ -94,13 +94,138 @@ void ensure_buffers(reyn_solver& sv, uint32_t n)
 void solver_step_wide(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     const reyn_boundary* bdy, float dt, cudaStream_t s, const float* bmin, const float* bmax);
 
-void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
+void solver_step_sorted(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     const reyn_boundary* bdy, float dt, cudaStream_t s, const float* bmin, const float* bmax)
 {
     if (sv.prm.block_size > NBR_THREADS)
         solver_step_wide(sv, st, grid, bdy, dt, s, bmin, bmax);
     else
         solver_step_t<NBR_THREADS>(sv, st, grid, bdy, dt, s, bmin, bmax);
+}
+
+// dst[k][perm[s]] = src[k][s]: arrays in grid order back to the caller's order
+__global__ void k_scatter_back(uint32_t n, const uint32_t* __restrict__ perm, GatherArgs a)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    const uint32_t p = perm[s];
+#pragma unroll
+    for (int k = 0; k < MAX_GATHER; ++k)
+        if (k < a.count)
+            a.dst[k][p] = __ldg(a.src[k] + s);
+}
+
+// the grid's last build was construct over this state's current positions
+// (the reference's UniformGrid<Resort::no>, uniformgrid.cuh:363-380)
+bool built_unsorted(const Grid& g, const reyn_particles& st)
+{
+    return !g.reordered && g.n_scenes == 0 && g.n == st.n && g.built_pos[0] == st.cur[FX].get()
+        && g.built_pos[1] == st.cur[FY].get() && g.built_pos[2] == st.cur[FZ].get();
+}
+
+// Solver::step with R = Resort::no (the solvers are instantiated for both,
+// IISPH.cu:264-269): neighbours come through the grid's permutation while the
+// particles keep the caller's order. The state is gathered into grid order in
+// solver-owned arrays, stepped there by the passes of the sorted step, and
+// positions, velocities and the solver's per-particle buffers are scattered
+// back. Neighbour sums then run in the order the reference's Resort::no
+// kernels visit them (cell by cell, each cell in the permutation's order).
+// IISPH's carried pressure stays in the caller's order between steps.
+void solver_step_unsorted(reyn_solver& sv, reyn_particles& st, const Grid& grid,
+    const reyn_boundary* bdy, float dt, cudaStream_t s, const float* bmin, const float* bmax)
+{
+    const uint32_t n = st.n;
+    require(n == sv.n, "particle count differs from the solver's");
+    require(dt > 0.f && std::isfinite(dt), "dt must be positive and finite");
+    require(!sv.graph, "a captured step reorders the state (construct_and_reorder)");
+    ensure_buffers(sv, n);
+    if (!sv.shadow)
+        sv.shadow = std::make_unique<reyn_particles>();
+    reyn_particles& sh = *sv.shadow;
+    sh.n = n;
+    sh.rho0 = st.rho0;
+    for (auto& a : sh.cur)
+        a.resize(n);
+    sh.pm.resize(n);
+    sh.vel.resize(n);
+    const uint32_t* perm = grid.sorted.get();
+    GatherArgs ga {};
+    for (int k = 0; k < NFIELDS; ++k) {
+        ga.src[k] = st.cur[k].get();
+        ga.dst[k] = sh.cur[k].get();
+    }
+    ga.count = NFIELDS;
+    ga.pm = sh.pm.get();
+    ga.vel = sh.vel.get();
+    launch_gather(n, perm, ga, s);
+    sh.packed_valid = true;
+    if (sv.scheme == REYN_IISPH) {
+        if (sv.p_state == &st && sv.p_epoch == st.epoch) { // warm: p in the caller's order
+            GatherArgs gp {};
+            gp.src[0] = sv.p.get();
+            gp.dst[0] = sv.p_tmp.get();
+            gp.count = 1;
+            launch_gather(n, perm, gp, s);
+            sv.p.swap(sv.p_tmp);
+        } else {
+            sv.p.zero(s);
+        }
+        sv.p_state = &sh;
+        sv.p_epoch = sh.epoch;
+    }
+    auto scatter = [&] {
+        DevArray<float>* bufs[] = { &sv.rho, &sv.p, &sv.aii, &sv.sii, &sv.ax, &sv.ay, &sv.az };
+        GatherArgs sa {};
+        int k = 0;
+        for (int f = FX; f <= FVZ; ++f, ++k) {
+            sa.src[k] = sh.cur[f].get();
+            sa.dst[k] = st.cur[f].get();
+        }
+        int nb = 0;
+        for (DevArray<float>* b : bufs) {
+            if (b->size() != n)
+                continue;
+            sv.shadow_out[nb].resize(n);
+            sa.src[k] = b->get();
+            sa.dst[k++] = sv.shadow_out[nb++].get();
+        }
+        sa.count = k;
+        if (n)
+            REYN_KERNEL("k_scatter_back", s,
+                k_scatter_back<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, perm, sa));
+        nb = 0;
+        for (DevArray<float>* b : bufs)
+            if (b->size() == n)
+                b->swap(sv.shadow_out[nb++]);
+        st.packed_valid = false;
+        st.version += 1;
+        if (sv.scheme == REYN_IISPH) {
+            sv.p_state = &st;
+            sv.p_epoch = st.epoch;
+        }
+        if (sv.vmax_state == &sh) {
+            sv.vmax_state = &st;
+            sv.vmax_version = st.version;
+        }
+    };
+    try {
+        solver_step_sorted(sv, sh, grid, bdy, dt, s, bmin, bmax);
+    } catch (const Error& e) {
+        if (e.code == REYN_ERR_ITER_LIMIT) // the step completed
+            scatter();
+        throw;
+    }
+    scatter();
+}
+
+void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
+    const reyn_boundary* bdy, float dt, cudaStream_t s, const float* bmin, const float* bmax)
+{
+    if (built_unsorted(grid, st) && &st != sv.shadow.get())
+        solver_step_unsorted(sv, st, grid, bdy, dt, s, bmin, bmax);
+    else
+        solver_step_sorted(sv, st, grid, bdy, dt, s, bmin, bmax);
 }
 
 // ---- FP64 diagnostics ----------------------------------------------------------

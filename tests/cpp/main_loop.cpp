@@ -5,7 +5,9 @@
 // With a third argument "fused" the loop uses the fused tail (next_dt and
 // step_bounded in place of simple_dt_controller, step and hard_enforce_bounds);
 // "fixed" keeps dt fixed (no controller; the id array is not reordered) and
-// "graph" runs that fixed-dt loop as replays of a StepGraph.
+// "graph" runs that fixed-dt loop as replays of a StepGraph; "unsorted" is
+// the default loop with IISPH<C2, Resort::no> on grids built by construct
+// (the particles keep their order).
 //
 // input  (little-endian): u32 N, u32 Nb, u32 steps, f32 h, rho0, nu, dt0,
 //        lambda, box_min[3], box_max[3], then N floats each of x y z vx vy vz
@@ -15,6 +17,7 @@
 #include "reyn_b200.hpp"
 
 #include <cstdio>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -62,6 +65,9 @@ int main(int argc, char** argv)
         const C2 W(2.f * h);
         UniformGridBuilder builder(bmin, bmax, 2.f * h);
         IISPH<C2, Resort::yes> solver(W, N, nu, h, rho0);
+        std::unique_ptr<IISPH<C2, Resort::no>> unsorted;
+        if (mode == "unsorted")
+            unsorted = std::make_unique<IISPH<C2, Resort::no>>(W, N, nu, h, rho0);
         const float3 g = make_float3(0.f, -9.81f, 0.f);
         std::vector<uint32_t> iters_log;
         std::vector<float> dt_log;
@@ -78,6 +84,11 @@ int main(int argc, char** argv)
             if (mode == "fixed") {
                 const auto grid { builder.construct_and_reorder(2.f * h, state) };
                 iters = solver.step_bounded(state, grid, bdy, dt, bmin, bmax);
+            } else if (unsorted) {
+                dt = simple_dt_controller(iters, dt, lambda, h, state, g, 10, 0.001f);
+                const UniformGrid<Resort::no> grid { builder.construct(2.f * h, state) };
+                iters = unsorted->step(state, grid, bdy, dt);
+                hard_enforce_bounds(state, bmin, bmax);
             } else if (fused) {
                 dt = solver.next_dt(state, iters, dt, lambda, h, g, 10, 0.001f);
                 const auto grid { builder.construct_and_reorder(2.f * h, state, d_id) };

@@ -40,9 +40,11 @@ def by_id(arrs: dict, ids: np.ndarray) -> dict:
 
 def run_engine(scheme: int, kind: int, fluid: dict, bdy: dict, box_min, box_max, h: float,
                rho0: float, nu: float, dt: float, steps: int, params=None, cell_ratio=0.5,
-               order=0):
+               order=0, resort=True):
     """The reference main loop on the engine: construct_and_reorder (with
-    the particle ID as an extra array), solver step, hard bounds."""
+    the particle ID as an extra array), solver step, hard bounds. With
+    resort=False the grid is built by construct over the state's positions
+    and the particles keep their order (the solvers' Resort::no form)."""
     import torch
 
     import reyn_b200 as rb
@@ -61,7 +63,10 @@ def run_engine(scheme: int, kind: int, fluid: dict, bdy: dict, box_min, box_max,
     sv = rb.Solver(scheme, prm, n)
     iters = []
     for _ in range(steps):
-        grid.construct_and_reorder(st, [ids])
+        if resort:
+            grid.construct_and_reorder(st, [ids])
+        else:
+            grid.construct_state(st)
         iters.append(sv.step(st, grid, bd, dt))
         rb.enforce_bounds(st, box_min, box_max)
     torch.cuda.synchronize()

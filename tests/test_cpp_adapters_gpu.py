@@ -50,7 +50,10 @@ def read_out(path, n):
     return iters, dts, dict(zip(("x", "y", "z", "vx", "vy", "vz", "id"), body))
 
 
-def test_cpp_main_loop_matches_oracle(cuda, tmp_path):
+@pytest.mark.parametrize("mode", [[], ["unsorted"]])
+def test_cpp_main_loop_matches_oracle(cuda, tmp_path, mode):
+    """The main loop with the solver on reordered state and, with
+    "unsorted", on grids built by construct (IISPH<C2, Resort::no>)."""
     exe = compile_main_loop(str(tmp_path))
     sc = scenes.dam_break((14, 12, 10), 0.02, (0.5, 0.5, 0.5), velocity_noise=0.02, seed=21)
     bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
@@ -58,8 +61,10 @@ def test_cpp_main_loop_matches_oracle(cuda, tmp_path):
     inp = os.path.join(str(tmp_path), "in.bin")
     out = os.path.join(str(tmp_path), "out.bin")
     write_scene(inp, sc, bm, steps, dt0, lam, nu)
-    subprocess.run([exe, inp, out], check=True)
+    subprocess.run([exe, inp, out] + mode, check=True)
     iters, dts, got = read_out(out, sc.n)
+    if mode:  # the particles kept their order
+        np.testing.assert_array_equal(got["id"], np.asarray(sc.fluid["id"], np.float32))
 
     # the same loop on the oracle
     fl = {k: v.copy() for k, v in sc.fluid.items()}
