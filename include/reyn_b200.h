@@ -224,6 +224,17 @@ int reyn_boundary_create_batched(const float* bx, const float* by,
 int reyn_boundary_arrays(const reyn_boundary* b, const float** bx,
     const float** by, const float** bz, const float** bm, uint32_t* nb);
 
+/* compute_densities<K, R> (solver.cuh:19-38): rho_i = sum_j m_j W(x_ij) over
+ * the fluid neighbours within the grid's radius r (self included) plus
+ * sum_b m_b W(x_ib) over the boundary samples (bdy may be NULL), `kernel` at
+ * support r. Positions and masses are the arrays the grid was built over:
+ * in grid order after construct_and_reorder, the caller's order after
+ * reyn_grid_construct (rho is then in the caller's order too). Not for
+ * batched grids. */
+int reyn_compute_densities(const reyn_grid* g, const float* xx,
+    const float* xy, const float* xz, const float* m, const reyn_boundary* bdy,
+    reyn_kernel kernel, float* rho, void* stream);
+
 /* ---- solvers (src/solvers/SESPH, PCISPH, IISPH) ------------------------- */
 typedef enum reyn_scheme {
     REYN_SESPH = 0, /* SESPH.cu:68-95   */

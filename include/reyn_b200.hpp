@@ -340,6 +340,20 @@ public:
     }
 };
 
+// ---- compute_densities<K, R> (solver.cuh:19-38) as a call ---------------------
+// the densities of the N points the grid was built over (grid order after
+// construct_and_reorder, the caller's order after construct); W's support
+// is the grid's search radius
+template <class K, Resort R>
+void compute_densities(const float* xx, const float* xy, const float* xz, const float* m,
+    float* rho, uint32_t N, const K&, const UniformGrid<R>& grid, const BoundarySamples& bdy,
+    cudaStream_t s = nullptr)
+{
+    if (N != grid.info.n)
+        throw Error(REYN_ERR_INVALID, "N differs from the grid's point count");
+    check(reyn_compute_densities(grid.grid, xx, xy, xz, m, bdy.handle(), K::kind, rho, s));
+}
+
 // ---- time step and bounds (cfl.cuh:13-32, scene.cu:485-491) --------------------
 inline float cfl_time_step(float lambda, float h, Particles& state, float3 g,
     cudaStream_t s = nullptr)

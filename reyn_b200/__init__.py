@@ -110,6 +110,7 @@ _SIGNATURES = {
     "reyn_grid_info_get": [_vp, ctypes.POINTER(GridInfo)],
     "reyn_grid_permutation": [_vp, ctypes.POINTER(_vp)],
     "reyn_grid_neighbour_stats": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp],
+    "reyn_compute_densities": [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp],
     "reyn_boundary_create": [_vp, _vp, _vp, _vp, _u32, _f, _f, _u32, _vp, ctypes.POINTER(_vp)],
     "reyn_boundary_destroy": [_vp],
     "reyn_boundary_arrays": [_vp] + [ctypes.POINTER(_vp)] * 4 + [ctypes.POINTER(_u32)],
@@ -347,6 +348,18 @@ class Grid:
                                               _ptr(count), _ptr(len2), _ptr(rho),
                                               _stream(stream)))
         return count, len2, rho
+
+    def compute_densities(self, x, y, z, m, bdy: Optional["Boundary"] = None, kernel: int = C2,
+                          stream=None):
+        """compute_densities (reference solver.cuh:19-38): fluid neighbours
+        plus boundary samples, over the arrays the grid was built over; the
+        result is in the order of those arrays."""
+        import torch
+        rho = torch.empty(x.numel(), device=x.device, dtype=torch.float32)
+        check(lib().reyn_compute_densities(self.h, _ptr(x), _ptr(y), _ptr(z), _ptr(m),
+                                           bdy.h if bdy is not None else None, kernel,
+                                           _ptr(rho), _stream(stream)))
+        return rho
 
 
 class Boundary:

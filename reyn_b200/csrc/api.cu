@@ -284,6 +284,20 @@ int reyn_grid_neighbour_stats(const reyn_grid* g, const float* xx, const float* 
     });
 }
 
+int reyn_compute_densities(const reyn_grid* g, const float* xx, const float* xy,
+    const float* xz, const float* m, const reyn_boundary* bdy, reyn_kernel kernel, float* rho,
+    void* stream)
+{
+    return guard([&] {
+        require(g != nullptr, "null grid");
+        require(g->n == 0 || (xx && xy && xz && m && rho), "null array");
+        check_kernel(kernel);
+        const cudaStream_t s = as_stream(stream);
+        compute_densities(*g, xx, xy, xz, m, bdy, kernel, rho, s);
+        const_cast<reyn_grid*>(g)->check_status(s, "compute_densities");
+    });
+}
+
 // ---- boundary -------------------------------------------------------------------
 
 int reyn_boundary_create(const float* bx, const float* by, const float* bz, const float* bm,

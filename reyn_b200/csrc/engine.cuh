@@ -220,6 +220,12 @@ void kernel_eval(int kind, float h_bar, const float* dx, const float* dy,
     const float* dz, uint32_t n, float* w, float* gx, float* gy, float* gz,
     cudaStream_t s);
 
+// (x, y, z, m) of point order[s] (s when order is null) into pts[s]
+void pack_positions(uint32_t n, const uint32_t* order, const float* x, const float* y,
+    const float* z, const float* m, float4* pts, cudaStream_t s);
+// compute_densities (solver.cuh:19-38) into rho[n], the caller's order
+void compute_densities(const Grid& g, const float* x, const float* y, const float* z,
+    const float* m, const reyn_boundary* bdy, int kind, float* rho, cudaStream_t s);
 void neighbour_stats(const Grid& g, const float* x, const float* y,
     const float* z, const float* m, int kind, uint32_t* count, float* len2,
     float* rho, cudaStream_t s);

@@ -589,6 +589,14 @@ __global__ void k_pack_positions(uint32_t n, const uint32_t* __restrict__ order,
     pts[s] = make_float4(x[p], y[p], z[p], m ? m[p] : 0.f);
 }
 
+void pack_positions(uint32_t n, const uint32_t* order, const float* x, const float* y,
+    const float* z, const float* m, float4* pts, cudaStream_t s)
+{
+    if (n)
+        REYN_KERNEL("k_pack_positions", s,
+            k_pack_positions<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, order, x, y, z, m, pts));
+}
+
 template <int KIND>
 static void launch_stats(int range, unsigned b, cudaStream_t s, uint32_t n, GridView g,
     KernelConst kc, const float4* pts, const uint32_t* owner, uint32_t* count, float* len2,

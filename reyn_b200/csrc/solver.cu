@@ -228,6 +228,85 @@ void solver_step(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         solver_step_sorted(sv, st, grid, bdy, dt, s, bmin, bmax);
 }
 
+// ---- densities alone ------------------------------------------------------------
+
+// compute_densities (solver.cuh:19-38): rho_i = sum_j m_j W_ij over the fluid
+// neighbours within r (self included) + sum_b m_b W_ib over the boundary
+// samples, per grid slot over packed points; `owner` maps a slot back to
+// the caller's index on a grid built without reorder
+template <int KIND, int R>
+__global__ void __launch_bounds__(NBR_THREADS) k_compute_densities(uint32_t n, GridView g,
+    KernelConst kc, const float4* __restrict__ pts, const uint32_t* __restrict__ owner, Bdy b,
+    float* __restrict__ rho, uint32_t* __restrict__ status)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    const float4 me = pts[s];
+    int3 c = cell_of(g, me.x, me.y, me.z);
+    if (!cell_inside(g, c, R) || !(isfinite(me.x) && isfinite(me.y) && isfinite(me.z))) {
+        atomicOr(status, STATUS_OUT_OF_GRID);
+        c = clamp_cell(g, c, R);
+    }
+    float rf = 0.f;
+    for_each_neighbour<R>(g, c, me.x, me.y, me.z, pts,
+        [&](uint32_t, const float4& q, float, float, float, float l2) {
+            rf += q.w * pair_w<KIND>(kc, l2);
+        });
+    float rb = 0.f;
+    for_each_boundary(b, me.x, me.y, me.z,
+        [&](uint32_t, const float4& q, float, float, float, float l2) {
+            rb += q.w * pair_w<KIND>(kc, l2);
+        });
+    rho[owner ? owner[s] : s] = rf + rb;
+}
+
+void compute_densities(const Grid& g, const float* x, const float* y, const float* z,
+    const float* m, const reyn_boundary* bdy, int kind, float* rho, cudaStream_t s)
+{
+    require(g.n_scenes == 0, "batched grids: the batched solver step computes densities");
+    const uint32_t n = g.n;
+    Bdy b {};
+    if (bdy && bdy->nb) {
+        require(bdy->grid.n_scenes == 0, "batched boundaries need the batched solver step");
+        require(bdy->grid.geom.r >= g.geom.r,
+            "the boundary grid's radius is below the fluid grid's search radius");
+        b.g = bdy->view();
+        b.g.r2 = g.geom.r * g.geom.r;
+        b.pm = bdy->pm.get();
+        b.near = bdy->near.get();
+        b.n = bdy->nb;
+    }
+    if (!n)
+        return;
+    DevArray<float4>& pts = g.pts_tmp;
+    pts.resize(n);
+    const uint32_t* order = g.reordered ? nullptr : g.sorted.get();
+    pack_positions(n, order, x, y, z, m, pts.get(), s);
+    const GridView v = g.view(g.geom.r);
+    const KernelConst kc = make_kernel(kind, g.geom.r);
+    const unsigned nb = blocks_for(n, NBR_THREADS);
+    uint32_t* st = const_cast<uint32_t*>(g.status.get());
+    auto go = [&](auto K) {
+        constexpr int KIND = decltype(K)::value;
+        if (g.geom.range == 2)
+            k_compute_densities<KIND, 2><<<nb, NBR_THREADS, 0, s>>>(n, v, kc, pts.get(), order, b,
+                rho, st);
+        else
+            k_compute_densities<KIND, 1><<<nb, NBR_THREADS, 0, s>>>(n, v, kc, pts.get(), order, b,
+                rho, st);
+    };
+    ProfScope scope("k_compute_densities", s);
+    switch (kind) {
+    case K_C2: go(std::integral_constant<int, K_C2> {}); break;
+    case K_B3: go(std::integral_constant<int, K_B3> {}); break;
+    case K_W6: go(std::integral_constant<int, K_W6> {}); break;
+    case K_COS: go(std::integral_constant<int, K_COS> {}); break;
+    default: fail(REYN_ERR_INVALID, "unknown kernel");
+    }
+    REYN_LAUNCHED("k_compute_densities");
+}
+
 // ---- FP64 diagnostics ----------------------------------------------------------
 
 // sum m, sum m v, sum m |v|^2 / 2 in FP64 (per-block FP64 partials, one
