@@ -95,6 +95,9 @@ def parse_args():
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the block-size / cell-ratio autotuner (128 threads, cell r/2)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--reorder-every", type=int, default=1,
+                    help="column_16m: reorder the state every K steps, the steps between on "
+                         "grids built without reorder")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -924,13 +927,19 @@ def run_column(a, world, rank, local):
         rb.PRECISION_MIXED_POS16 if a.precision == "mixed_pos16" else rb.PRECISION_FP32)
     sv = rb.Solver(rb.IISPH, prm, n)
     dt_visc = viscous_dt_limit(h, nu)
-    state = {"dt": DT0, "it": 0}
+    state = {"dt": DT0, "it": 0, "k": 0}
     log = []
 
     def step():
         state["dt"] = min(sv.next_dt(st, state["it"], state["dt"], LAMBDA, h, (0.0, -9.81, 0.0),
                                      10, 0.001, stream=S), dt_visc)
-        grid.construct_and_reorder(st, stream=S)
+        # the state is reordered every `reorder_every` steps; the steps
+        # between run on a grid built by construct (Resort::no)
+        if state["k"] % a.reorder_every == 0:
+            grid.construct_and_reorder(st, stream=S)
+        else:
+            grid.construct_state(st, stream=S)
+        state["k"] += 1
         try:
             state["it"] = sv.step(st, grid, bd, state["dt"], stream=S, bounds=((0, 0, 0), box))
         except rb.ReynError as err:
@@ -971,7 +980,8 @@ def run_column(a, world, rank, local):
                 "Fibonacci sphere, generated on the GPU)",
         "config": {"workload": "column_16m", "particles": n, "boundary_particles": bd.nb,
                    "kernel": "W6", "h": h, "nu": nu, "precision": prm.precision,
-                   "cell_order": a.order, "convergence": "avg density error <= 0.1%"},
+                   "cell_order": a.order, "convergence": "avg density error <= 0.1%",
+                   "reorder_every": a.reorder_every},
         "clocks": ck_clocks, "gpu_launches": sum(v[0] for v in prof.values()),
         "iters_per_step": [x[0] for x in log],
         "avg_density_error_per_step": [round(x[1], 7) for x in log],
