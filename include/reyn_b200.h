@@ -84,6 +84,21 @@ int reyn_particles_soa(reyn_particles* p, reyn_soa* out);
 int reyn_particles_upload(reyn_particles* p, const float* xx, const float* xy,
     const float* xz, const float* vx, const float* vy, const float* vz,
     const float* m, void* stream);
+/* Particles::reorder(sorted, tmp) (particles.cu:93-113): every attribute
+ * gathered by `sorted` (device, n entries: new[i] = old[sorted[i]]). The
+ * array must be a permutation of [0, n): it is checked first (the call
+ * synchronises) and REYN_ERR_INVALID leaves the state unchanged. Like the
+ * reference, solver buffers are not permuted: IISPH's next step on this
+ * state starts from zero pressure. */
+int reyn_particles_reorder(reyn_particles* p, const uint32_t* sorted,
+    void* stream);
+/* Particles::resize_truncate (keep != 0: the first min(old, n) particles
+ * are kept) and resize_uninit (keep == 0) (particles.cu:35-91); particles
+ * not kept are zero. A solver created for the old count rejects the state;
+ * the positions_only form of resize_uninit is not offered (it leaves the
+ * arrays at different sizes). Synchronises the stream. */
+int reyn_particles_resize(reyn_particles* p, uint32_t n, int keep,
+    void* stream);
 int reyn_particles_download(reyn_particles* p, float* xx, float* xy,
     float* xz, float* vx, float* vy, float* vz, float* m, void* stream);
 /* save_to_ply (ply_io.cu:7-55): the positions as a binary PLY point cloud

@@ -93,6 +93,20 @@ public:
     {
         check(reyn_particles_download(h_, xx, xy, xz, vx, vy, vz, m, s));
     }
+    // Particles::reorder (particles.cu:93-113): device permutation of n entries
+    void reorder(const uint32_t* sorted, cudaStream_t s = nullptr)
+    {
+        check(reyn_particles_reorder(h_, sorted, s));
+    }
+    // resize_truncate / resize_uninit (particles.cu:35-91); new particles are zero
+    void resize_truncate(uint32_t N, cudaStream_t s = nullptr)
+    {
+        check(reyn_particles_resize(h_, N, 1, s));
+    }
+    void resize_uninit(uint32_t N, cudaStream_t s = nullptr)
+    {
+        check(reyn_particles_resize(h_, N, 0, s));
+    }
     reyn_particles* handle() { return h_; }
 
 private:

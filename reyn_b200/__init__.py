@@ -101,6 +101,8 @@ _SIGNATURES = {
     "reyn_particles_create": [_u32, _f, ctypes.POINTER(_vp)],
     "reyn_particles_destroy": [_vp],
     "reyn_particles_soa": [_vp, ctypes.POINTER(Soa)],
+    "reyn_particles_reorder": [_vp, _vp, _vp],
+    "reyn_particles_resize": [_vp, _u32, ctypes.c_int, _vp],
     "reyn_particles_upload": [_vp] + [_vp] * 7 + [_vp],
     "reyn_particles_download": [_vp] + [_vp] * 7 + [_vp],
     "reyn_grid_create": [_f * 3, _f * 3, _f, _f, ctypes.c_int, ctypes.POINTER(_vp)],
@@ -261,6 +263,16 @@ class Particles:
         check(lib().reyn_particles_upload(self.h, *ptrs, _stream(stream)))
         import torch
         torch.cuda.synchronize()
+
+    def reorder(self, sorted_, stream=None) -> None:
+        """Particles::reorder by a device permutation (uint32/int32 tensor):
+        new[i] = old[sorted_[i]]; checked to be a permutation first."""
+        check(lib().reyn_particles_reorder(self.h, _ptr(sorted_), _stream(stream)))
+
+    def resize(self, n: int, keep: bool = True, stream=None) -> None:
+        """resize_truncate (keep) / resize_uninit: new particles are zero."""
+        check(lib().reyn_particles_resize(self.h, n, int(keep), _stream(stream)))
+        self.n = n
 
     def download(self, stream=None) -> dict:
         out = {k: np.empty(self.n, np.float32) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}

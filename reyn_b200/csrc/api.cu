@@ -125,6 +125,22 @@ int reyn_particles_upload(reyn_particles* p, const float* xx, const float* xy, c
     });
 }
 
+int reyn_particles_reorder(reyn_particles* p, const uint32_t* sorted, void* stream)
+{
+    return guard([&] {
+        require(p != nullptr, "null particles");
+        reorder_by(*p, sorted, as_stream(stream));
+    });
+}
+
+int reyn_particles_resize(reyn_particles* p, uint32_t n, int keep, void* stream)
+{
+    return guard([&] {
+        require(p != nullptr, "null particles");
+        resize_state(*p, n, keep != 0, as_stream(stream));
+    });
+}
+
 int reyn_particles_download(reyn_particles* p, float* xx, float* xy, float* xz, float* vx,
     float* vy, float* vz, float* m, void* stream)
 {

@@ -220,6 +220,12 @@ void kernel_eval(int kind, float h_bar, const float* dx, const float* dy,
     const float* dz, uint32_t n, float* w, float* gx, float* gy, float* gz,
     cudaStream_t s);
 
+// Particles::reorder (particles.cu:93-113) by a caller's permutation, which
+// is checked first (synchronises); the state is unchanged when it fails
+void reorder_by(reyn_particles& st, const uint32_t* sorted, cudaStream_t s);
+// resize_truncate / resize_uninit (particles.cu:35-91): keep the first
+// min(old, n) particles or none; the others are zero
+void resize_state(reyn_particles& st, uint32_t n, bool keep, cudaStream_t s);
 // (x, y, z, m) of point order[s] (s when order is null) into pts[s]
 void pack_positions(uint32_t n, const uint32_t* order, const float* x, const float* y,
     const float* z, const float* m, float4* pts, cudaStream_t s);

@@ -499,6 +499,90 @@ void reorder_state(reyn_particles& st, Grid& g, float* const* extra, uint32_t n_
     g.reorder_epoch = st.epoch;
 }
 
+// a caller's permutation, checked before it is applied: bit 0 of `bad` for
+// an index >= n, bit 1 for an index seen twice (`seen` holds n bits, zeroed)
+__global__ void k_check_perm(uint32_t n, const uint32_t* __restrict__ perm,
+    uint32_t* __restrict__ seen, uint32_t* __restrict__ bad)
+{
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n)
+        return;
+    const uint32_t p = perm[s];
+    if (p >= n) {
+        atomicOr(bad, 1u);
+        return;
+    }
+    const uint32_t bit = 1u << (p & 31u);
+    if (atomicOr(seen + (p >> 5), bit) & bit)
+        atomicOr(bad, 2u);
+}
+
+void reorder_by(reyn_particles& st, const uint32_t* sorted, cudaStream_t s)
+{
+    const uint32_t n = st.n;
+    if (!n)
+        return;
+    require(sorted != nullptr, "null permutation");
+    {
+        DevArray<uint32_t> seen((n + 31) / 32 + 1); // last word: the error bits
+        seen.zero(s);
+        uint32_t* bad = seen.get() + (n + 31) / 32;
+        REYN_KERNEL("k_check_perm", s,
+            k_check_perm<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, sorted, seen.get(), bad));
+        uint32_t host = 0;
+        REYN_CUDA(cudaMemcpyAsync(&host, bad, sizeof(host), cudaMemcpyDeviceToHost, s));
+        REYN_CUDA(cudaStreamSynchronize(s));
+        if (host)
+            fail(REYN_ERR_INVALID, (host & 1u) ? "permutation index out of range"
+                                               : "permutation repeats an index");
+    }
+    for (auto& a : st.alt)
+        a.resize(n);
+    st.pm.resize(n);
+    st.vel.resize(n);
+    GatherArgs a {};
+    a.count = NFIELDS;
+    for (int k = 0; k < NFIELDS; ++k) {
+        a.src[k] = st.cur[k].get();
+        a.dst[k] = st.alt[k].get();
+    }
+    a.pm = st.pm.get();
+    a.vel = st.vel.get();
+    launch_gather(n, sorted, a, s);
+    for (int k = 0; k < NFIELDS; ++k)
+        st.cur[k].swap(st.alt[k]);
+    st.packed_valid = true;
+    st.epoch += 1;
+    st.version += 1;
+}
+
+void resize_state(reyn_particles& st, uint32_t n, bool keep, cudaStream_t s)
+{
+    const uint32_t m = keep ? std::min(st.n, n) : 0u;
+    // every new array first: a failed allocation leaves the state as it was
+    std::array<DevArray<float>, NFIELDS> fresh;
+    for (auto& a : fresh)
+        a.resize(n);
+    for (int k = 0; k < NFIELDS; ++k) {
+        if (m)
+            REYN_CUDA(cudaMemcpyAsync(fresh[k].get(), st.cur[k].get(), size_t(m) * sizeof(float),
+                cudaMemcpyDeviceToDevice, s));
+        if (n > m)
+            REYN_CUDA(cudaMemsetAsync(fresh[k].get() + m, 0, size_t(n - m) * sizeof(float), s));
+    }
+    REYN_CUDA(cudaStreamSynchronize(s)); // the old arrays are freed below
+    for (int k = 0; k < NFIELDS; ++k) {
+        st.cur[k] = std::move(fresh[k]);
+        st.alt[k] = DevArray<float>();
+    }
+    st.pm = DevArray<float4>();
+    st.vel = DevArray<float4>();
+    st.n = n;
+    st.packed_valid = false;
+    st.epoch += 1;
+    st.version += 1;
+}
+
 // ---- kernel evaluation -------------------------------------------------------
 
 // Kernel::operator() and Kernel::nabla (kernels.cuh:40-64) for arbitrary

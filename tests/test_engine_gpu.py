@@ -395,3 +395,62 @@ def test_fp64_diagnostics(cuda):
     np.testing.assert_allclose(d["momentum"], (m[:, None] * v).sum(0), rtol=1e-10, atol=1e-14)
     assert abs(d["kinetic"] - 0.5 * (m * (v * v).sum(1)).sum()) <= 1e-10 * d["kinetic"]
     st.close()
+
+
+def test_particles_reorder_by_permutation(cuda):
+    """Particles::reorder (particles.cu:93-113) by a caller's permutation:
+    every attribute gathered; a non-permutation is rejected before the state
+    changes."""
+    import torch
+
+    import reyn_b200 as rb
+    rng = np.random.default_rng(3)
+    n = 10_001
+    host = {k: rng.random(n, dtype=np.float32) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    st = rb.Particles(n, 1000.0)
+    st.upload(host)
+    perm = rng.permutation(n).astype(np.int32)
+    st.reorder(torch.tensor(perm, device="cuda"))
+    got = st.download()
+    for k in host:
+        np.testing.assert_array_equal(got[k], host[k][perm], err_msg=k)
+    for bad in (np.concatenate([perm[:-1], [n]]), np.concatenate([perm[:-1], perm[:1]])):
+        with pytest.raises(rb.ReynError) as e:
+            st.reorder(torch.tensor(bad.astype(np.int32), device="cuda"))
+        assert e.value.code == rb.ERR_INVALID
+        again = st.download()
+        for k in host:
+            np.testing.assert_array_equal(again[k], host[k][perm], err_msg=k)
+    st.close()
+
+
+def test_particles_resize(cuda):
+    """resize_truncate keeps the first min(old, new) particles; resize_uninit
+    keeps none; new particles are zero; a solver for the old count rejects
+    the resized state."""
+    import reyn_b200 as rb
+    rng = np.random.default_rng(4)
+    n = 5000
+    host = {k: rng.random(n, dtype=np.float32) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    st = rb.Particles(n, 1000.0)
+    st.upload(host)
+    sv = rb.Solver(rb.SESPH, rb.reference_params(rb.SESPH, rb.B3, 0.02, 1000.0, 0.01), n)
+    st.resize(3000, keep=True)
+    got = st.download()
+    for k in host:
+        np.testing.assert_array_equal(got[k], host[k][:3000], err_msg=k)
+    st.resize(7000, keep=True)
+    got = st.download()
+    for k in host:
+        np.testing.assert_array_equal(got[k][:3000], host[k][:3000], err_msg=k)
+        assert not got[k][3000:].any()
+    grid = rb.Grid((0, 0, 0), (1, 1, 1), 0.04)
+    grid.construct_and_reorder(st)
+    with pytest.raises(rb.ReynError) as e:
+        sv.step(st, grid, None, 1e-3)
+    assert e.value.code == rb.ERR_INVALID
+    st.resize(100, keep=False)
+    got = st.download()
+    assert all(not got[k].any() for k in host) and got["x"].size == 100
+    for o in (grid, sv, st):
+        o.close()
