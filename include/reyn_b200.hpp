@@ -27,6 +27,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -120,20 +121,103 @@ private:
 };
 
 // ---- UniformGrid<R> (uniformgrid.cuh:84-179) --------------------------------
+// A POD passed by value to the caller's own kernels, as the reference's is:
+// in nvcc-compiled code ff_nbrs maps over the neighbours of a point and
+// reduces, like the reference's UniformGrid<R>::ff_nbrs.
 template <Resort R> struct UniformGrid {
     reyn_grid_info info;
     const reyn_grid* grid;
+
+#ifdef __CUDACC__
+    // Resort::yes: the arrays are in grid order; Resort::no: the grid's
+    // permutation maps a sorted slot to the caller's index
+    __device__ uint32_t sorted_lookup(uint32_t index) const
+    {
+        if constexpr (R == Resort::yes)
+            return index;
+        else
+            return info.sorted[index];
+    }
+
+    template <class MapOp>
+    using AccType = std::invoke_result_t<MapOp, const uint32_t, const float3, const float>;
+
+    // acc += map(j, x_i - x_j, |x_i - x_j|^2) for every j (self included)
+    // with |x_i - x_j|^2 <= r^2, over the (2 range + 1)^2 rows of cells
+    // around x_i in z, then y, then x order. xx, xy, xz are the arrays the
+    // grid was built over. Unlike the reference (whose traversal has no
+    // checks), a point outside the grid's searchable interior is mapped to
+    // the nearest interior cell, so no access leaves the grid.
+    template <class MapOp>
+    __device__ AccType<MapOp> ff_nbrs(const float3 x_i, const float* __restrict__ xx,
+        const float* __restrict__ xy, const float* __restrict__ xz, MapOp map,
+        AccType<MapOp> initial_value = AccType<MapOp> {}) const
+    {
+        AccType<MapOp> acc { initial_value };
+        const int rg = info.range;
+        // _index3 (uniformgrid.cuh:17-22)
+        int cx = (int)floorf((x_i.x - info.bound_min[0]) / info.cell_size);
+        int cy = (int)floorf((x_i.y - info.bound_min[1]) / info.cell_size);
+        int cz = (int)floorf((x_i.z - info.bound_min[2]) / info.cell_size);
+        cx = min(max(cx, rg), info.nx - 1 - rg);
+        cy = min(max(cy, rg), info.ny - 1 - rg);
+        cz = min(max(cz, rg), info.nz - 1 - rg);
+        const bool zorder = info.order == REYN_ORDER_ZORDER;
+        const int tx = (info.nx + 31) / 32, txy = tx * ((info.ny + 31) / 32);
+        for (int z = cz - rg; z <= cz + rg; ++z)
+            for (int y = cy - rg; y <= cy + rg; ++y) {
+                // one run of cells in XYZ order; in Z-order the cells of a
+                // row are contiguous within each 4-cell brick
+                for (int x = cx - rg; x <= cx + rg;) {
+                    const int xe = zorder ? min(cx + rg, x | 3) : cx + rg;
+                    const uint32_t k = zorder ? zorder_cell(tx, txy, x, y, z)
+                                              : uint32_t(z) * uint32_t(info.nxny)
+                            + uint32_t(y) * uint32_t(info.nx) + uint32_t(x);
+                    const uint32_t end = info.prefix[k + uint32_t(xe - x + 1)];
+                    for (uint32_t j = info.prefix[k]; j < end; ++j) {
+                        const uint32_t s_j = sorted_lookup(j);
+                        const float3 x_ij = make_float3(x_i.x - xx[s_j], x_i.y - xy[s_j],
+                            x_i.z - xz[s_j]);
+                        // the engine's |x_ij|^2, so that both prune alike
+                        const float l2 = fmaf(x_ij.x, x_ij.x, fmaf(x_ij.y, x_ij.y,
+                            x_ij.z * x_ij.z));
+                        if (l2 <= info.r_c_2)
+                            acc += map(s_j, x_ij, l2);
+                    }
+                    x = xe + 1;
+                }
+            }
+        return acc;
+    }
+
+private:
+    // the engine's Z-order cell key: 4x4x4 bricks (x fastest) on the Morton
+    // curve inside 32^3-cell tiles, tiles in XYZ order
+    __device__ static uint32_t spread3(uint32_t v)
+    {
+        return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4);
+    }
+    __device__ static uint32_t zorder_cell(int tx, int txy, int cx, int cy, int cz)
+    {
+        const uint32_t tile = uint32_t(cz >> 5) * uint32_t(txy) + uint32_t(cy >> 5) * uint32_t(tx)
+            + uint32_t(cx >> 5);
+        const uint32_t brick = spread3(uint32_t(cx >> 2) & 7u)
+            | (spread3(uint32_t(cy >> 2) & 7u) << 1) | (spread3(uint32_t(cz >> 2) & 7u) << 2);
+        const uint32_t local = uint32_t(cx & 3) | (uint32_t(cy & 3) << 2) | (uint32_t(cz & 3) << 4);
+        return (((tile << 9) | brick) << 6) | local;
+    }
+#endif
 };
 
 // ---- UniformGridBuilder (uniformgrid.cuh:200-489) ---------------------------
 class UniformGridBuilder {
 public:
     UniformGridBuilder(float3 bound_min, float3 bound_max, float search_radius,
-        float cell_ratio = 0.5f)
+        float cell_ratio = 0.5f, reyn_cell_order order = REYN_ORDER_XYZ)
     {
         const float lo[3] = { bound_min.x, bound_min.y, bound_min.z };
         const float hi[3] = { bound_max.x, bound_max.y, bound_max.z };
-        check(reyn_grid_create(lo, hi, search_radius, cell_ratio, REYN_ORDER_XYZ, &g_));
+        check(reyn_grid_create(lo, hi, search_radius, cell_ratio, order, &g_));
     }
     ~UniformGridBuilder() { reyn_grid_destroy(g_); }
     UniformGridBuilder(const UniformGridBuilder&) = delete;

@@ -150,3 +150,20 @@ def test_cpp_mesh_adapters(cuda, tmp_path):
     assert float(last[1]) < float(first[1])       # max/min number density ratio falls
     assert float(out[3]) < 1e-5                    # every sample on the surface
     assert float(out[4]) == pytest.approx(4.0 / 3.0, rel=1e-12)
+
+
+@pytest.mark.parametrize("order,ratio", [("xyz", "0.5"), ("xyz", "1.0"), ("zorder", "0.5")])
+def test_cpp_user_kernel_ff_nbrs(cuda, tmp_path, order, ratio):
+    """UniformGrid<R>::ff_nbrs from a user kernel (tests/cpp/ff_nbrs.cu),
+    Resort::no and Resort::yes: neighbour counts exactly and |x_ij|^2 sums
+    within 1e-5 of the engine's neighbour statistics."""
+    exe = os.path.join(str(tmp_path), "ff_nbrs")
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    subprocess.run([nvcc, "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a",
+                    "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "ff_nbrs.cu"),
+                    "-L" + os.path.join(ROOT, "reyn_b200"), "-lreyn_b200",
+                    "-Xlinker", "-rpath," + os.path.join(ROOT, "reyn_b200"), "-o", exe],
+                   check=True)
+    r = subprocess.run([exe, order, ratio], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
