@@ -239,6 +239,11 @@ int reyn_boundary_create_batched(const float* bx, const float* by,
 int reyn_boundary_arrays(const reyn_boundary* b, const float** bx,
     const float** by, const float** bz, const float** bm, uint32_t* nb);
 
+/* BoundarySamples::bound_min / bound_max (scene.cuh:35-36): the smallest
+ * box holding every sample (zeros without samples) */
+int reyn_boundary_bounds(const reyn_boundary* b, float bound_min[3],
+    float bound_max[3]);
+
 /* compute_densities<K, R> (solver.cuh:19-38): rho_i = sum_j m_j W(x_ij) over
  * the fluid neighbours within the grid's radius r (self included) plus
  * sum_b m_b W(x_ib) over the boundary samples (bdy may be NULL), `kernel` at
@@ -488,6 +493,13 @@ int reyn_scene_box_walls(const float bound_min[3], const float bound_max[3],
 int reyn_scene_sphere(const float center[3], float radius, float spacing,
     float* x, float* y, float* z, uint32_t capacity, uint32_t* count,
     void* stream);
+/* jitter_positions (scene.cu:232-253): particles first .. first + count - 1
+ * move by a uniform [-amplitude, amplitude] per axis from the counter-based
+ * streams 0..2 keyed by the particle index (the fluid blocks' jitter). The
+ * reference draws normal jitter of standard deviation sigma; amplitude
+ * sqrt(3) sigma gives the same standard deviation. */
+int reyn_scene_jitter(reyn_particles* p, uint32_t first, uint32_t count,
+    float amplitude, uint64_t seed, void* stream);
 /* the reference's cull of fluid particles too close to the boundary
  * (CullPredicate + remove_if, scene.cu:59-83, 176-205): removes, keeping the
  * order of the rest, every particle with a boundary sample within `radius`

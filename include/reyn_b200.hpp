@@ -24,6 +24,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -283,11 +285,28 @@ public:
         check(reyn_boundary_create(xs, ys, zs, m, nb, h, rho0, mass_iters, s, &b_));
     }
     ~BoundarySamples() { reyn_boundary_destroy(b_); }
+    BoundarySamples(BoundarySamples&& o) noexcept : b_(std::exchange(o.b_, nullptr)) { }
     BoundarySamples(const BoundarySamples&) = delete;
     BoundarySamples& operator=(const BoundarySamples&) = delete;
     const reyn_boundary* handle() const { return b_; }
+    // bound_min / bound_max (scene.cuh:35-36): the samples' bounds
+    float3 bound_min() const { return bounds().first; }
+    float3 bound_max() const { return bounds().second; }
+    uint32_t size() const
+    {
+        const float *x, *y, *z, *m;
+        uint32_t nb = 0;
+        check(reyn_boundary_arrays(b_, &x, &y, &z, &m, &nb));
+        return nb;
+    }
 
 private:
+    std::pair<float3, float3> bounds() const
+    {
+        float lo[3], hi[3];
+        check(reyn_boundary_bounds(b_, lo, hi));
+        return { make_float3(lo[0], lo[1], lo[2]), make_float3(hi[0], hi[1], hi[2]) };
+    }
     reyn_boundary* b_ = nullptr;
 };
 
@@ -607,6 +626,150 @@ void relax_sampling(float* xs, float* ys, float* zs, uint32_t n, const DeviceMes
         for (uint32_t i = 0; i < relaxation_iters; ++i)
             (*debug_stream) << i + 1 << "," << st[2 * i] << "," << st[2 * i + 1] << "\n";
 }
+
+// sample_mesh (sample_boundary.cu:391-439; defaults of sample_boundary.cuh:
+// 160-163): uniform samples at h / oversampling_factor, relaxed, then the
+// boundary with its grid at support 2h and Akinci masses
+inline BoundarySamples sample_mesh(const DeviceMesh& mesh, float h, float rho0,
+    float oversampling_factor = 2.f, uint32_t relaxation_iters = 50,
+    float relaxation_factor = 1.f, uint32_t mass_refinement_iterations = 5,
+    uint64_t seed = 1614201312, cudaStream_t s = nullptr)
+{
+    const uint32_t n = uniform_sample_mesh(nullptr, nullptr, nullptr, 0, mesh, h,
+        oversampling_factor, seed, s);
+    float* d = nullptr;
+    if (cudaMalloc(&d, 3 * sizeof(float) * std::max<size_t>(n, 1)) != cudaSuccess)
+        throw Error(REYN_ERR_ALLOC, "sample_mesh: cudaMalloc");
+    struct Free {
+        float* p;
+        ~Free() { cudaFree(p); }
+    } guard { d };
+    uniform_sample_mesh(d, d + n, d + 2 * size_t(n), n, mesh, h, oversampling_factor, seed, s);
+    if (relaxation_iters > 0)
+        check(reyn_mesh_relax(mesh.handle(), d, d + n, d + 2 * size_t(n), n,
+            h / oversampling_factor, relaxation_factor, relaxation_iters, nullptr, nullptr, s));
+    return BoundarySamples(d, d + n, d + 2 * size_t(n), nullptr, n, h, rho0,
+        mass_refinement_iterations, s);
+}
+
+// ---- Scene (scene.cuh:48-157, scene.cu:255-464) ---------------------------------
+// The reference's scene set-up on the engine's kernels. Differences: the
+// temporary buffers of the reference's signatures are the engine's own; the
+// fluid jitter is uniform with the reference's standard deviation
+// (counter-based, seeded) where the reference draws normal jitter.
+class Scene {
+public:
+    float rho0; // the reference's ρ₀
+    const float h;
+    uint32_t N;
+    const BoundarySamples bdy;
+    float3 bound_min;
+    float3 bound_max;
+
+    // a box [min, max) of fluid at close to N_desired particles inside the
+    // boundary the OBJ file's shapes not named "fluid" describe (scene.cu:255-314)
+    Scene(const std::string& path, uint32_t N_desired, float3 min, float3 max, float rho0_,
+        Particles& state, float bdy_oversampling_factor = 2.f, float cull_bdy_radius = 1.f,
+        float jitter_stddev = 0.01f, uint64_t seed = 1)
+        : rho0(rho0_)
+        , h(cbrtf((max.x - min.x) * (max.y - min.y) * (max.z - min.z) / float(N_desired)))
+        , N(0)
+        , bdy(sample_mesh(DeviceMesh::from_obj(path, { "fluid" }), h, rho0_,
+              bdy_oversampling_factor))
+        , bound_min(bdy.bound_min())
+        , bound_max(bdy.bound_max())
+        , grid_builder_(bound_min, bound_max, 2.f * h)
+    {
+        const int nx = (int)floorf((max.x - min.x) / h), ny = (int)floorf((max.y - min.y) / h),
+                  nz = (int)floorf((max.z - min.z) / h);
+        const uint64_t n = uint64_t(std::abs(nx)) * uint64_t(std::abs(ny)) * uint64_t(std::abs(nz));
+        if (n == 0)
+            throw std::domain_error("Initialization of box failed, zero particles placed");
+        if (n > UINT32_MAX)
+            throw Error(REYN_ERR_INVALID, "too many particles for one state");
+        state.resize_uninit(uint32_t(n));
+        const uint32_t counts[3] = { uint32_t(std::abs(nx)), uint32_t(std::abs(ny)),
+            uint32_t(std::abs(nz)) };
+        const float origin[3] = { min.x, min.y, min.z };
+        check(reyn_scene_fluid_block(state.handle(), 0, counts, origin, h, rho0 * h * h * h, 0.f,
+            0.f, seed, nullptr));
+        N = cull_and_jitter(state, bdy, uint32_t(n), h, cull_bdy_radius, jitter_stddev, seed);
+    }
+
+    // Scene::from_obj (scene.cu:316-464): the watertight shape named "fluid"
+    // filled at spacing h = cbrt(volume / N_desired), the other shapes sampled
+    // as the boundary, the bounds grown to hold the fluid with h / 2 to spare
+    static Scene from_obj(const std::string& path, uint32_t N_desired, float rho0,
+        Particles& state, float bdy_oversampling_factor = 2.f, float cull_bdy_radius = 1.f,
+        float jitter_stddev = 0.01f, uint64_t seed = 1)
+    {
+        const DeviceMesh fluid = DeviceMesh::from_obj(path, {}, "fluid");
+        const reyn_mesh_info fi = fluid.info();
+        const float h = static_cast<float>(std::cbrt(fi.volume / double(N_desired)));
+        BoundarySamples bdy = sample_mesh(DeviceMesh::from_obj(path, { "fluid" }), h, rho0,
+            bdy_oversampling_factor);
+        const float e = 0.5f * h;
+        const float3 blo = bdy.bound_min(), bhi = bdy.bound_max();
+        const float3 lo = make_float3(std::min(blo.x, float(fi.bounds_min[0]) - e),
+            std::min(blo.y, float(fi.bounds_min[1]) - e), std::min(blo.z, float(fi.bounds_min[2]) - e));
+        const float3 hi = make_float3(std::max(bhi.x, float(fi.bounds_max[0]) + e),
+            std::max(bhi.y, float(fi.bounds_max[1]) + e), std::max(bhi.z, float(fi.bounds_max[2]) + e));
+        uint32_t n = 0;
+        check(reyn_mesh_fill(fluid.handle(), h, 0.f, seed, nullptr, nullptr, nullptr, 0, &n,
+            nullptr));
+        if (n == 0)
+            throw std::domain_error("Initialization of box failed, zero particles placed");
+        state.resize_uninit(n);
+        const reyn_soa v = state.soa();
+        check(reyn_mesh_fill(fluid.handle(), h, 0.f, seed, v.xx, v.xy, v.xz, n, &n, nullptr));
+        const std::vector<float> m(n, rho0 * h * h * h);
+        state.upload(nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, m.data());
+        n = cull_and_jitter(state, bdy, n, h, cull_bdy_radius, jitter_stddev, seed);
+        return Scene(rho0, h, n, std::move(bdy), lo, hi);
+    }
+
+    // hard_enforce_bounds (scene.cu:485-491)
+    void hard_enforce_bounds(Particles& state, cudaStream_t s = nullptr) const
+    {
+        const float lo[3] = { bound_min.x, bound_min.y, bound_min.z };
+        const float hi[3] = { bound_max.x, bound_max.y, bound_max.z };
+        check(reyn_enforce_bounds(state.handle(), lo, hi, s));
+    }
+
+    // get_grid (scene.cuh:150-157): construct_and_reorder at search_radius h
+    template <class... Extra>
+    UniformGrid<Resort::yes> get_grid(Particles& state, float search_radius = 2.f,
+        Extra*... reorder)
+    {
+        return grid_builder_.construct_and_reorder(search_radius * h, state, reorder...);
+    }
+
+private:
+    Scene(float rho0_, float h_, uint32_t n, BoundarySamples&& b, float3 lo, float3 hi)
+        : rho0(rho0_)
+        , h(h_)
+        , N(n)
+        , bdy(std::move(b))
+        , bound_min(lo)
+        , bound_max(hi)
+        , grid_builder_(bound_min, bound_max, 2.f * h)
+    {
+    }
+    // cull fluid within cull_bdy_radius h of the boundary (scene.cu:59-83,
+    // 176-205), then jitter (scene.cu:232-253); returns the count left
+    static uint32_t cull_and_jitter(Particles& state, const BoundarySamples& b, uint32_t n,
+        float h, float cull_bdy_radius, float jitter_stddev, uint64_t seed)
+    {
+        if (cull_bdy_radius > 0.f)
+            check(reyn_scene_cull(state.handle(), b.handle(), cull_bdy_radius * h, &n, nullptr));
+        check(reyn_scene_jitter(state.handle(), 0, n, 1.7320508f * jitter_stddev * h, seed,
+            nullptr));
+        if (cudaDeviceSynchronize() != cudaSuccess)
+            throw Error(REYN_ERR_CUDA, "scene set-up failed");
+        return n;
+    }
+    UniformGridBuilder grid_builder_;
+};
 
 } // namespace reyn
 

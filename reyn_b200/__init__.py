@@ -103,6 +103,8 @@ _SIGNATURES = {
     "reyn_particles_soa": [_vp, ctypes.POINTER(Soa)],
     "reyn_particles_reorder": [_vp, _vp, _vp],
     "reyn_particles_resize": [_vp, _u32, ctypes.c_int, _vp],
+    "reyn_boundary_bounds": [_vp, _vp, _vp],
+    "reyn_scene_jitter": [_vp, _u32, _u32, _f, ctypes.c_uint64, _vp],
     "reyn_particles_upload": [_vp] + [_vp] * 7 + [_vp],
     "reyn_particles_download": [_vp] + [_vp] * 7 + [_vp],
     "reyn_grid_create": [_f * 3, _f * 3, _f, _f, ctypes.c_int, ctypes.POINTER(_vp)],
@@ -403,6 +405,12 @@ class Boundary:
         self.h = None
 
     __del__ = close
+
+    def bounds(self):
+        """(bound_min, bound_max) of the samples."""
+        lo, hi = (_f * 3)(), (_f * 3)()
+        check(lib().reyn_boundary_bounds(self.h, lo, hi))
+        return tuple(lo), tuple(hi)
 
     def arrays(self):
         """(x, y, z, m) device pointers of the reordered samples."""
@@ -729,6 +737,14 @@ def scene_sphere(center, radius: float, spacing: float, stream=None):
     check(lib().reyn_scene_sphere(_f3(center), radius, spacing, x.data_ptr(), y.data_ptr(),
                                   z.data_ptr(), cnt.value, ctypes.byref(cnt), _stream(stream)))
     return x[:cnt.value], y[:cnt.value], z[:cnt.value]
+
+
+def scene_jitter(state: Particles, amplitude: float, seed: int = 1, first: int = 0,
+                 count: Optional[int] = None, stream=None) -> None:
+    """jitter_positions: uniform [-amplitude, amplitude] per axis, keyed by
+    the particle index (sqrt(3) sigma matches the reference's normal sigma)."""
+    n = state.n - first if count is None else count
+    check(lib().reyn_scene_jitter(state.h, first, n, amplitude, seed, _stream(stream)))
 
 
 def scene_cull(state: Particles, bdy: Boundary, radius: float, stream=None) -> int:

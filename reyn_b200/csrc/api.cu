@@ -352,6 +352,17 @@ int reyn_boundary_destroy(reyn_boundary* b)
     return guard([&] { delete b; });
 }
 
+int reyn_boundary_bounds(const reyn_boundary* b, float bound_min[3], float bound_max[3])
+{
+    return guard([&] {
+        require(b && bound_min && bound_max, "null argument");
+        for (int a = 0; a < 3; ++a) {
+            bound_min[a] = b->lo[a];
+            bound_max[a] = b->hi[a];
+        }
+    });
+}
+
 int reyn_boundary_arrays(const reyn_boundary* b, const float** bx, const float** by,
     const float** bz, const float** bm, uint32_t* nb)
 {

@@ -134,6 +134,7 @@ struct reyn_grid : reyn::Grid { };
 struct reyn_boundary {
     uint32_t nb = 0;
     float h = 0.f;
+    float lo[3] = { 0.f, 0.f, 0.f }, hi[3] = { 0.f, 0.f, 0.f }; // the samples' bounds
     reyn::Grid grid;
     reyn::DevArray<float> x, y, z, m;
     reyn::DevArray<float4> pm;

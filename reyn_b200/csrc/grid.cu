@@ -820,6 +820,8 @@ void boundary_build(reyn_boundary& b, const float* bx, const float* by, const fl
     for (int a = 0; a < 3; ++a) {
         lo[a] = from_ordered_bits(hb[a]);
         hi[a] = from_ordered_bits(hb[3 + a]);
+        b.lo[a] = lo[a];
+        b.hi[a] = hi[a];
     }
     // the boundary grid: support 2h over the samples' own bounds, reference
     // geometry (sample_boundary.cu:420-428)

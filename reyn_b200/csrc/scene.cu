@@ -163,9 +163,42 @@ __global__ void k_cull_scatter(uint32_t n, const uint32_t* __restrict__ keep,
         a.dst[k][o] = a.src[k][i];
 }
 
+// jitter_positions (scene.cu:232-253) with the counter-based streams 0..2 of
+// the fluid blocks: particle q of [first, first + count) moves by a uniform
+// [-a, a] per axis, keyed by its index
+__global__ void k_jitter(uint32_t count, uint32_t first, float a, uint64_t seed,
+    float* __restrict__ x, float* __restrict__ y, float* __restrict__ z)
+{
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= count)
+        return;
+    const uint32_t o = first + q;
+    x[o] = __fadd_rn(x[o], symmetric(uniform01(seed, 0, o), a));
+    y[o] = __fadd_rn(y[o], symmetric(uniform01(seed, 1, o), a));
+    z[o] = __fadd_rn(z[o], symmetric(uniform01(seed, 2, o), a));
+}
+
 } // namespace reyn
 
 using namespace reyn;
+
+extern "C" int reyn_scene_jitter(reyn_particles* p, uint32_t first, uint32_t count,
+    float amplitude, uint64_t seed, void* stream)
+{
+    return guard([&] {
+        require(p != nullptr, "null particles");
+        require(amplitude >= 0.f && std::isfinite(amplitude), "amplitude must be >= 0");
+        require(uint64_t(first) + count <= p->n, "range does not fit the particle state");
+        if (!count || amplitude == 0.f)
+            return;
+        const cudaStream_t s = as_stream(stream);
+        REYN_KERNEL("k_jitter", s,
+            k_jitter<<<blocks_for(count, THREADS), THREADS, 0, s>>>(count, first, amplitude,
+            seed, p->cur[FX].get(), p->cur[FY].get(), p->cur[FZ].get()));
+        p->packed_valid = false;
+        p->version += 1;
+    });
+}
 
 extern "C" int reyn_scene_fluid_block(reyn_particles* p, uint32_t first, const uint32_t counts[3],
     const float origin[3], float spacing, float mass, float jitter, float velocity_noise,

@@ -167,3 +167,99 @@ def test_cpp_user_kernel_ff_nbrs(cuda, tmp_path, order, ratio):
                    check=True)
     r = subprocess.run([exe, order, ratio], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def _scene_obj(path):
+    """A container (shape "walls") with a fluid block (shape "fluid") inside."""
+    from reyn_b200 import meshes
+    walls = meshes.box((0.0, 0.0, 0.0), (1.0, 0.6, 0.6), 2)
+    fluid = meshes.box((0.05, 0.05, 0.05), (0.45, 0.4, 0.4), 1)
+    meshes.write_obj(path, [("walls", *walls), ("fluid", *fluid)])
+    return walls, fluid
+
+
+def _read_scene(path):
+    raw = open(path, "rb").read()
+    n, nb, steps = struct.unpack("<3I", raw[:12])
+    geo = np.frombuffer(raw[12:40], np.float32)
+    off = 40
+    arr = np.frombuffer(raw[off:off + 4 * 3 * n], np.float32).reshape(3, n)
+    off += 12 * n
+    bdy = np.frombuffer(raw[off:off + 12 * nb], np.float32).reshape(3, nb)
+    off += 12 * nb
+    iters = np.frombuffer(raw[off:off + 4 * steps], np.uint32)
+    off += 4 * steps
+    fin = np.frombuffer(raw[off:], np.float32).reshape(3, n)
+    return n, float(geo[0]), geo[1:4], geo[4:7], arr.T, bdy.T, iters, fin.T
+
+
+def _compile_scene_loop(tmp):
+    exe = os.path.join(tmp, "scene_loop")
+    cxx = shutil.which("g++") or "g++"
+    subprocess.run([cxx, "-std=c++17", "-O2", "-I" + os.path.join(ROOT, "include"),
+                    "-I/usr/local/cuda/include",
+                    os.path.join(ROOT, "tests", "cpp", "scene_loop.cpp"),
+                    "-L" + os.path.join(ROOT, "reyn_b200"), "-lreyn_b200",
+                    "-L/usr/local/cuda/lib64", "-lcudart",
+                    "-Wl,-rpath," + os.path.join(ROOT, "reyn_b200"), "-o", exe], check=True)
+    return exe
+
+
+@pytest.mark.parametrize("mode", ["obj", "box"])
+def test_cpp_scene_main_loop(cuda, tmp_path, mode):
+    """The reference's main loop with its Scene (Scene::from_obj, or the box
+    constructor), oversampling 3 and cull radius 1h as main.cu:43-44 has it:
+    spacing from the fluid volume (or the box) and the desired count, the
+    fluid lattice filled inside the "fluid" shape, every particle with a
+    boundary sample within h culled, the rest jittered by at most sqrt(3)
+    0.01 h, scene bounds holding boundary and fluid; then IISPH steps keep
+    every particle inside the bounds."""
+    from scipy.spatial import cKDTree
+    exe = _compile_scene_loop(str(tmp_path))
+    obj = os.path.join(str(tmp_path), "scene.obj")
+    walls, fluid = _scene_obj(obj)
+    out = os.path.join(str(tmp_path), "out.bin")
+    n_desired, steps = 20000, 3
+    subprocess.run([exe, obj, out, mode, str(n_desired), str(steps)], check=True)
+    n, h, lo, hi, x0, bdy, iters, x1 = _read_scene(out)
+    if mode == "obj":
+        # the "fluid" shape as loaded: the reference's loader keeps every
+        # vertex of the file, so the mesh's (and its LBVH's) bounds span all
+        # shapes and the fill lattice starts at the file's lowest vertex
+        verts = np.concatenate([np.asarray(walls[0], float), np.asarray(fluid[0], float)])
+        faces = np.asarray(fluid[1], np.int64) + len(walls[0])
+        vol = oracle.mesh_measure(verts, faces)[1]
+        assert h == pytest.approx(float(np.float32(np.cbrt(vol / n_desired))), rel=1e-6)
+        lx, ly, lz = oracle.mesh_fill(verts, faces, h)
+        lat = np.stack([lx, ly, lz], 1)
+        fmin = verts.min(0).astype(np.float32)
+        fmax = verts.max(0).astype(np.float32)
+        np.testing.assert_allclose(lo, np.minimum(bdy.min(0), fmin - np.float32(0.5 * h)),
+                                   rtol=1e-6)
+        np.testing.assert_allclose(hi, np.maximum(bdy.max(0), fmax + np.float32(0.5 * h)),
+                                   rtol=1e-6)
+    else:
+        f32 = np.float32
+        ext = [f32(0.45) - f32(0.05), f32(0.4) - f32(0.05), f32(0.4) - f32(0.05)]
+        assert h == pytest.approx(float(np.cbrt(ext[0] * ext[1] * ext[2] / f32(n_desired))),
+                                  rel=1e-6)
+        cnt = [int(np.floor(e / f32(h))) for e in ext]
+        i, j, k = np.meshgrid(*(np.arange(c) for c in cnt), indexing="ij")
+        lat = np.stack([np.float32(0.05) + i.T.ravel() * np.float32(h),
+                        np.float32(0.05) + j.T.ravel() * np.float32(h),
+                        np.float32(0.05) + k.T.ravel() * np.float32(h)], 1).astype(np.float32)
+        np.testing.assert_array_equal(lo, bdy.min(0))
+        np.testing.assert_array_equal(hi, bdy.max(0))
+    d, _ = cKDTree(bdy.astype(np.float64)).query(lat.astype(np.float64))
+    near = np.abs(d - h) < 1e-5 * h  # ties at the cull radius may go either way
+    kept = d > h
+    assert kept.sum() <= n <= (kept | near).sum()
+    if not near.any():
+        dev = np.abs(x0 - lat[kept])
+        # the amplitude plus the rounding of the jittered coordinate
+        assert dev.max() <= np.sqrt(3.0) * 0.01 * h + 4 * np.finfo(np.float32).eps * np.abs(
+            lat).max()
+        assert dev.max() > 0.5 * 0.01 * h  # jitter applied
+    assert len(iters) == steps and min(iters) >= 3
+    assert np.isfinite(x1).all()
+    assert (x1 >= lo).all() and (x1 <= hi).all()
