@@ -84,6 +84,15 @@ int reyn_particles_soa(reyn_particles* p, reyn_soa* out);
 int reyn_particles_upload(reyn_particles* p, const float* xx, const float* xy,
     const float* xz, const float* vx, const float* vy, const float* vz,
     const float* m, void* stream);
+int reyn_particles_download(reyn_particles* p, float* xx, float* xy,
+    float* xz, float* vx, float* vy, float* vz, float* m, void* stream);
+/* reyn_particles_download without the final synchronisation: the copies are
+ * enqueued on `stream` (asynchronous for page-locked host memory); the host
+ * arrays are valid once the stream has passed this point. Copies of single
+ * fields (the others NULL) on their own streams let a caller overlap the
+ * download of one field with the upload of another. */
+int reyn_particles_download_async(reyn_particles* p, float* xx, float* xy,
+    float* xz, float* vx, float* vy, float* vz, float* m, void* stream);
 /* Particles::reorder(sorted, tmp) (particles.cu:93-113): every attribute
  * gathered by `sorted` (device, n entries: new[i] = old[sorted[i]]). The
  * array must be a permutation of [0, n): it is checked first (the call
@@ -99,8 +108,6 @@ int reyn_particles_reorder(reyn_particles* p, const uint32_t* sorted,
  * arrays at different sizes). Synchronises the stream. */
 int reyn_particles_resize(reyn_particles* p, uint32_t n, int keep,
     void* stream);
-int reyn_particles_download(reyn_particles* p, float* xx, float* xy,
-    float* xz, float* vx, float* vy, float* vz, float* m, void* stream);
 /* save_to_ply (ply_io.cu:7-55): the positions as a binary PLY point cloud
  * (header: format binary_<native>_endian 1.0, element vertex n, float32
  * properties x, y, z; payload x y z per particle). Synchronises the stream. */

@@ -107,6 +107,7 @@ _SIGNATURES = {
     "reyn_scene_jitter": [_vp, _u32, _u32, _f, ctypes.c_uint64, _vp],
     "reyn_particles_upload": [_vp] + [_vp] * 7 + [_vp],
     "reyn_particles_download": [_vp] + [_vp] * 7 + [_vp],
+    "reyn_particles_download_async": [_vp] + [_vp] * 7 + [_vp],
     "reyn_grid_create": [_f * 3, _f * 3, _f, _f, ctypes.c_int, ctypes.POINTER(_vp)],
     "reyn_grid_destroy": [_vp],
     "reyn_grid_construct": [_vp, _f, _vp, _vp, _vp, _u32, _vp],

@@ -141,18 +141,33 @@ int reyn_particles_resize(reyn_particles* p, uint32_t n, int keep, void* stream)
     });
 }
 
+static void download_fields(reyn_particles* p, float* const dst[NFIELDS], cudaStream_t s)
+{
+    for (int k = 0; k < NFIELDS; ++k)
+        if (dst[k] && p->n)
+            REYN_CUDA(cudaMemcpyAsync(dst[k], p->cur[k].get(), size_t(p->n) * sizeof(float),
+                cudaMemcpyDeviceToHost, s));
+}
+
 int reyn_particles_download(reyn_particles* p, float* xx, float* xy, float* xz, float* vx,
     float* vy, float* vz, float* m, void* stream)
 {
     return guard([&] {
         require(p != nullptr, "null particles");
-        float* dst[NFIELDS] = { xx, xy, xz, vx, vy, vz, m };
+        float* const dst[NFIELDS] = { xx, xy, xz, vx, vy, vz, m };
         const cudaStream_t s = as_stream(stream);
-        for (int k = 0; k < NFIELDS; ++k)
-            if (dst[k] && p->n)
-                REYN_CUDA(cudaMemcpyAsync(dst[k], p->cur[k].get(), size_t(p->n) * sizeof(float),
-                    cudaMemcpyDeviceToHost, s));
+        download_fields(p, dst, s);
         REYN_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int reyn_particles_download_async(reyn_particles* p, float* xx, float* xy, float* xz,
+    float* vx, float* vy, float* vz, float* m, void* stream)
+{
+    return guard([&] {
+        require(p != nullptr, "null particles");
+        float* const dst[NFIELDS] = { xx, xy, xz, vx, vy, vz, m };
+        download_fields(p, dst, as_stream(stream));
     });
 }
 
