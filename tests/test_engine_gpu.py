@@ -454,3 +454,27 @@ def test_particles_resize(cuda):
     assert all(not got[k].any() for k in host) and got["x"].size == 100
     for o in (grid, sv, st):
         o.close()
+
+
+def test_particles_download_async_per_field(cuda):
+    """reyn_particles_download_async: single-field copies on a side stream
+    into page-locked memory agree with the synchronous download."""
+    import torch
+
+    import reyn_b200 as rb
+    rng = np.random.default_rng(5)
+    n = 70_001
+    keys = ("x", "y", "z", "vx", "vy", "vz", "m")
+    host = {k: rng.random(n, dtype=np.float32) for k in keys}
+    st = rb.Particles(n, 1000.0)
+    st.upload(host)
+    side = torch.cuda.Stream()
+    out = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in keys]
+    for f in range(7):
+        ptrs = [None] * 7
+        ptrs[f] = out[f].data_ptr()
+        rb.check(rb.lib().reyn_particles_download_async(st.h, *ptrs, side.cuda_stream))
+    side.synchronize()
+    for f, k in enumerate(keys):
+        np.testing.assert_array_equal(out[f].numpy(), host[k], err_msg=k)
+    st.close()
