@@ -366,18 +366,19 @@ def run_engine(a, world, rank, local):
     S = stream.cuda_stream
 
     names = ["fp32", "mixed", "mixed_pos16"] if a.precision == "all" else [a.precision]
-    # the autotuner (block size of the neighbour passes, cell size) on the
-    # headline configuration, from the scene's initial state
-    ratio, block, tuned = 0.5, 0, None
+    # the autotuner (block size of the neighbour passes, cell size) for every
+    # precision, from the scene's initial state
+    config = {name: (0.5, 0, None) for name in names}
     if not a.no_autotune:
         sc = DeviceScene(rank, a.scale)
         bd = rb.Boundary(*sc.walls, None, h=sc.h, rho0=sc.rho0, mass_iters=5)
-        best, pts = rb.autotune(rb.IISPH, EngineRun.params(rb, sc, names[0]), sc.st, bd,
-                                viscous_dt_limit(sc.h, NU), steps=3,
-                                bounds=(sc.box_min, sc.box_max), stream=S)
-        ratio, block = best.cell_ratio, best.block_size
-        tuned = [{"block_size": p.block_size, "cell_ratio": p.cell_ratio,
-                  "ms_per_step": round(p.ms_per_step, 3)} for p in pts]
+        for name in names:
+            best, pts = rb.autotune(rb.IISPH, EngineRun.params(rb, sc, name), sc.st, bd,
+                                    viscous_dt_limit(sc.h, NU), steps=3,
+                                    bounds=(sc.box_min, sc.box_max), stream=S)
+            config[name] = (best.cell_ratio, best.block_size,
+                            [{"block_size": p.block_size, "cell_ratio": p.cell_ratio,
+                              "ms_per_step": round(p.ms_per_step, 3)} for p in pts])
         bd.close()
         sc.st.close()
         torch.cuda.synchronize()
@@ -386,6 +387,7 @@ def run_engine(a, world, rank, local):
     # others are reported beside it), then timed end to end
     results = {}
     for name in names:
+        ratio, block, _ = config[name]
         run = EngineRun(rank, a.scale, dev, name, a.order, ratio, block)
         results[name] = (run, timed_steps(run, a, world, stream, dev))
     headline = min(names, key=lambda k: results[k][1][2])  # ms_max: the same on every rank
@@ -396,6 +398,7 @@ def run_engine(a, world, rank, local):
         r, (_, _, msl, _, clk, logl) = results[name]
         legs[name] = leg_summary(r, a, world, msl, logl)
         legs[name]["clocks"] = clk
+        legs[name]["cell_ratio"], legs[name]["block_size"] = config[name][0], config[name][1]
         r.close()
     torch.cuda.synchronize()
     run, (ck, ms, ms_max, prof, ck_clocks, log) = results[headline]
@@ -500,11 +503,11 @@ def run_engine(a, world, rank, local):
                    "dt": f"min(simple_dt_controller(lambda={LAMBDA}, target 10 iters, "
                          f"0.1%/step) from {DT0}, 0.08 h^2/nu = {run.dt_visc:.2e})",
                    "precision": precision, "cell_order": a.order,
-                   "block_size": block or 128, "cell_ratio": ratio,
+                   "block_size": config[headline][1] or 128, "cell_ratio": config[headline][0],
                    "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (state 4M x 28 B + grid 70 MB per step)"},
         "clocks": ck_clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-        "cpu_baseline": cpu, "autotune": tuned,
+        "cpu_baseline": cpu, "autotune": config[headline][2],
         "iters_per_step": [x[0] for x in log],
         "avg_density_error_per_step": [round(x[1], 7) for x in log],
         "dt_per_step": [float(f"{x[2]:.4e}") for x in log],

@@ -953,8 +953,8 @@ __global__ void __launch_bounds__(MB) k_iisph_diag_pacc(uint32_t n, Fluid f,
 }
 
 // _set_pressure_accelerations (IISPH.cu:68-98)
-template <int KIND, int R, int MIX = 0, bool BATCH = false, int MB = NBR_THREADS>
-__global__ void __launch_bounds__(MB) k_iisph_pacc(uint32_t n, Fluid f,
+template <int KIND, int R, int MIX, bool BATCH>
+__device__ __forceinline__ void iisph_pacc(uint32_t n, const Fluid& f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     float4* __restrict__ acc, uint2* __restrict__ acch_out, const uint32_t* __restrict__ gate)
 {
@@ -988,8 +988,8 @@ __global__ void __launch_bounds__(MB) k_iisph_pacc(uint32_t n, Fluid f,
 // _jacobi_update_pressures (IISPH.cu:119-162); the convergence bitmask of the
 // reference becomes a count of particles above the threshold, reduced per
 // block together with the FP64 sum of max(0, error)
-template <int KIND, int R, int MIX = 0, bool BATCH = false, int MB = NBR_THREADS>
-__global__ void __launch_bounds__(MB) k_iisph_jacobi(uint32_t n, Fluid f,
+template <int KIND, int R, int MIX, bool BATCH>
+__device__ __forceinline__ void iisph_jacobi(uint32_t n, const Fluid& f,
     const float4* __restrict__ acc, const float4* __restrict__ bterm,
     const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
     float dt, float omega, float tiny, float thr, SweepStats* stats)
@@ -1042,6 +1042,67 @@ __global__ void __launch_bounds__(MB) k_iisph_jacobi(uint32_t n, Fluid f,
         scene_accumulate(stats, sc, live, over, epos, 0.0, emax);
     else
         block_accumulate(stats, over, epos, 0.0, emax);
+}
+
+template <int KIND, int R, int MIX = 0, bool BATCH = false, int MB = NBR_THREADS>
+__global__ void __launch_bounds__(MB) k_iisph_pacc(uint32_t n, Fluid f,
+    const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
+    float4* __restrict__ acc, uint2* __restrict__ acch_out, const uint32_t* __restrict__ gate)
+{
+    iisph_pacc<KIND, R, MIX, BATCH>(n, f, p, bterm, r0i, acc, acch_out, gate);
+}
+
+template <int KIND, int R, int MIX = 0, bool BATCH = false, int MB = NBR_THREADS>
+__global__ void __launch_bounds__(MB) k_iisph_jacobi(uint32_t n, Fluid f,
+    const float4* __restrict__ acc, const float4* __restrict__ bterm,
+    const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
+    float dt, float omega, float tiny, float thr, SweepStats* stats)
+{
+    iisph_jacobi<KIND, R, MIX, BATCH>(n, f, acc, bterm, aii, sii, p, dt, omega, tiny, thr, stats);
+}
+
+// The mixed modes' sweep kernels for one scene and the polynomial kernels,
+// compiled for 40 registers a thread (12 resident blocks of 128): the FP16
+// neighbour records leave these passes waiting on load latency rather than
+// on the L1 data pipe, and the extra resident warps cover it (Jacobi 0.315 ->
+// 0.251 ms at 4M particles). The FP32 passes are L1-bound and keep the
+// compiler's own register choice.
+template <int KIND, int MIX>
+constexpr bool occupancy_variant = MIX != 0 && KIND != K_COS;
+
+template <int KIND, int R, int MIX, int MB>
+__global__ void __launch_bounds__(MB, (65536 / 40) / MB) k_iisph_pacc_occ(uint32_t n, Fluid f,
+    const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
+    float4* __restrict__ acc, uint2* __restrict__ acch_out, const uint32_t* __restrict__ gate)
+{
+    iisph_pacc<KIND, R, MIX, false>(n, f, p, bterm, r0i, acc, acch_out, gate);
+}
+
+template <int KIND, int R, int MIX, int MB>
+__global__ void __launch_bounds__(MB, (65536 / 40) / MB) k_iisph_jacobi_occ(uint32_t n, Fluid f,
+    const float4* __restrict__ acc, const float4* __restrict__ bterm,
+    const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
+    float dt, float omega, float tiny, float thr, SweepStats* stats)
+{
+    iisph_jacobi<KIND, R, MIX, false>(n, f, acc, bterm, aii, sii, p, dt, omega, tiny, thr, stats);
+}
+
+template <int KIND, int R, int MIX, bool BATCH, int MB, class... A>
+void launch_iisph_pacc(unsigned nb, unsigned bs, cudaStream_t q, A... a)
+{
+    if constexpr (!BATCH && occupancy_variant<KIND, MIX>)
+        k_iisph_pacc_occ<KIND, R, MIX, MB><<<nb, bs, 0, q>>>(a...);
+    else
+        k_iisph_pacc<KIND, R, MIX, BATCH, MB><<<nb, bs, 0, q>>>(a...);
+}
+
+template <int KIND, int R, int MIX, bool BATCH, int MB, class... A>
+void launch_iisph_jacobi(unsigned nb, unsigned bs, cudaStream_t q, A... a)
+{
+    if constexpr (!BATCH && occupancy_variant<KIND, MIX>)
+        k_iisph_jacobi_occ<KIND, R, MIX, MB><<<nb, bs, 0, q>>>(a...);
+    else
+        k_iisph_jacobi<KIND, R, MIX, BATCH, MB><<<nb, bs, 0, q>>>(a...);
 }
 
 // final _set_pressure_accelerations + integrate (IISPH.cu:248-257)
@@ -1396,8 +1457,8 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             const float tiny = tiny_threshold();
             auto pacc = [&] {
                 REYN_KERNEL("k_iisph_pacc", s,
-                    k_iisph_pacc<K, R, MIX, B, MB><<<nb, bs, 0, s>>>(n, f, sv.p.get(),
-                    sv.bterm.get(), r0i, sv.acc.get(), ACH, nullptr));
+                    launch_iisph_pacc<K, R, MIX, B, MB>(nb, bs, s, n, f, sv.p.get(),
+                    sv.bterm.get(), r0i, sv.acc.get(), ACH, (const uint32_t*)nullptr));
             };
             if (P.warmstart) {
                 REYN_KERNEL("k_iisph_diag_pacc", s,
@@ -1420,13 +1481,14 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 graph_loop([&](cudaStream_t q, cudaGraphConditionalHandle h) {
                     SweepStats* slot = ns ? scene_slot : slots;
                     REYN_KERNEL("k_iisph_pacc", q,
-                        k_iisph_pacc<K, R, MIX, B, MB><<<nb, bs, 0, q>>>(n, f, sv.p.get(),
-                        sv.bterm.get(), r0i, sv.acc.get(), ACH, gx->gate));
+                        launch_iisph_pacc<K, R, MIX, B, MB>(nb, bs, q, n, f, sv.p.get(),
+                        sv.bterm.get(), r0i, sv.acc.get(), ACH, (const uint32_t*)gx->gate));
                     REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), q));
                     REYN_KERNEL("k_iisph_jacobi", q,
-                        k_iisph_jacobi<K, R, MIX, B, MB><<<nb, bs, 0, q>>>(n, f, sv.acc.get(),
-                        sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, tiny,
-                        thr, slot));
+                        launch_iisph_jacobi<K, R, MIX, B, MB>(nb, bs, q, n, f,
+                        (const float4*)sv.acc.get(), (const float4*)sv.bterm.get(),
+                        (const float*)sv.aii.get(), (const float*)sv.sii.get(), sv.p.get(), dt,
+                        P.omega, tiny, thr, slot));
                     if (ns)
                         scene_converge_dev(q, P.convergence == REYN_CONV_AVERAGE ? 1 : 2);
                     decide(q, h, slot);
@@ -1438,9 +1500,10 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
                 REYN_KERNEL("k_iisph_jacobi", s,
-                    k_iisph_jacobi<K, R, MIX, B, MB><<<nb, bs, 0, s>>>(n, f, sv.acc.get(),
-                    sv.bterm.get(), sv.aii.get(), sv.sii.get(), sv.p.get(), dt, P.omega, tiny,
-                    thr, slot));
+                    launch_iisph_jacobi<K, R, MIX, B, MB>(nb, bs, s, n, f,
+                    (const float4*)sv.acc.get(), (const float4*)sv.bterm.get(),
+                    (const float*)sv.aii.get(), (const float*)sv.sii.get(), sv.p.get(), dt,
+                    P.omega, tiny, thr, slot));
                 iters += 1;
                 const bool last = max_it && iters >= max_it;
                 if (iters < P.min_iter && !last) {
