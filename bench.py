@@ -248,7 +248,7 @@ class EngineRun:
     and the main-loop step (main.cu:64-75)."""
 
     def __init__(self, rank: int, scale: int, dev, precision: str, order: str = "xyz",
-                 ratio: float = 0.5, block: int = 0):
+                 ratio: float = 0.5, block: int = 0, reorder_every: int = 1):
         import reyn_b200 as rb
 
         self.rb = rb
@@ -263,6 +263,9 @@ class EngineRun:
         prm.block_size = block
         self.sv = rb.Solver(rb.IISPH, prm, sc.n)
         self.dt, self.iters = DT0, 0
+        # the state is reordered every `reorder_every` steps; the steps
+        # between run on grids built without reorder (Resort::no)
+        self.reorder_every, self.k = reorder_every, 0
         self.dt_visc = viscous_dt_limit(sc.h, NU)
         self.log = []
         self.limit_hits = 0
@@ -285,7 +288,11 @@ class EngineRun:
         # (scene.cu:466-491)
         self.dt = min(self.sv.next_dt(self.st, self.iters, self.dt, LAMBDA, sc.h,
                                       (0.0, -9.81, 0.0), 10, 0.001, stream=S), self.dt_visc)
-        self.grid.construct_and_reorder(self.st, stream=S)
+        if self.k % self.reorder_every == 0:
+            self.grid.construct_and_reorder(self.st, stream=S)
+        else:
+            self.grid.construct_state(self.st, stream=S)
+        self.k += 1
         try:
             it = self.sv.step(self.st, self.grid, self.bd, self.dt, stream=S,
                               bounds=(sc.box_min, sc.box_max))
@@ -298,13 +305,13 @@ class EngineRun:
         self.log.append((it, self.sv.stats().avg_density_error, self.dt))
 
     def checkpoint(self):
-        return (self.st.download(), self.sv.pressure(), self.dt, self.iters)
+        return (self.st.download(), self.sv.pressure(), self.dt, self.iters, self.k)
 
     def restore(self, ck):
-        state, p, dt, iters = ck
+        state, p, dt, iters, k = ck
         self.st.upload(state)
         self.sv.set_pressure(self.st, p)
-        self.dt, self.iters = dt, iters
+        self.dt, self.iters, self.k = dt, iters, k
 
     def close(self):
         for o in (self.sv, self.grid, self.bd, self.st):
@@ -368,17 +375,26 @@ def run_engine(a, world, rank, local):
     names = ["fp32", "mixed", "mixed_pos16"] if a.precision == "all" else [a.precision]
     # the autotuner (block size of the neighbour passes, cell size) for every
     # precision, from the scene's initial state
-    config = {name: (0.5, 0, None) for name in names}
+    config = {name: (0.5, 0, None, 1) for name in names}
     if not a.no_autotune:
         sc = DeviceScene(rank, a.scale)
         bd = rb.Boundary(*sc.walls, None, h=sc.h, rho0=sc.rho0, mass_iters=5)
         for name in names:
-            best, pts = rb.autotune(rb.IISPH, EngineRun.params(rb, sc, name), sc.st, bd,
-                                    viscous_dt_limit(sc.h, NU), steps=3,
-                                    bounds=(sc.box_min, sc.box_max), stream=S)
+            prm = EngineRun.params(rb, sc, name)
+            best, pts = rb.autotune(rb.IISPH, prm, sc.st, bd, viscous_dt_limit(sc.h, NU),
+                                    steps=3, bounds=(sc.box_min, sc.box_max), stream=S)
+            # then the reorder interval at that block size and cell ratio
+            prm.block_size = best.block_size
+            every = (1, 2, 5, 10)
+            k_best, k_ms = rb.autotune_reorder(rb.IISPH, prm, sc.st, bd,
+                                               viscous_dt_limit(sc.h, NU),
+                                               (sc.box_min, sc.box_max), best.cell_ratio,
+                                               every, steps=10, stream=S)
             config[name] = (best.cell_ratio, best.block_size,
                             [{"block_size": p.block_size, "cell_ratio": p.cell_ratio,
-                              "ms_per_step": round(p.ms_per_step, 3)} for p in pts])
+                              "ms_per_step": round(p.ms_per_step, 3)} for p in pts]
+                            + [{"reorder_every": e, "ms_per_step": round(m, 3)}
+                               for e, m in zip(every, k_ms)], k_best)
         bd.close()
         sc.st.close()
         torch.cuda.synchronize()
@@ -387,8 +403,8 @@ def run_engine(a, world, rank, local):
     # others are reported beside it), then timed end to end
     results = {}
     for name in names:
-        ratio, block, _ = config[name]
-        run = EngineRun(rank, a.scale, dev, name, a.order, ratio, block)
+        ratio, block, _, every = config[name]
+        run = EngineRun(rank, a.scale, dev, name, a.order, ratio, block, every)
         results[name] = (run, timed_steps(run, a, world, stream, dev))
     headline = min(names, key=lambda k: results[k][1][2])  # ms_max: the same on every rank
     legs = {}
@@ -399,6 +415,7 @@ def run_engine(a, world, rank, local):
         legs[name] = leg_summary(r, a, world, msl, logl)
         legs[name]["clocks"] = clk
         legs[name]["cell_ratio"], legs[name]["block_size"] = config[name][0], config[name][1]
+        legs[name]["reorder_every"] = config[name][3]
         r.close()
     torch.cuda.synchronize()
     run, (ck, ms, ms_max, prof, ck_clocks, log) = results[headline]
@@ -504,6 +521,7 @@ def run_engine(a, world, rank, local):
                          f"0.1%/step) from {DT0}, 0.08 h^2/nu = {run.dt_visc:.2e})",
                    "precision": precision, "cell_order": a.order,
                    "block_size": config[headline][1] or 128, "cell_ratio": config[headline][0],
+                   "reorder_every": config[headline][3],
                    "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (state 4M x 28 B + grid 70 MB per step)"},
         "clocks": ck_clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
@@ -538,7 +556,7 @@ def cpu_baseline_from(ck, run):
     import oracle
     import reyn_b200 as rb
 
-    state, p, dt_prev, iters = ck
+    state, p, dt_prev, iters = ck[:4]
     sc = run.sc
     fl = {k: v.copy() for k, v in state.items()}
     fl["id"] = np.arange(sc.n, dtype=np.float32)

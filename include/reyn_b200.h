@@ -447,6 +447,22 @@ int reyn_autotune(reyn_scheme scheme, const reyn_params* params,
     const float* scene_min, const float* scene_max, float dt, uint32_t steps,
     reyn_tune_point* best, reyn_tune_point* points, void* stream);
 
+/* The reorder frequency for one scene at a chosen block size
+ * (params->block_size) and cell ratio: for every candidate interval K in
+ * every[0 .. n_every-1], from the state as it is on entry, with a fresh
+ * solver, `steps` timed steps that reorder the state (construct_and_reorder)
+ * when the step index is a multiple of K and otherwise build the grid
+ * without reorder (reyn_grid_construct over the state's arrays: the solvers'
+ * Resort::no form). A multiple of every K for `steps` times whole cycles.
+ * The state is restored before returning. *best_every is the fastest
+ * interval; ms_per_step (may be NULL) receives n_every times. Synchronises
+ * the stream. */
+int reyn_autotune_reorder(reyn_scheme scheme, const reyn_params* params,
+    reyn_particles* state, const reyn_boundary* bdy, const float bound_min[3],
+    const float bound_max[3], float cell_ratio, float dt, uint32_t steps,
+    const uint32_t* every, uint32_t n_every, uint32_t* best_every,
+    float* ms_per_step, void* stream);
+
 /* ---- captured steps (no counterpart in the reference) -------------------- */
 typedef struct reyn_step_graph reyn_step_graph;
 /* Records one full step of the main loop at a fixed dt — construct_and_reorder

@@ -138,6 +138,8 @@ _SIGNATURES = {
     "reyn_solver_scene_stats": [_vp, _u32, _vp],
     "reyn_autotune": [ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp, _f, _u32,
                       _vp, _vp, _vp],
+    "reyn_autotune_reorder": [ctypes.c_int, _vp, _vp, _vp, _f * 3, _f * 3, _f, _f, _u32, _vp,
+                              _u32, ctypes.POINTER(_u32), _vp, _vp],
     "reyn_diagnostics": [_vp, ctypes.POINTER(Diag), _vp],
     "reyn_solver_step": [_vp, _vp, _vp, _vp, _f, ctypes.POINTER(_u32), _vp],
     "reyn_solver_step_bounded": [_vp, _vp, _vp, _vp, _f, _f * 3, _f * 3, ctypes.POINTER(_u32),
@@ -775,6 +777,21 @@ def autotune(scheme: int, params: Params, state: Particles, bdy, dt: float, step
                                   hi.ctypes.data, dt, steps, ctypes.byref(best), pts,
                                   _stream(stream)))
     return best, list(pts)
+
+
+def autotune_reorder(scheme: int, params: Params, state: Particles, bdy, dt: float, bounds,
+                     cell_ratio: float = 0.5, every=(1, 2, 5, 10), steps: int = 10,
+                     stream=None):
+    """reyn_autotune_reorder: returns (best interval, [ms per step for each
+    candidate]); params.block_size is the block size timed."""
+    ev = np.ascontiguousarray(every, np.uint32)
+    ms = np.zeros(ev.size, np.float32)
+    best = _u32()
+    check(lib().reyn_autotune_reorder(scheme, ctypes.byref(params), state.h,
+                                      bdy.h if bdy else None, _f3(bounds[0]), _f3(bounds[1]),
+                                      cell_ratio, dt, steps, ev.ctypes.data, ev.size,
+                                      ctypes.byref(best), ms.ctypes.data, _stream(stream)))
+    return best.value, [float(x) for x in ms]
 
 
 def profile_enable(on: bool = True) -> None:

@@ -4,7 +4,9 @@
 // is restored to the snapshot taken on entry, a fresh grid and solver are
 // built, one untimed step warms them up, and `steps` steps (grid build with
 // reorder + solver step) are timed with CUDA events on the caller's stream.
-// The state is left as it was found.
+// The state is left as it was found. A second entry times the reorder
+// frequency: the state reordered every K steps, the steps between on grids
+// built without reorder (the solvers' Resort::no form).
 #include "engine.cuh"
 
 #include <vector>
@@ -121,6 +123,72 @@ extern "C" int reyn_autotune(reyn_scheme scheme, const reyn_params* params,
         if (points)
             for (int q = 0; q < 8; ++q)
                 points[q] = all[q];
+        REYN_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+extern "C" int reyn_autotune_reorder(reyn_scheme scheme, const reyn_params* params,
+    reyn_particles* state, const reyn_boundary* bdy, const float bound_min[3],
+    const float bound_max[3], float cell_ratio, float dt, uint32_t steps, const uint32_t* every,
+    uint32_t n_every, uint32_t* best_every, float* ms_per_step, void* stream)
+{
+    return guard([&] {
+        require(params && state && best_every && every && bound_min && bound_max,
+            "null argument");
+        require(n_every >= 1 && steps >= 1, "at least one candidate and one timed step");
+        require(dt > 0.f && std::isfinite(dt), "dt must be positive and finite");
+        require(cell_ratio == 0.5f || cell_ratio == 1.0f, "cell ratio must be 0.5 or 1.0");
+        for (uint32_t q = 0; q < n_every; ++q)
+            require(every[q] >= 1, "a reorder interval is at least one step");
+        const cudaStream_t s = as_stream(stream);
+        Snapshot snap;
+        snap.take(*state, s);
+        reyn_grid grid;
+        grid.geom = make_geom(bound_min, bound_max, 2.f * params->h, cell_ratio);
+        grid.ratio = cell_ratio;
+        Event e0, e1;
+        std::vector<float> ms(n_every);
+        for (uint32_t q = 0; q < n_every; ++q) {
+            reyn_solver sv;
+            sv.scheme = scheme;
+            sv.prm = *params;
+            sv.n = state->n;
+            if (scheme == REYN_PCISPH)
+                sv.pcisph_delta = pcisph_template_delta(params->kernel, params->h);
+            snap.restore(*state, s);
+            auto one = [&](bool reorder) {
+                grid.build(state->cur[FX].get(), state->cur[FY].get(), state->cur[FZ].get(),
+                    state->n, s);
+                if (reorder)
+                    reorder_state(*state, grid, nullptr, 0, s);
+                try {
+                    solver_step(sv, *state, grid, bdy, dt, s);
+                } catch (const Error& e) {
+                    if (e.code != REYN_ERR_ITER_LIMIT)
+                        throw;
+                }
+            };
+            // warm-up, two steps for every candidate so that all are timed
+            // from the same state: buffers, caches, the unsorted step's own
+            one(true);
+            one(every[q] == 1);
+            REYN_CUDA(cudaEventRecord(e0.e, s));
+            for (uint32_t t = 0; t < steps; ++t)
+                one(t % every[q] == 0);
+            REYN_CUDA(cudaEventRecord(e1.e, s));
+            REYN_CUDA(cudaEventSynchronize(e1.e));
+            REYN_CUDA(cudaEventElapsedTime(&ms[q], e0.e, e1.e));
+            ms[q] /= float(steps);
+        }
+        snap.restore(*state, s);
+        uint32_t bi = 0;
+        for (uint32_t q = 1; q < n_every; ++q)
+            if (ms[q] < ms[bi])
+                bi = q;
+        *best_every = every[bi];
+        if (ms_per_step)
+            for (uint32_t q = 0; q < n_every; ++q)
+                ms_per_step[q] = ms[q];
         REYN_CUDA(cudaStreamSynchronize(s));
     });
 }

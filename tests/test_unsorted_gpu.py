@@ -143,3 +143,22 @@ def test_unsorted_grid_over_other_positions_is_rejected(cuda):
         sv.step(st, grid, bd, 1e-3)
     assert e.value.code == rb.ERR_NOT_READY
     _close(sv, grid, bd, st)
+
+
+def test_autotune_reorder_interval(cuda):
+    """reyn_autotune_reorder times every candidate interval from the same
+    state and restores the state; each candidate's steps run (the unsorted
+    ones included) and the best is one of the candidates."""
+    import reyn_b200 as rb
+    sc, bdy = _scene()
+    st, bd, grid, sv = _setup(rb, sc, bdy)
+    before = st.download()
+    prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, 0.01)
+    prm.block_size = 128
+    best, ms = rb.autotune_reorder(rb.IISPH, prm, st, bd, 1e-3, (sc.box_min, sc.box_max),
+                                   0.5, (1, 2, 4), steps=4)
+    assert best in (1, 2, 4) and len(ms) == 3 and all(m > 0 for m in ms)
+    after = st.download()
+    for k in before:
+        np.testing.assert_array_equal(after[k], before[k], err_msg=k)
+    _close(sv, grid, bd, st)
