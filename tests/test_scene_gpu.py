@@ -88,3 +88,38 @@ def test_cull_removes_particles_near_the_boundary(cuda):
     assert not set(np.flatnonzero(close)) & set(order.tolist())
     for o in (st, bd):
         o.close()
+
+
+def test_jitter_matches_host_generator(cuda):
+    """reyn_scene_jitter: particle q of [first, first + count) moves by the
+    uniform [-a, a] of streams 0..2 at counter q, as the fluid blocks' jitter;
+    particles outside the range stay; the boundary reports its samples'
+    bounds."""
+    import torch
+
+    import reyn_b200 as rb
+    rng = np.random.default_rng(9)
+    n, first, count = 5000, 700, 3000
+    host = {k: rng.random(n, dtype=np.float32) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+    st = rb.Particles(n, 1000.0)
+    st.upload(host)
+    a = np.float32(0.0123)
+    rb.scene_jitter(st, float(a), seed=77, first=first, count=count)
+    got = st.download()
+    idx = np.arange(first, first + count, dtype=np.uint64)
+    for t, k in enumerate(("x", "y", "z")):
+        want = host[k].copy()
+        want[first:first + count] = host[k][first:first + count] + scenes._symmetric(
+            scenes.uniform01(77, t, idx), a)
+        np.testing.assert_array_equal(got[k], want, err_msg=k)
+    for k in ("vx", "vy", "vz", "m"):
+        np.testing.assert_array_equal(got[k], host[k], err_msg=k)
+    st.close()
+    b = [torch.tensor(rng.random(300, dtype=np.float32) * 2 - 0.5, device="cuda")
+         for _ in range(3)]
+    bd = rb.Boundary(*b, torch.ones(300, device="cuda"), h=0.05, rho0=1000.0)
+    lo, hi = bd.bounds()
+    for ax in range(3):
+        v = b[ax].cpu().numpy()
+        assert lo[ax] == v.min() and hi[ax] == v.max()
+    bd.close()
