@@ -280,18 +280,33 @@ class EngineRun:
                          "fp32": rb.PRECISION_FP32}[precision]
         return prm
 
-    def step(self, S):
+    def step(self, S, ready=None):
+        """One main-loop step on stream S. ready = (positions, everything):
+        callables that make S wait for the host uploads of the positions and
+        of the whole state; the grid is then built while the velocities and
+        masses still arrive and the state reordered after them."""
         rb, sc = self.rb, self.sc
+        dt_next = lambda: min(self.sv.next_dt(self.st, self.iters, self.dt, LAMBDA, sc.h,
+                                              (0.0, -9.81, 0.0), 10, 0.001, stream=S),
+                              self.dt_visc)
         # simple_dt_controller (cfl.cu:39-52) at lambda 0.4, capped by the
         # explicit-viscosity bound; its max |v| comes from the previous
         # step's integrating kernel, which also applied the hard bounds
         # (scene.cu:466-491)
-        self.dt = min(self.sv.next_dt(self.st, self.iters, self.dt, LAMBDA, sc.h,
-                                      (0.0, -9.81, 0.0), 10, 0.001, stream=S), self.dt_visc)
-        if self.k % self.reorder_every == 0:
-            self.grid.construct_and_reorder(self.st, stream=S)
-        else:
+        if ready is not None and self.k % self.reorder_every == 0:
+            ready[0]()
             self.grid.construct_state(self.st, stream=S)
+            ready[1]()
+            self.dt = dt_next()
+            self.grid.reorder(self.st, stream=S)
+        else:
+            if ready is not None:
+                ready[1]()
+            self.dt = dt_next()
+            if self.k % self.reorder_every == 0:
+                self.grid.construct_and_reorder(self.st, stream=S)
+            else:
+                self.grid.construct_state(self.st, stream=S)
         self.k += 1
         try:
             it = self.sv.step(self.st, self.grid, self.bd, self.dt, stream=S,
@@ -454,11 +469,12 @@ def run_engine(a, world, rank, local):
         run.log.clear()
         # the copies run field by field on two copy streams: the upload of
         # a field for step k + 1 waits only for that field's download of step
-        # k, so the two directions of the link overlap
+        # k, so the two directions of the link overlap, and the grid is built
+        # as soon as the positions are in
         up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
         su, sd = up.cuda_stream, down.cuda_stream
         ev_down = [torch.cuda.Event() for _ in range(6)]
-        ev_up, ev_step = torch.cuda.Event(), torch.cuda.Event()
+        ev_up, ev_step, ev_xyz = torch.cuda.Event(), torch.cuda.Event(), torch.cuda.Event()
 
         def one(f):
             ptrs = [None] * 7
@@ -474,13 +490,15 @@ def run_engine(a, world, rank, local):
         for k in range(a.steps):
             if k:
                 up.wait_event(ev_step)  # the state's arrays are free again
-            for f in (6, 0, 1, 2, 3, 4, 5):  # the masses, never downloaded, first
+            for f in (0, 1, 2, 6, 3, 4, 5):  # positions first, then the masses
                 if k and f < 6:
                     up.wait_event(ev_down[f])
                 rb.check(L.reyn_particles_upload(run.st.h, *one(f), su))
+                if f == 2:
+                    ev_xyz.record(up)
             ev_up.record(up)
-            stream.wait_event(ev_up)
-            run.step(S)
+            run.step(S, ready=(lambda: stream.wait_event(ev_xyz),
+                               lambda: stream.wait_event(ev_up)))
             ev_step.record(stream)
             down.wait_event(ev_step)
             for f in range(6):

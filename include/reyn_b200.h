@@ -183,6 +183,14 @@ int reyn_grid_construct(reyn_grid* g, float search_radius, const float* xx,
 int reyn_grid_construct_and_reorder(reyn_grid* g, float search_radius,
     reyn_particles* state, float* const* extra, uint32_t n_extra,
     void* stream);
+/* the second half of construct_and_reorder: after reyn_grid_construct over
+ * `state`'s own position arrays (reyn_particles_soa), permute the state and
+ * the extra arrays by that build's permutation (Particles::reorder,
+ * particles.cu:93-113), which makes the grid a reordered one. Between the
+ * two calls the positions must not change; the other arrays may still be
+ * arriving (a caller can build the grid while velocities upload). */
+int reyn_grid_reorder(reyn_grid* g, reyn_particles* state,
+    float* const* extra, uint32_t n_extra, void* stream);
 int reyn_grid_info_get(const reyn_grid* g, reyn_grid_info* out);
 /* after a construct_and_reorder: the permutation applied (new[i] =
  * old[perm[i]]), device array of n entries */

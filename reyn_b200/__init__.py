@@ -113,6 +113,7 @@ _SIGNATURES = {
     "reyn_grid_construct": [_vp, _f, _vp, _vp, _vp, _u32, _vp],
     "reyn_grid_construct_and_reorder": [_vp, _f, _vp, ctypes.POINTER(_vp), _u32, _vp],
     "reyn_grid_info_get": [_vp, ctypes.POINTER(GridInfo)],
+    "reyn_grid_reorder": [_vp, _vp, ctypes.POINTER(_vp), _u32, _vp],
     "reyn_grid_permutation": [_vp, ctypes.POINTER(_vp)],
     "reyn_grid_neighbour_stats": [_vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp, _vp, _vp],
     "reyn_compute_densities": [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp, _vp],
@@ -344,6 +345,12 @@ class Grid:
         ptrs = (_vp * max(len(extra), 1))(*[_ptr(t) for t in extra])
         check(lib().reyn_grid_construct_and_reorder(self.h, self.r, state.h, ptrs, len(extra),
                                                     _stream(stream)))
+
+    def reorder(self, state: Particles, extra: Sequence = (), stream=None):
+        """after construct_state: permute the state (and extra arrays) by
+        that build's permutation, as construct_and_reorder would have."""
+        ptrs = (_vp * max(len(extra), 1))(*[_ptr(t) for t in extra])
+        check(lib().reyn_grid_reorder(self.h, state.h, ptrs, len(extra), _stream(stream)))
 
     def info(self) -> GridInfo:
         g = GridInfo()

@@ -271,6 +271,20 @@ int reyn_grid_construct_and_reorder(reyn_grid* g, float search_radius, reyn_part
     });
 }
 
+int reyn_grid_reorder(reyn_grid* g, reyn_particles* state, float* const* extra,
+    uint32_t n_extra, void* stream)
+{
+    return guard([&] {
+        require(g && state, "null argument");
+        require(n_extra == 0 || extra != nullptr, "null extra array list");
+        if (!built_unsorted(*g, *state))
+            fail(REYN_ERR_NOT_READY,
+                "the grid's last build must be construct over this state's positions");
+        const cudaStream_t s = as_stream(stream);
+        reorder_state(*state, *g, extra, n_extra, s);
+    });
+}
+
 int reyn_grid_info_get(const reyn_grid* g, reyn_grid_info* out)
 {
     return guard([&] {

@@ -208,6 +208,8 @@ void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& part, uin
 // packs the particle arrays into pm/vel (after a direct SoA write)
 void pack_state(reyn_particles& st, cudaStream_t s);
 
+// the grid's last build was construct over this state's current positions
+bool built_unsorted(const Grid& g, const reyn_particles& st);
 void reorder_state(reyn_particles& st, Grid& g, float* const* extra,
     uint32_t n_extra, cudaStream_t s);
 

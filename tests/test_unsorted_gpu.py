@@ -162,3 +162,38 @@ def test_autotune_reorder_interval(cuda):
     for k in before:
         np.testing.assert_array_equal(after[k], before[k], err_msg=k)
     _close(sv, grid, bd, st)
+
+
+def test_two_phase_construct_then_reorder(cuda):
+    """reyn_grid_reorder after construct over the state's positions equals
+    construct_and_reorder (state, extra arrays, and a step on the result),
+    and is refused for a grid built over other positions."""
+    import torch
+
+    import reyn_b200 as rb
+    sc, bdy = _scene()
+    out = []
+    for two_phase in (False, True):
+        st, bd, grid, sv = _setup(rb, sc, bdy)
+        ids = torch.tensor(np.asarray(sc.fluid["id"], np.float32), device="cuda")
+        if two_phase:
+            grid.construct_state(st)
+            grid.reorder(st, [ids])
+        else:
+            grid.construct_and_reorder(st, [ids])
+        it = sv.step(st, grid, bd, 1e-3)
+        o = st.download()
+        o["id"] = ids.cpu().numpy()
+        out.append((o, it))
+        if two_phase:
+            h = st.download()
+            xyz = [torch.tensor(h[k], device="cuda") for k in ("x", "y", "z")]
+            grid.construct(*xyz)
+            with pytest.raises(rb.ReynError) as e:
+                grid.reorder(st)
+            assert e.value.code == rb.ERR_NOT_READY
+        _close(sv, grid, bd, st)
+    (a, ia), (b, ib) = out
+    assert ia == ib
+    for k in a:
+        np.testing.assert_array_equal(b[k], a[k], err_msg=k)
