@@ -74,3 +74,18 @@ def test_reference_params_per_scheme():
     assert p.eta == pytest.approx(0.001) and p.min_iter == 3
     p = rb.reference_params(rb.SESPH, rb.B3, 0.01, 1000.0, 0.01)
     assert p.k_sesph == 500.0
+
+
+def test_header_is_plain_c_and_adapter_compiles(tmp_path):
+    """include/reyn_b200.h compiles as strict C99 (the ABI a cgo/ctypes/JNI
+    binding sees), and the C++ adapter include/reyn_b200.hpp as C++17."""
+    c = tmp_path / "abi.c"
+    c.write_text('#include "reyn_b200.h"\nint main(void) { return reyn_abi_version() != 1; }\n')
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                    "-I" + os.path.join(ROOT, "include"), "-c", str(c), "-o",
+                    str(tmp_path / "abi.o")], check=True)
+    cc = tmp_path / "adapter.cpp"
+    cc.write_text('#include "reyn_b200.hpp"\nint main() { return 0; }\n')
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror",
+                    "-I" + os.path.join(ROOT, "include"), "-I/usr/local/cuda/include",
+                    "-fsyntax-only", str(cc)], check=True)
