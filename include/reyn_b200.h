@@ -207,22 +207,25 @@ int reyn_grid_neighbour_stats(const reyn_grid* g, const float* xx,
 
 /* ---- uniform grid without allocation --------------------------------------
  * No counterpart in the reference: an added entry point for callers that
- * cannot allocate device memory — code recorded into CUDA graphs or running
- * under stream capture, real-time loops that must not wait on the allocator,
- * and hosts whose device memory belongs to another runtime's pool. It builds
- * the same grid as reyn_grid_create + reyn_grid_construct (identical prefix
- * and canonical sorted indices) into the caller's buffers, with its scratch
- * in one file-scope device array of REYN_GRID_NOALLOC_SCRATCH_WORDS 32-bit
- * words (32 MiB) that every GPU loading the library holds until exit.
+ * cannot allocate device memory — real-time loops that must not wait on the
+ * device allocator, and hosts whose device memory belongs to another
+ * runtime's pool (a game engine, a framework allocator) that only hands out
+ * the buffers it created. It builds the same grid as reyn_grid_create +
+ * reyn_grid_construct (identical prefix and canonical sorted indices) into
+ * the caller's buffers, with its scratch in one file-scope device array of
+ * REYN_GRID_NOALLOC_SCRATCH_WORDS 32-bit words (32 MiB) that every GPU
+ * loading the library holds until exit. It calls no allocating routine.
  *
  * Limit: nx*ny*nz + 2 n + ceil(nx*ny*nz / 4096) + 2 <= the scratch words
  * (e.g. 1M particles over 5M cells); larger sizes fail with REYN_ERR_INVALID.
  * dims (may be NULL) receives nx, ny, nz; prefix == NULL only reports dims.
- * prefix needs nx*ny*nz + 1 entries (prefix_capacity), sorted n entries.
- * The first call on each device looks up the scratch array's device address
- * (cudaGetSymbolAddress) and should come before any stream capture. All
- * calls share the array: calls that overlap on the GPU race; serialise them.
- * It synchronises `stream` (to report particles outside the grid). */
+ * prefix needs nx*ny*nz + 1 entries (prefix_capacity); xx, xy, xz and sorted
+ * n entries each. The first call on each device looks up the scratch array's
+ * device address (cudaGetSymbolAddress) and should come before any stream
+ * capture. All calls share the array and it keeps the last call's contents
+ * (each call clears the counters it needs): calls that overlap on the GPU
+ * race; serialise them. It synchronises `stream` (to report particles
+ * outside the grid: REYN_ERR_OUT_OF_BOUNDS, REYN_ERR_NONFINITE). */
 #define REYN_GRID_NOALLOC_SCRATCH_WORDS (8u * 1024u * 1024u)
 int reyn_grid_construct_noalloc(const float bound_min[3],
     const float bound_max[3], float search_radius, float cell_ratio,

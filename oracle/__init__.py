@@ -28,7 +28,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_HOST_PATH = os.path.join(HERE, "_ref", "libreyn_ref_host.so")
 REF_CUDA_PATH = os.path.join(HERE, "_ref", "libreyn_ref.so")
-REFERENCE_SRC = "/root/reference/src"
+# the reference checkout (its src/ is compiled into _ref/ when present);
+# REYN_REFERENCE overrides the default location
+REFERENCE_SRC = os.path.join(os.environ.get("REYN_REFERENCE", "/root/reference"), "src")
 
 SESPH, PCISPH, IISPH = 0, 1, 2
 C2, B3, W6, COS = 0, 1, 2, 3
@@ -47,7 +49,8 @@ def build(force: bool = False) -> None:
     if force or not os.path.exists(LIB_PATH):
         subprocess.check_call(["make", "-s", "-C", HERE])
     if os.path.isdir(REFERENCE_SRC):
-        subprocess.check_call(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref")])
+        subprocess.check_call(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"),
+                               "REF=" + os.path.dirname(REFERENCE_SRC)])
 
 
 class Geom(ctypes.Structure):

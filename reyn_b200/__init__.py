@@ -590,11 +590,30 @@ NOALLOC_SCRATCH_WORDS = 8 * 1024 * 1024
 def grid_construct_noalloc(bmin, bmax, search_radius: float, x, y, z, prefix, sorted_,
                            cell_ratio: float = 0.5, stream=None):
     """Uniform-grid build into caller-owned device tensors without any device
-    allocation (reyn_grid_construct_noalloc). prefix=None only returns dims.
+    allocation (reyn_grid_construct_noalloc), for callers that cannot
+    allocate device memory. prefix=None only returns dims. x, y, z are
+    float32 tensors of n entries, sorted_ a 4-byte integer tensor of n
+    entries, prefix a 4-byte integer tensor of at least nx*ny*nz + 1.
     Returns (nx, ny, nz)."""
+    import torch
+
     dims = (ctypes.c_int32 * 3)()
     n = 0 if x is None else x.numel()
     cap = 0 if prefix is None else prefix.numel()
+    if prefix is not None:
+        if n and any(t is None for t in (x, y, z, sorted_)):
+            raise ValueError("x, y, z and sorted_ are needed with prefix")
+        for name, t in (("x", x), ("y", y), ("z", z)):
+            if t is not None and (t.dtype != torch.float32 or t.numel() != n):
+                raise ValueError(f"{name} must be float32 with {n} entries")
+        ints = (torch.int32, getattr(torch, "uint32", torch.int32))
+        if prefix.dtype not in ints:
+            raise ValueError("prefix must hold 4-byte integers")
+        if sorted_ is not None and (sorted_.dtype not in ints or sorted_.numel() != n):
+            raise ValueError(f"sorted_ must hold {n} 4-byte integers")
+        for t in (x, y, z, prefix, sorted_):
+            if t is not None and not t.is_contiguous():
+                raise ValueError("tensors must be contiguous")
     check(lib().reyn_grid_construct_noalloc(_f3(bmin), _f3(bmax), search_radius, cell_ratio,
                                             _ptr(x), _ptr(y), _ptr(z), n, _ptr(prefix), cap,
                                             _ptr(sorted_), dims, _stream(stream)))

@@ -1,15 +1,15 @@
 // reyn_grid_construct_noalloc: the uniform-grid build for callers that must
 // not allocate device memory.
 //
-// Some callers cannot call cudaMalloc: code that records work into a CUDA
-// graph or runs under a stream capture (allocation calls are not allowed or
-// not replayable there), real-time loops that must not stall on the
-// allocator, and hosts whose device memory is owned by another runtime's pool
-// (a game engine, a framework allocator) and that only hand out the buffers
-// they created. reyn_grid_construct keeps its scratch (per-cell counters,
-// keys, unordered slots, scan partials) in device arrays the grid object
-// allocates; this variant keeps it in one file-scope device array instead,
-// so a call needs nothing but the caller's input and output buffers.
+// Some callers cannot call cudaMalloc: real-time loops that must not stall
+// on the device allocator (cudaMalloc can synchronise the device and take
+// milliseconds), and hosts whose device memory is owned by another runtime's
+// pool (a game engine, a framework allocator) that only hand out the buffers
+// they created and forbid allocations behind the pool's back.
+// reyn_grid_construct keeps its scratch (per-cell counters, keys, unordered
+// slots, scan partials) in device arrays the grid object allocates; this
+// variant keeps it in one file-scope device array instead, so a call needs
+// nothing but the caller's input and output buffers.
 //
 // The array is REYN_GRID_NOALLOC_SCRATCH_WORDS 32-bit words (32 MiB). It is
 // part of this library's device image: every GPU that loads it holds the
@@ -131,22 +131,21 @@ extern "C" int reyn_grid_construct_noalloc(const float bound_min[3], const float
         v.nxny = geom.n[0] * geom.n[1];
         v.prefix = prefix;
         if (n) {
-            k_keys_count<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, xx, xy, xz, v, keys,
-                counts, status);
-            REYN_LAUNCHED("k_keys_count");
+            REYN_KERNEL("k_keys_count", s,
+                k_keys_count<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, xx, xy, xz, v, keys,
+                counts, status));
         }
-        k_scan_tiles<<<nparts, 256, 0, s>>>(counts, C, parts);
-        REYN_LAUNCHED("k_scan_tiles");
-        k_scan_parts<<<1, 256, 0, s>>>(parts, nparts);
-        REYN_LAUNCHED("k_scan_parts");
-        k_scan_apply<<<nparts, 256, 0, s>>>(counts, C, parts, nparts, prefix);
-        REYN_LAUNCHED("k_scan_apply");
+        REYN_KERNEL("k_scan_tiles", s, k_scan_tiles<<<nparts, 256, 0, s>>>(counts, C, parts));
+        REYN_KERNEL("k_scan_parts", s, k_scan_parts<<<1, 256, 0, s>>>(parts, nparts));
+        REYN_KERNEL("k_scan_apply", s,
+            k_scan_apply<<<nparts, 256, 0, s>>>(counts, C, parts, nparts, prefix));
         if (n) {
-            k_scatter<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, keys, prefix, counts, slots);
-            REYN_LAUNCHED("k_scatter");
-            k_canonical<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, slots, keys, prefix,
-                sorted);
-            REYN_LAUNCHED("k_canonical");
+            REYN_KERNEL("k_scatter", s,
+                k_scatter<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, keys, prefix, counts,
+                slots));
+            REYN_KERNEL("k_canonical", s,
+                k_canonical<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, slots, keys, prefix,
+                sorted));
         }
         uint32_t bits = 0;
         REYN_CUDA(cudaMemcpyAsync(&bits, status, sizeof(bits), cudaMemcpyDeviceToHost, s));

@@ -1,9 +1,11 @@
 """reyn_grid_construct_noalloc: the grid build for callers that cannot
-allocate device memory (work recorded into CUDA graphs or stream captures,
-real-time loops, hosts whose device memory belongs to another pool). It must
-produce exactly what reyn_grid_construct produces — the prefix over all cells
-and the canonical sorted indices — from its file-scope scratch array, on
-consecutive calls that reuse that array, and must refuse sizes beyond the
+allocate device memory (real-time loops that must not wait on the device
+allocator, hosts whose device memory belongs to another runtime's pool). It
+must produce exactly what reyn_grid_construct produces — the prefix over all
+cells and the canonical sorted indices — from its file-scope scratch array,
+on consecutive calls that reuse that array, must leave the device's free
+memory unchanged, must report particles outside the grid and non-finite
+positions like the allocating build, and must refuse sizes beyond the
 scratch limit.
 
 This file is collected last, so that a run stopping at the first failure has
@@ -74,3 +76,41 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(cuda):
     with pytest.raises(rb.ReynError):
         rb.grid_construct_noalloc(bmin, bmax, r, x[:10], x[:10], x[:10], prefix[:5],
                                   sorted_[:10])
+
+
+def test_noalloc_allocates_nothing_and_reports_bad_positions(cuda):
+    import torch
+
+    import reyn_b200 as rb
+
+    bmin, bmax, r = [0, 0, 0], [1, 1, 1], 0.04
+    x, y, z = scenes.uniform_cloud(100_000, seed=43)
+    tx, ty, tz = _t(x), _t(y), _t(z)
+    dims = rb.grid_construct_noalloc(bmin, bmax, r, None, None, None, None, None)
+    C = dims[0] * dims[1] * dims[2]
+    prefix = torch.empty(C + 1, dtype=torch.int32, device="cuda")
+    sorted_ = torch.empty(x.size, dtype=torch.int32, device="cuda")
+    bad = tx.clone()
+    rb.grid_construct_noalloc(bmin, bmax, r, tx, ty, tz, prefix, sorted_)  # warm
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    rb.grid_construct_noalloc(bmin, bmax, r, tx, ty, tz, prefix, sorted_)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0, "a warm call changed the free device memory"
+
+    # a non-finite position and a position outside the grid are reported
+    bad[123] = float("nan")
+    with pytest.raises(rb.ReynError) as e:
+        rb.grid_construct_noalloc(bmin, bmax, r, bad, ty, tz, prefix, sorted_)
+    assert e.value.code == rb.ERR_NONFINITE
+    bad[123] = 5.0
+    with pytest.raises(rb.ReynError) as e:
+        rb.grid_construct_noalloc(bmin, bmax, r, bad, ty, tz, prefix, sorted_)
+    assert e.value.code == rb.ERR_OUT_OF_BOUNDS
+
+    # the next valid call starts from cleared counters and status
+    rb.grid_construct_noalloc(bmin, bmax, r, tx, ty, tz, prefix, sorted_)
+    want_dims, want_prefix, want_sorted = _existing(x, y, z, bmin, bmax, r)
+    assert dims == want_dims
+    np.testing.assert_array_equal(prefix.cpu().numpy().view(np.uint32), want_prefix)
+    np.testing.assert_array_equal(sorted_.cpu().numpy().view(np.uint32), want_sorted)
