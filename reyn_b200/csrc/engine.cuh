@@ -152,7 +152,9 @@ struct reyn_solver {
     reyn::DevArray<float4> acc, vel2, bterm;
     reyn::DevArray<float> p_tmp;
     reyn::DevArray<uint32_t> nbr, ncount; // per-step neighbour list
-    reyn::DevArray<uint2> pmh, acch, velh, velh2; // mixed-precision neighbour records
+    reyn::DevArray<uint2> acch, velh, velh2; // MIXED: FP16 neighbour records
+    reyn::DevArray<uint4> rec0, rec1;        // MIXED_POS16: 16-byte neighbour records
+    reyn::DevArray<float4> gq;               // MIXED_POS16: (G, gsq), then (G, a_ii)
     reyn::DevArray<unsigned char> sweep_stats; // per-sweep reductions
     std::unique_ptr<reyn::PinnedArray<unsigned char>> readback;
     uint64_t p_epoch = 0;      // particle epoch p is ordered for

@@ -37,16 +37,20 @@ namespace {
 // Slot k of particle i lives at list_slot(i, k): blocks of 128 particles
 // store their slot rows contiguously, so that a warp reads one 128-byte row
 // per slot. A particle with more than KMAX neighbours keeps its count
-// (> KMAX) and is served by the cell traversal instead.
+// (> KMAX) and is served by the cell traversal instead. Each block of 128
+// particles owns LROWS = KMAX + 4 rows, so that a loop may load the indices
+// of the next four slots past a particle's last one without a bound check
+// (the values are not used).
 constexpr int KMAX = 64;
+constexpr int LROWS = KMAX + 4;
 // (the layout is independent of the block size of the passes)
 
 __host__ __device__ __forceinline__ size_t list_slot(uint32_t i, uint32_t k)
 {
-    return size_t(i >> 7) * (KMAX * 128) + size_t(k) * 128 + (i & 127u);
+    return size_t(i >> 7) * (LROWS * 128) + size_t(k) * 128 + (i & 127u);
 }
 
-inline size_t list_capacity(uint32_t n) { return size_t((n + 127) / 128) * KMAX * 128; }
+inline size_t list_capacity(uint32_t n) { return size_t((n + 127) / 128) * LROWS * 128; }
 
 struct Fluid {
     GridView g;
@@ -55,11 +59,9 @@ struct Fluid {
     uint32_t* status;
     uint32_t* __restrict__ nbr;    // neighbour list (list_slot layout)
     uint32_t* __restrict__ ncount; // neighbours per particle
-    // mixed precision: per particle its position as three 16-bit wrapped
-    // fixed-point coordinates and m / m_0 as FP16, m_0 = pm[0].w; its
-    // pressure acceleration as FP16 (scaled by ACC_SCALE) for the Jacobi
-    // sweeps, and the FP32 accelerations for particles off the list
-    const uint2* __restrict__ pmh;
+    // MIXED: per particle its pressure acceleration as FP16 (scaled by
+    // ACC_SCALE) for the Jacobi sweeps, and the FP32 accelerations for
+    // particles off the list
     const uint2* __restrict__ acch;
     const float4* __restrict__ acc32;
     // batched scenes: per-scene flag, 0 once the scene's iteration has
@@ -68,24 +70,23 @@ struct Fluid {
 };
 
 // ---- mixed precision ----------------------------------------------------------
-// Neighbour records are 8 bytes: each position coordinate as a 16-bit
+// MIXED_POS16 records are 16 bytes: each position coordinate as a 16-bit
 // wrapped fixed-point number, the position in cells modulo 4 at a resolution
-// of 1/16384 cell, and the mass relative to particle 0's as FP16; velocities,
-// densities and pressure accelerations of neighbours are FP16. The
-// particle's own data and all arithmetic stay FP32. Neighbours lie within 2
-// cells (r), so the 16-bit difference u_i - u_j, read as a signed number, is
-// the pair vector x_ij in units of 1/16384 cell exactly, with no cell index
-// stored: three subtractions and conversions per pair. (A coordinate
-// difference of exactly 2 cells reads as -2; such a pair lies on the
-// support's edge, where the kernel and its gradient vanish.) Both ends use
-// their quantised records, so x_ji = -x_ij holds exactly and pair forces stay
-// antisymmetric. The quantisation error is at most 1/32768 cell per
-// coordinate (FP16 offsets within a cell would round to 1/4096).
+// of 1/16384 cell, and 10 bytes of the quantity the reading pass needs.
+// Neighbours lie within 2 cells (r), so the 16-bit difference u_i - u_j, read
+// as a signed number, is the pair vector x_ij in units of 1/16384 cell
+// exactly, with no cell index stored. (A coordinate difference of exactly 2
+// cells reads as -2; such a pair lies on the support's edge, where the kernel
+// and its gradient vanish.) Both ends use their quantised records, so
+// x_ji = -x_ij holds exactly and pair forces stay antisymmetric. The
+// quantisation error is at most 1/32768 cell per coordinate (FP16 offsets
+// within a cell would round to 1/4096).
 constexpr float FIXQ = 16384.f;
 
 // storage modes of the neighbour loops (the template argument MIX):
 // 0 FP32; MIX_F16 FP16 velocities, densities and pressure accelerations of
-// neighbours; MIX_POS16 those plus the 16-bit position records
+// neighbours; MIX_POS16 the 16-byte records (16-bit positions, FP16
+// velocities and accelerations, FP32 pressures)
 constexpr int MIX_F16 = 1;
 constexpr int MIX_POS16 = 2;
 
@@ -107,6 +108,27 @@ __device__ __forceinline__ uint2 float4_to_half4(float4 v)
     return u;
 }
 
+__device__ __forceinline__ uint32_t half2_bits(float a, float b)
+{
+    const __half2 h = __floats2half2_rn(a, b);
+    uint32_t u;
+    memcpy(&u, &h, 4);
+    return u;
+}
+
+__device__ __forceinline__ float2 bits_half2(uint32_t u)
+{
+    __half2 h;
+    memcpy(&h, &u, 4);
+    return __half22float2(h);
+}
+
+// the FP16 number in the upper half of u
+__device__ __forceinline__ float upper_half(uint32_t u)
+{
+    return __half2float(__ushort_as_half((unsigned short)(u >> 16)));
+}
+
 // one coordinate: (cell index mod 4) * 16384 + the offset in the cell in
 // units of 1/16384, modulo 2^16 (an offset that rounds up to 16384 carries
 // into the cell index)
@@ -116,35 +138,117 @@ __device__ __forceinline__ uint32_t fix_coord(float p, float lo, float inv_cell,
     return ((uint32_t(c) << 14) + __float2uint_rn(o * FIXQ)) & 0xffffu;
 }
 
-// the record of a particle at (x, y, z) with mass ratio mr in grid cell c
-__device__ __forceinline__ uint2 pack_record(const GridView& g, int3 c, float x, float y,
-    float z, float mr)
+// words 0 and 1 of a record: x | y << 16 and z | a << 16 (a: 16 payload bits)
+__device__ __forceinline__ uint2 record_position(const GridView& g, int3 c, float x, float y,
+    float z, uint32_t a)
 {
     const uint32_t ux = fix_coord(x, g.lox, g.inv_cell, c.x);
     const uint32_t uy = fix_coord(y, g.loy, g.inv_cell, c.y);
     const uint32_t uz = fix_coord(z, g.loz, g.inv_cell, c.z);
-    const __half hm = __float2half_rn(mr);
-    uint16_t bm;
-    memcpy(&bm, &hm, 2);
-    return make_uint2(ux | (uy << 16), uz | (uint32_t(bm) << 16));
+    return make_uint2(ux | (uy << 16), uz | (a << 16));
 }
 
-// x_i - x_j from two records, in units of 1/FIXQ cell
-__device__ __forceinline__ float3 record_delta(uint2 ri, uint2 rj)
+// Record layouts (word 0 = x | y << 16 and the low half of word 1 = z are the
+// position in every layout):
+//   NP (density -> non-pressure): w1 hi m/m_0 (FP16), w2 (vx, vy), w3 (vz, rho)
+//   DG (non-pressure -> diagonal): w1 hi, w2 = m v* / m_0 (3 x FP16),
+//      w3 = m p_old (FP32)
+//   Y (pressure accelerations -> Jacobi): w1 hi m/m_0, w2, w3 lo =
+//      m a ACC_SCALE / m_0 (3 x FP16)
+//   X (Jacobi -> pressure accelerations): w1 hi m/m_0, w2 = p (FP32)
+__device__ __forceinline__ uint32_t half_bits(float a)
 {
-    // per-halfword subtraction without a borrow between the halves
-    const uint32_t dxy = __vsub2(ri.x, rj.x);
-    const uint32_t dz = ri.y - rj.y; // the low half is exact modulo 2^16
-    return make_float3(float(int16_t(dxy & 0xffffu)), float(int16_t(dxy >> 16)),
-        float(int16_t(dz & 0xffffu)));
+    return __half_as_ushort(__float2half_rn(a));
 }
 
-__device__ __forceinline__ float record_mass_ratio(uint2 r)
+// the FP16 number in the lower half of u
+__device__ __forceinline__ float lower_half(uint32_t u)
 {
-    const uint16_t bm = uint16_t(r.y >> 16);
-    __half hm;
-    memcpy(&hm, &bm, 2);
-    return __half2float(hm);
+    return __half2float(__ushort_as_half((unsigned short)(u & 0xffffu)));
+}
+
+__device__ __forceinline__ uint4 rec_np(const GridView& g, int3 c, const float4& me,
+    uint32_t m16, float vx, float vy, float vz, float rho)
+{
+    const uint2 p = record_position(g, c, me.x, me.y, me.z, m16);
+    return make_uint4(p.x, p.y, half2_bits(vx, vy), half2_bits(vz, rho));
+}
+
+// word 1 of a record with the mass ratio m16 in its upper half
+__device__ __forceinline__ uint32_t rec_w1(const uint4& r, uint32_t m16)
+{
+    return (r.y & 0xffffu) | (m16 << 16);
+}
+
+__device__ __forceinline__ uint4 rec_dg(const uint4& prev, float vx, float vy, float vz, float mp)
+{
+    return make_uint4(prev.x, (prev.y & 0xffffu) | (half_bits(vx) << 16), half2_bits(vy, vz),
+        __float_as_uint(mp));
+}
+
+__device__ __forceinline__ float3 rec_dg_vec(const uint4& r)
+{
+    const float2 yz = bits_half2(r.z);
+    return make_float3(upper_half(r.y), yz.x, yz.y);
+}
+
+__device__ __forceinline__ float rec_dg_mp(const uint4& r) { return __uint_as_float(r.w); }
+
+__device__ __forceinline__ uint4 rec_y(uint32_t w0, uint32_t w1, float ax, float ay, float az)
+{
+    return make_uint4(w0, w1, half2_bits(ax, ay), half_bits(az));
+}
+
+__device__ __forceinline__ float3 rec_y_vec(const uint4& r)
+{
+    const float2 xy = bits_half2(r.z);
+    return make_float3(xy.x, xy.y, lower_half(r.w));
+}
+
+__device__ __forceinline__ uint4 rec_x(uint32_t w0, uint32_t w1, float p)
+{
+    return make_uint4(w0, w1, __float_as_uint(p), 0u);
+}
+
+__device__ __forceinline__ float rec_x_p(const uint4& r) { return __uint_as_float(r.z); }
+
+// the mass ratio m/m_0 of a NP, Y or X record
+__device__ __forceinline__ float rec_m16(const uint4& r) { return upper_half(r.y); }
+
+// A particle's own coordinates, offset by half the 16-bit range, laid out so
+// that one 32-bit subtraction per coordinate leaves (u_i - u_j + 2^15) mod
+// 2^16 in one half of the result: x and z in the low half, y in the high half
+// (its low half 0xffff, so that no borrow crosses into it).
+struct Own16 {
+    uint32_t bx, by, bz;
+};
+
+__device__ __forceinline__ Own16 own16(const uint4& r)
+{
+    return Own16 { (r.x + 0x8000u) & 0xffffu, ((r.x + 0x80000000u) & 0xffff0000u) | 0xffffu,
+        (r.y + 0x8000u) & 0xffffu };
+}
+
+// x_i - x_j in units of 1/FIXQ cell, exactly: the 16-bit half t of each
+// difference is placed under the exponent of 2^23 (a float 2^23 + t, built by
+// one byte permutation), and 2^23 + 2^15 is subtracted. No integer-to-float
+// conversion instruction is needed.
+__device__ __forceinline__ float3 delta16(const Own16& o, const uint4& rj)
+{
+    constexpr float BIAS = 8421376.f; // 2^23 + 2^15
+    const uint32_t tx = o.bx - rj.x, ty = o.by - rj.x, tz = o.bz - rj.y;
+    return make_float3(__uint_as_float(__byte_perm(tx, 0x4B000000u, 0x7610)) - BIAS,
+        __uint_as_float(__byte_perm(ty, 0x4B000000u, 0x7632)) - BIAS,
+        __uint_as_float(__byte_perm(tz, 0x4B000000u, 0x7610)) - BIAS);
+}
+
+// the kernel constants for pair vectors in units of 1/FIXQ cell: with
+// h_inv scaled by the unit, pair_w gives W and pair_g gives g' = g * unit,
+// so that grad W = g' d for the pair vector d in those units
+__host__ __device__ __forceinline__ KernelConst kernel_in_units(KernelConst k, float unit)
+{
+    k.h_inv *= unit;
+    return k;
 }
 
 // accelerations are stored as FP16 of a * 2^-6: up to 4e6 m/s^2 before
@@ -244,31 +348,16 @@ __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, cons
     F&& fn)
 {
     static_assert(MIX || !ACC, "accelerations travel with the mixed records only");
+    static_assert(MIX != MIX_POS16, "the 16-byte records have their own loop (for_each_rec)");
     const uint32_t cnt = __ldg(f.ncount + i);
     if (cnt <= KMAX) {
         const uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
-        [[maybe_unused]] uint2 ri {};
-        [[maybe_unused]] float m0 = 0.f, unit = 0.f;
-        if constexpr (MIX == MIX_POS16) {
-            ri = __ldg(f.pmh + i);
-            m0 = __ldg(&f.pm[0].w);
-            unit = f.g.cell * (1.f / FIXQ);
-        }
         // one neighbour: index, position data, the pair
         auto pair = [&](uint32_t j, float4& q, float& dx, float& dy, float& dz) {
-            if constexpr (MIX == MIX_POS16) {
-                const uint2 rj = __ldg(f.pmh + j);
-                const float3 d = record_delta(ri, rj);
-                dx = d.x * unit;
-                dy = d.y * unit;
-                dz = d.z * unit;
-                q.w = m0 * record_mass_ratio(rj);
-            } else {
-                q = __ldg(f.pm + j);
-                dx = me.x - q.x;
-                dy = me.y - q.y;
-                dz = me.z - q.z;
-            }
+            q = __ldg(f.pm + j);
+            dx = me.x - q.x;
+            dy = me.y - q.y;
+            dz = me.z - q.z;
             if constexpr (ACC) {
                 const float3 a = unpack_acc_scaled(__ldg(f.acch + j));
                 q.x = a.x;
@@ -321,6 +410,88 @@ __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, cons
                 } else {
                     fn(j, q, dx, dy, dz, l2);
                 }
+            });
+    }
+}
+
+// MIXED_POS16: the fluid neighbours j != i of particle i with their 16-byte
+// records: fn(j, rec_j, d, g) with d = x_i - x_j in units of 1/FIXQ cell and
+// g the kernel-gradient factor of the pair in those units (grad W_ij = g d;
+// kc holds the kernel constants in record units), in the traversal order of
+// the cells. ri is the particle's own record in `rec`. A particle whose list
+// overflowed walks the cell traversal over the FP32 positions, its pair
+// vectors converted to the record units.
+template <int KIND, int R, bool BATCH = false, class F>
+__device__ __forceinline__ void for_each_rec(const Fluid& f, const KernelConst& kc,
+    const uint4* __restrict__ rec, uint32_t i, const uint4& ri, F&& fn)
+{
+    const uint32_t cnt = __ldg(f.ncount + i);
+    {
+        // ask the L2 for the warp's list rows up front (one 128-byte segment
+        // per row and lane), so that the loop's index loads do not each wait
+        // for DRAM
+        const unsigned m = __activemask();
+        const uint32_t mc = __reduce_max_sync(m, min(cnt, uint32_t(KMAX)));
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t* seg = f.nbr + list_slot(i & ~31u, 0);
+        if (lane < mc)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(seg + size_t(lane) * 128));
+        if (lane + 32u < mc)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(seg + size_t(lane + 32u) * 128));
+    }
+    if (cnt <= KMAX) {
+        const Own16 o = own16(ri);
+        const uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
+        uint32_t k = 0;
+        // four neighbours per round, the next round's indices loaded before
+        // this round's records are used (the list streams from DRAM and each
+        // record load depends on its index); the rows past a particle's last
+        // slot are padding, read but not used
+        uint32_t jn[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+            jn[u] = __ldg(row + size_t(u) * 128);
+        for (; k + 4 <= cnt; k += 4) {
+            uint32_t j[4];
+            uint4 r[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                j[u] = jn[u];
+                r[u] = __ldg(rec + j[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                jn[u] = __ldg(row + size_t(k + 4 + u) * 128);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float3 d = delta16(o, r[u]);
+                fn(j[u], r[u], d, pair_g<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+            if (k + u < cnt) {
+                const uint4 r = __ldg(rec + jn[u]);
+                const float3 d = delta16(o, r);
+                fn(jn[u], r, d, pair_g<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
+            }
+        }
+    } else {
+        const float4 me = f.pm[i];
+        GridView gv = f.g;
+        if constexpr (BATCH)
+            gv = at_scene(gv, scene_of(gv, i));
+        int3 c = cell_of(gv, me.x, me.y, me.z);
+        if (!cell_inside(gv, c, R)) // flagged by the density pass already
+            c = clamp_cell(gv, c, R);
+        const float to_units = FIXQ / gv.cell;
+        for_each_neighbour<R>(gv, c, me.x, me.y, me.z, f.pm,
+            [&](uint32_t j, const float4&, float dx, float dy, float dz, float) {
+                if (j == i)
+                    return;
+                const float3 d = make_float3(dx * to_units, dy * to_units, dz * to_units);
+                fn(j, __ldg(rec + j), d,
+                    pair_g<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
             });
     }
 }
@@ -607,12 +778,12 @@ __device__ __forceinline__ void tail_reduce(const Tail& t, float v)
 // compute_densities (solver.cuh:18-38) + cached boundary sums + the step's
 // neighbour list, written entry by entry (a block's rows form one 32 KB
 // region, so the L2 merges the scattered 4-byte stores into full lines).
-// Mixed precision: the particle's 8-byte position and velocity records are
-// written for later passes.
+// MIXED: the particle's FP16 velocity/density record is written for later
+// passes; MIXED_POS16: its 16-byte record for the non-pressure pass.
 template <int KIND, int R, int MIX = 0, bool BATCH = false, int MB = NBR_THREADS>
 __global__ void __launch_bounds__(MB) k_density(uint32_t n, Fluid f, Bdy b,
     float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm,
-    uint2* __restrict__ pmh_out, uint2* __restrict__ velh_out)
+    uint4* __restrict__ rec_out, uint2* __restrict__ velh_out)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
@@ -655,13 +826,14 @@ __global__ void __launch_bounds__(MB) k_density(uint32_t n, Fluid f, Bdy b,
     vel[i].w = r;
     bterm[i] = make_float4(gx, gy, gz, rb);
     f.ncount[i] = cnt;
-    if constexpr (MIX) {
+    if constexpr (MIX == MIX_POS16) {
+        const float4 v = vel[i];
+        const float m0 = __ldg(&f.pm[0].w);
+        rec_out[i] = rec_np(f.g, c, me, half_bits(me.w / (m0 != 0.f ? m0 : 1.f)), v.x, v.y, v.z,
+            r);
+    } else if constexpr (MIX) {
         const float4 v = vel[i];
         velh_out[i] = float4_to_half4(make_float4(v.x, v.y, v.z, r));
-    }
-    if constexpr (MIX == MIX_POS16) {
-        const float m0 = __ldg(&f.pm[0].w);
-        pmh_out[i] = pack_record(f.g, c, me.x, me.y, me.z, me.w / (m0 != 0.f ? m0 : 1.f));
     }
 }
 
@@ -1194,6 +1366,8 @@ __global__ void k_gather_p(uint32_t n, const uint32_t* __restrict__ perm,
         dst[i] = src[perm[i]];
 }
 
+#include "passes_rec.cuh"
+
 template <class F> void dispatch(int kind, int range, F&& f)
 {
     auto go = [&](auto K) {
@@ -1284,7 +1458,6 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     f.status = const_cast<uint32_t*>(grid.status.get());
     f.nbr = sv.nbr.get();
     f.ncount = sv.ncount.get();
-    f.pmh = nullptr;
     f.acch = nullptr;
     f.acc32 = sv.acc.get();
     f.active = ns ? sv.scene_active.get() : nullptr;
@@ -1394,12 +1567,13 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             &gx->stats->iters, P.min_iter, max_it));
     };
 
-    const bool mixed = P.precision != REYN_PRECISION_FP32;
-    uint2* PMH = P.precision == REYN_PRECISION_MIXED_POS16 ? sv.pmh.get() : nullptr;
+    const bool mixed = P.precision == REYN_PRECISION_MIXED;
+    const bool rec16 = P.precision == REYN_PRECISION_MIXED_POS16;
     uint2* ACH = mixed ? sv.acch.get() : nullptr;
     uint2* VH = mixed ? sv.velh.get() : nullptr;
     uint2* VH2 = mixed ? sv.velh2.get() : nullptr;
-    f.pmh = PMH;
+    uint4* REC0 = rec16 ? sv.rec0.get() : nullptr;
+    uint4* REC1 = rec16 ? sv.rec1.get() : nullptr;
     f.acch = ACH;
     auto body = [&](auto KC, auto RC, auto MC, auto BC) {
         constexpr int K = decltype(KC)::value;
@@ -1408,7 +1582,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         constexpr bool B = decltype(BC)::value;
         REYN_KERNEL("k_density", s,
             k_density<K, R, MIX, B, MB><<<nb, bs, 0, s>>>(n, f, b, sv.rho.get(), st.vel.get(),
-            sv.bterm.get(), PMH, VH));
+            sv.bterm.get(), REC0, VH));
         if (sv.scheme == REYN_SESPH) {
             REYN_KERNEL("k_sesph", s,
                 k_sesph<K, R, B, MB><<<nb, bs, 0, s>>>(n, f, st.vel.get(), sv.bterm.get(),
@@ -1485,6 +1659,97 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             }
             REYN_KERNEL("k_advect", s,
                 k_advect<B><<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, st.pm.get(), v, dt, X, Y, Z,
+                VX, VY, VZ, tail));
+        } else if constexpr (MIX == MIX_POS16) { // IISPH over 16-byte records
+            RecConst rc;
+            rc.unit = f.g.cell / FIXQ;
+            rc.kc = kernel_in_units(f.kc, rc.unit);
+            const float tiny = tiny_threshold();
+            const float thr = P.eta * rho0;
+            // the density pass wrote the non-pressure records into REC0
+            REYN_KERNEL("k_np_rec", s,
+                k_np_rec<K, R, B, MB><<<nb, bs, 0, s>>>(n, f, rc, st.vel.get(),
+                (const float4*)sv.bterm.get(), sv.p.get(), nu10, eps, grav, dt, REC0, REC1,
+                sv.vel2.get(), sv.gq.get()));
+            // the sweeps alternate between RX (records with m p, read by the
+            // pressure accelerations) and RY (records with m a, read by Jacobi)
+            uint4* RX = REC1;
+            uint4* RY = REC0;
+            auto pacc = [&](cudaStream_t q, const uint32_t* gate) {
+                REYN_KERNEL("k_pacc_rec", q,
+                    k_pacc_rec<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, rc,
+                    (const float4*)sv.gq.get(), r0i, RX, RY, gate));
+            };
+            auto jacobi = [&](cudaStream_t q, SweepStats* slot) {
+                REYN_KERNEL("k_jacobi_rec", q,
+                    k_jacobi_rec<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, rc,
+                    (const float4*)sv.gq.get(), (const float*)sv.sii.get(), sv.p.get(), dt,
+                    P.omega, tiny, thr, slot, RY, RX));
+            };
+            if (P.warmstart) {
+                REYN_KERNEL("k_diag_pacc_rec", s,
+                    k_diag_pacc_rec<K, R, B, MB><<<nb, bs, 0, s>>>(n, f, rc, sv.vel2.get(),
+                    sv.gq.get(), rho0, dt, r0i, sv.p.get(), sv.aii.get(), sv.sii.get(),
+                    sv.p_tmp.get(), REC1, REC0));
+                sv.p.swap(sv.p_tmp);
+            } else {
+                REYN_KERNEL("k_diag_rec", s,
+                    k_diag_rec<K, R, B, MB><<<nb, bs, 0, s>>>(n, f, rc, sv.vel2.get(),
+                    sv.gq.get(), rho0, dt, P.omega, tiny, sv.aii.get(), sv.sii.get(),
+                    sv.p.get(), REC1, REC0));
+                RX = REC0;
+                RY = REC1;
+                pacc(s, nullptr);
+            }
+            if (gx) {
+                REYN_CUDA(cudaMemsetAsync(gx->gate, 0, sizeof(uint32_t), s));
+                graph_loop([&](cudaStream_t q, cudaGraphConditionalHandle h) {
+                    SweepStats* slot = ns ? scene_slot : slots;
+                    pacc(q, gx->gate);
+                    REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), q));
+                    jacobi(q, slot);
+                    if (ns)
+                        scene_converge_dev(q, P.convergence == REYN_CONV_AVERAGE ? 1 : 2);
+                    decide(q, h, slot);
+                });
+            }
+            for (; !gx;) {
+                SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
+                REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
+                jacobi(s, slot);
+                iters += 1;
+                const bool last = max_it && iters >= max_it;
+                if (iters < P.min_iter && !last) {
+                    pacc(s, nullptr);
+                    continue;
+                }
+                if (ns) {
+                    if (!scenes_go_on(P.convergence == REYN_CONV_AVERAGE ? 1 : 2))
+                        break;
+                    if (last) {
+                        converged = false;
+                        break;
+                    }
+                    pacc(s, nullptr);
+                    continue;
+                }
+                readback(slot);
+                sv.stats.avg_density_error = host.err_sum / n / rho0;
+                sv.stats.max_density_error = host.err_max / rho0;
+                const bool more = P.convergence == REYN_CONV_AVERAGE
+                    ? host.err_sum / n > (double)P.eta * rho0
+                    : host.over > 0; // IISPH.cu:246
+                if (!more)
+                    break;
+                if (last) {
+                    converged = false;
+                    break;
+                }
+                pacc(s, nullptr);
+            }
+            REYN_KERNEL("k_final_rec", s,
+                k_final_rec<K, R, B, MB><<<nb, bs, 0, s>>>(n, f, rc,
+                (const float4*)sv.gq.get(), r0i, sv.vel2.get(), dt, sv.acc.get(), RX, X, Y, Z,
                 VX, VY, VZ, tail));
         } else { // IISPH
             REYN_KERNEL("k_nonpressure", s,

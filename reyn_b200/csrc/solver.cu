@@ -70,12 +70,14 @@ void ensure_buffers(reyn_solver& sv, uint32_t n)
     sv.bterm.resize(n);
     sv.nbr.resize(list_capacity(n));
     sv.ncount.resize(n);
-    if (sv.prm.precision != REYN_PRECISION_FP32) {
-        if (sv.prm.precision == REYN_PRECISION_MIXED_POS16)
-            sv.pmh.resize(n);
+    if (sv.prm.precision == REYN_PRECISION_MIXED) {
         sv.acch.resize(n);
         sv.velh.resize(n);
         sv.velh2.resize(n);
+    } else if (sv.prm.precision == REYN_PRECISION_MIXED_POS16) {
+        sv.rec0.resize(n);
+        sv.rec1.resize(n);
+        sv.gq.resize(n);
     }
     if (sv.p.size() != n) {
         sv.p.resize(n);
