@@ -56,6 +56,14 @@ ALG_BYTES = {
     "k_iisph_pacc": 12 + 4 + 4 + 12,  # x, m, p -> a
     "k_iisph_jacobi": 12 + 4 + 12 + 8 + 4 + 4,  # x, m, a, p r/w, a_ii, s_i
     "k_iisph_final": 12 + 4 + 4 + 12 + 12 + 12 + 12,  # x, m, p, v* -> a, x, v
+    # the same passes over 16-byte neighbour records (mixed_pos16): the same
+    # compulsory arrays of their reference counterparts
+    "k_np_rec": 12 + 12 + 4 + 4 + 12 + 12,
+    "k_diag_pacc_rec": 12 + 12 + 4 + 4 + 4 + 4 + 4 + 12,
+    "k_diag_rec": 12 + 12 + 4 + 4 + 4 + 4 + 4,
+    "k_pacc_rec": 12 + 4 + 4 + 12,
+    "k_jacobi_rec": 12 + 4 + 12 + 8 + 4 + 4,
+    "k_final_rec": 12 + 4 + 4 + 12 + 12 + 12 + 12,
     "k_keys_count": 12 + 4,           # x -> key (+ histogram)
     "k_scatter": 4 + 4 + 4,           # key, prefix -> slot
     "k_canonical": 4 + 4 + 4 + 4,     # slot, key, prefix -> sorted
@@ -99,12 +107,36 @@ def parse_args():
                     help="column_16m: reorder the state every K steps, the steps between on "
                          "grids built without reorder")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision-check", action="store_true",
+                    help="iisph_4m: skip the error of every precision mode against the "
+                         "FP64 checker on the benchmark scene")
+    ap.add_argument("--develop-steps", type=int, default=2500,
+                    help="iisph_4m: untimed FP32 steps that develop the flow before the "
+                         "'developed' leg times every precision from the same state "
+                         "(0: no developed leg)")
     return ap.parse_args()
 
 
 NU = 0.01
 LAMBDA = 0.4
 DT0 = 5e-4
+# the steps both arms time with the reference's own constants: the reference
+# arm on the reference's CUDA, the engine arm on the engine
+REF_CUDA_STEPS = 5
+REF_CUDA_DT = 2e-4
+
+
+def workload_config(n: int, nb: int, h: float, rho0: float, world: int) -> dict:
+    """The workload as both arms state it (the same keys and values): scene,
+    kernel, solver constants and dt rule. Engine settings (precision, block
+    size, cell size, reorder interval) are reported under "engine"."""
+    return {"workload": WORKLOAD, "particles_per_gpu": n, "boundary_particles": nb,
+            "kernel": "C2", "h": h, "rho0": rho0, "nu": NU, "omega": 0.5,
+            "convergence": "avg density error <= 0.1% (FP64 reduction)",
+            "dt": f"min(simple_dt_controller(lambda={LAMBDA}, target 10 iters, "
+                  f"0.1%/step) from {DT0}, 0.08 h^2/nu = {viscous_dt_limit(h, NU):.2e})",
+            "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (state 4M x 28 B + grid 70 MB per step)"}
 
 
 def scene_spec(rank: int, scale: int) -> dict:
@@ -377,6 +409,162 @@ def leg_summary(run, a, world, ms_max, log):
             "iter_limit_hits": run.limit_hits}
 
 
+def developed_leg(a, world, rank, dev, stream, names, config):
+    """The flow developed by a.develop_steps untimed FP32 main-loop steps
+    (the dam break's column collapsing), checkpointed; every precision then
+    runs W warm-up and K timed steps from that same state. The sweeps per
+    step there exceed the 3 of the first steps from rest."""
+    import torch
+
+    S = stream.cuda_stream
+    base = EngineRun(rank, a.scale, dev, "fp32", a.order, *config["fp32"][:2]
+                     if "fp32" in config else (0.5, 0))
+    for _ in range(a.develop_steps):
+        base.step(S)
+    torch.cuda.synchronize()
+    ck = base.checkpoint()
+    t_sim = float(sum(x[2] for x in base.log))
+    base_iters = [x[0] for x in base.log[-10:]]
+    base.close()
+    out = {"develop_steps": a.develop_steps, "simulated_seconds": round(t_sim, 5),
+           "iters_last_develop_steps": base_iters}
+    for name in names:
+        ratio, block, _, every = config[name]
+        r = EngineRun(rank, a.scale, dev, name, a.order, ratio, block, every)
+        r.restore(ck)
+        _, _, ms_max, _, clk, log = timed_steps(r, a, world, stream, dev)
+        leg = leg_summary(r, a, world, ms_max, log)
+        leg["dt_per_step"] = [float(f"{x[2]:.4e}") for x in log]
+        leg["clocks"] = clk
+        out[name] = leg
+        r.close()
+    mixed = [k for k in ("mixed", "mixed_pos16") if k in out]
+    if "fp32" in out and mixed:
+        out["mixed_over_fp32_by_mode"] = {k: round(out[k]["value"] / out["fp32"]["value"], 3)
+                                          for k in mixed}
+    return out
+
+
+PREC_STEPS, PREC_SWEEPS, PREC_DT = 2, 4, 2e-4
+PREC_FIELDS = ("x", "y", "z", "vx", "vy", "vz", "rho", "p", "aii", "sii")
+
+
+def precision_vs_fp64(rank: int, scale: int, names, stream=None):
+    """Error of each precision mode against the FP64 restatement of the IISPH
+    step (oracle/fp64.py, the checker: torch float64 on this GPU, pairs by
+    cube bucketing) on the benchmark scene itself: PREC_STEPS main-loop steps
+    of exactly PREC_SWEEPS Jacobi sweeps at dt PREC_DT from rest, the same
+    initial state and boundary masses for every run. Per quantity the largest
+    error relative to the field's largest magnitude, and the mean
+    |rho - rho_FP64| / rho0."""
+    import torch
+
+    import reyn_b200 as rb
+    from oracle import fp64
+
+    S = None if stream is None else stream.cuda_stream
+    sc = DeviceScene(rank, scale)
+    bd = rb.Boundary(*sc.walls, None, h=sc.h, rho0=sc.rho0, mass_iters=5)
+    fluid = sc.st.download()
+    (px, py, pz, pm), nb = bd.arrays()
+    bdy = {"x": rb.device_to_numpy(px, nb), "y": rb.device_to_numpy(py, nb),
+           "z": rb.device_to_numpy(pz, nb), "m": rb.device_to_numpy(pm, nb)}
+    grav = (0.0, -9.81, 0.0)
+    t0 = time.perf_counter()
+    want = fp64.iisph_run(rb.C2, fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, NU, grav,
+                          PREC_DT, PREC_STEPS, PREC_SWEEPS, 0.5, True, device="cuda")
+    t_fp64 = time.perf_counter() - t0
+    out = {"what": "error against the FP64 restatement (checker) on the benchmark scene, "
+                   f"{PREC_STEPS} steps of {PREC_SWEEPS} Jacobi sweeps at dt {PREC_DT} from "
+                   "rest; per field max |err| / max |field|, and mean |rho - rho_FP64| / rho0",
+           "particles": sc.n, "fp64_seconds": round(t_fp64, 1)}
+    dev = torch.device("cuda")
+    ids0 = torch.arange(sc.n, dtype=torch.float32, device=dev)
+    for name in names:
+        sc.st.upload(fluid)
+        ids = ids0.clone()
+        prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, NU)
+        prm.min_iter = prm.max_iter = PREC_SWEEPS
+        prm.eta = 1.0  # met after every sweep: exactly PREC_SWEEPS sweeps
+        prm.precision = {"mixed": rb.PRECISION_MIXED, "mixed_pos16": rb.PRECISION_MIXED_POS16,
+                         "fp32": rb.PRECISION_FP32}[name]
+        sv = rb.Solver(rb.IISPH, prm, sc.n)
+        grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h)
+        for _ in range(PREC_STEPS):
+            grid.construct_and_reorder(sc.st, [ids], stream=S)
+            sv.step(sc.st, grid, bd, PREC_DT, stream=S, bounds=(sc.box_min, sc.box_max))
+        torch.cuda.synchronize()
+        got = sc.st.download()
+        buf = sv.buffers()
+        for k in ("rho", "p", "aii", "sii"):
+            got[k] = rb.device_to_numpy(getattr(buf, k), sc.n)
+        order = np.argsort(ids.cpu().numpy().astype(np.int64))
+        err = {}
+        for k in PREC_FIELDS:
+            g = np.asarray(got[k], np.float64)[order]
+            w = np.asarray(want[k], np.float64)
+            err[k] = float(f"{np.abs(g - w).max() / max(np.abs(w).max(), 1e-30):.3g}")
+        drho = np.abs(np.asarray(got["rho"], np.float64)[order] - want["rho"])
+        err["mean_abs_rho_rel"] = float(f"{np.mean(drho) / sc.rho0:.3g}")
+        out[name] = err
+        sv.close()
+        grid.close()
+    bd.close()
+    sc.st.close()
+    return out
+
+
+def reference_constants_leg(a, rank, dev, stream, names):
+    """The engine on the steps the reference arm's "reference_cuda" leg times:
+    the scene at rest, REF_CUDA_STEPS main-loop steps at the fixed dt
+    REF_CUDA_DT with the reference's hard-coded IISPH constants
+    (reyn_params_reference: any particle above 0.5 % error, min 3 sweeps,
+    omega 0.5, warm start), after one untimed run of the same steps; FP32
+    and each mixed mode."""
+    import torch
+
+    import reyn_b200 as rb
+
+    S = stream.cuda_stream
+    out = {"what": "the engine on the steps of the reference arm's reference_cuda leg "
+                   "(reference constants, fixed dt, from rest)",
+           "steps": REF_CUDA_STEPS, "dt": REF_CUDA_DT}
+    for name in names:
+        sc = DeviceScene(rank, a.scale)
+        bd = rb.Boundary(*sc.walls, None, h=sc.h, rho0=sc.rho0, mass_iters=5)
+        grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h)
+        prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, NU)
+        prm.precision = {"mixed": rb.PRECISION_MIXED, "mixed_pos16": rb.PRECISION_MIXED_POS16,
+                         "fp32": rb.PRECISION_FP32}[name]
+        sv = rb.Solver(rb.IISPH, prm, sc.n)
+        init = sc.st.download()
+
+        def steps():
+            it = []
+            for _ in range(REF_CUDA_STEPS):
+                grid.construct_and_reorder(sc.st, stream=S)
+                it.append(sv.step(sc.st, grid, bd, REF_CUDA_DT, stream=S,
+                                  bounds=(sc.box_min, sc.box_max)))
+            return it
+
+        steps()
+        sc.st.upload(init)
+        sv.set_pressure(sc.st, np.zeros(sc.n, np.float32))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        it = steps()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / REF_CUDA_STEPS
+        out[name] = {"ms_per_step": round(t, 3), "value": round(sc.n / (t / 1e3), 1),
+                     "unit": UNIT, "iters_per_step": it}
+        for o in (sv, grid, bd, sc.st):
+            o.close()
+    return out
+
+
 def run_engine(a, world, rank, local):
     import torch
 
@@ -518,45 +706,56 @@ def run_engine(a, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline_from(ck, run)
+    run.close()
+
+    developed = None
+    if a.develop_steps > 0:
+        developed = developed_leg(a, world, rank, dev, stream, names, config)
+    ref_constants = None
+    if world == 1 and a.scale == 1:
+        ref_constants = reference_constants_leg(a, rank, dev, stream, names)
+    precision_error = None
+    if rank == 0 and world == 1 and not a.no_precision_check:
+        precision_error = precision_vs_fp64(rank, a.scale, names, stream)
 
     precision = {
         "fp32": "fp32 storage and math",
         "mixed": "mixed: neighbour velocities, densities and pressure accelerations FP16; "
                  "positions, own data and all arithmetic FP32; Kahan density and divergence "
                  "sums; FP64 convergence reduction",
-        "mixed_pos16": "mixed with neighbour positions as 16-bit fixed point (1/16384 cell) "
-                       "and masses FP16"}[headline]
+        "mixed_pos16": "mixed_pos16: every neighbour pass reads one 16-byte record per "
+                       "neighbour (positions 16-bit fixed point at 1/16384 cell, masses, "
+                       "velocities and m a FP16, m p FP32); own data and all arithmetic "
+                       "FP32; Kahan density and divergence sums; FP64 convergence "
+                       "reduction"}[headline]
     out = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded lattice + jitter dam break; Akinci box walls)",
-        "config": {"workload": WORKLOAD, "particles_per_gpu": n,
-                   "boundary_particles": run.sc.nb, "kernel": "C2", "h": run.sc.h,
-                   "rho0": run.sc.rho0, "nu": NU, "omega": 0.5,
-                   "convergence": "avg density error <= 0.1% (FP64 reduction)",
-                   "dt": f"min(simple_dt_controller(lambda={LAMBDA}, target 10 iters, "
-                         f"0.1%/step) from {DT0}, 0.08 h^2/nu = {run.dt_visc:.2e})",
-                   "precision": precision, "cell_order": a.order,
+        "config": workload_config(n, run.sc.nb, run.sc.h, run.sc.rho0, world),
+        "engine": {"precision": precision, "cell_order": a.order,
                    "block_size": config[headline][1] or 128, "cell_ratio": config[headline][0],
-                   "reorder_every": config[headline][3],
-                   "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (state 4M x 28 B + grid 70 MB per step)"},
+                   "reorder_every": config[headline][3]},
         "clocks": ck_clocks, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
         "cpu_baseline": cpu, "autotune": config[headline][2],
         "iters_per_step": [x[0] for x in log],
         "avg_density_error_per_step": [round(x[1], 7) for x in log],
         "dt_per_step": [float(f"{x[2]:.4e}") for x in log],
         "iter_limit_hits": run.limit_hits, "kernels": kernels,
+        "developed": developed, "reference_constants": ref_constants,
+        "precision_error": precision_error,
     }
     out["headline_precision"] = headline
     out.update(legs)
     vals = dict({k: v["value"] for k, v in legs.items()}, **{headline: value})
-    if "fp32" in vals and "mixed" in vals:
-        out["mixed_over_fp32"] = round(vals["mixed"] / vals["fp32"], 3)
+    mixed = [k for k in ("mixed", "mixed_pos16") if k in vals]
+    if "fp32" in vals and mixed:
+        best = max(mixed, key=lambda k: vals[k])
+        out["mixed_over_fp32"] = round(vals[best] / vals["fp32"], 3)
+        out["mixed_over_fp32_by_mode"] = {k: round(vals[k] / vals["fp32"], 3) for k in mixed}
     if rank == 0:
         print(json.dumps(out), flush=True)
-    run.close()
 
 
 def oracle_params(h: float, rho0: float):
@@ -642,9 +841,9 @@ def run_reference(a, world, rank):
            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
            "ms_per_step": round(secs / a.steps * 1e3, 3), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-           "config": {"workload": WORKLOAD, "particles_per_gpu": sc.n,
-                      "parallelism": "host threads", "setup_s": round(setup, 1),
-                      "iters_per_step": log},
+           "config": workload_config(sc.n, int(sc.bdy["x"].size), sc.h, sc.rho0, world),
+           "reference_run": {"threads": oracle.threads(), "setup_s": round(setup, 1),
+                             "iters_per_step": log},
            "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": oracle.threads(),
                             "kind": "port",
                             "sample": f"{a.steps} timed steps of the full workload after "
@@ -652,7 +851,54 @@ def run_reference(a, world, rank):
                                       f"of the reference's algorithm"},
            "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
+    out["reference_cuda"] = reference_cuda_leg(sc, bm)
     print(json.dumps(out), flush=True)
+
+
+def reference_cuda_leg(sc, bm):
+    """The reference's own CUDA step (its src/ compiled unmodified for sm_100a
+    into oracle/_ref/ by oracle/ref/Makefile) on the same scene and boundary
+    masses: REF_CUDA_STEPS main-loop steps (construct_and_reorder, IISPH step
+    with the reference's hard-coded constants, hard bounds) at the fixed dt
+    REF_CUDA_DT from rest, device-timed, after one untimed run of the same
+    steps (kernel loading, allocation). The engine arm's "reference_constants"
+    leg runs the same steps with the same constants."""
+    import ctypes
+
+    import oracle
+    try:
+        L = oracle.ref_cuda()
+    except (OSError, FileNotFoundError) as e:
+        return {"unavailable": f"reference CUDA library not built: {e}"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no GPU"}
+    except ImportError:
+        return {"unavailable": "no torch"}
+    P = lambda x: x.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    F32 = lambda x: np.ascontiguousarray(x, np.float32)  # noqa: E731
+    keys = ("x", "y", "z", "vx", "vy", "vz", "m", "id")
+    bx, by, bz, bmf = F32(sc.bdy["x"]), F32(sc.bdy["y"]), F32(sc.bdy["z"]), F32(bm)
+    lo, hi = F32(sc.box_min), F32(sc.box_max)
+    iters = np.zeros(REF_CUDA_STEPS, np.uint32)
+    ms = np.zeros(1, np.float32)
+    for _ in range(2):  # the second run, from the same state, is the one reported
+        st = {k: F32(sc.fluid[k]).copy() for k in keys}
+        rc = L.ref_run_timed(2, 0, ctypes.c_uint(sc.n), *(P(st[k]) for k in keys),
+                             ctypes.c_uint(int(bx.size)), P(bx), P(by), P(bz), P(bmf), P(lo),
+                             P(hi), ctypes.c_float(sc.h), ctypes.c_float(sc.rho0),
+                             ctypes.c_float(NU), ctypes.c_float(REF_CUDA_DT),
+                             ctypes.c_uint(REF_CUDA_STEPS), P(iters), P(ms))
+        if rc:
+            return {"unavailable": "reference CUDA run failed: "
+                    + L.ref_last_error().decode()}
+    t = float(ms[0])
+    return {"what": "the reference's own CUDA IISPH main-loop step on this GPU (reference "
+                    "constants: any particle above 0.5 % error, min 3 sweeps; fixed dt)",
+            "steps": REF_CUDA_STEPS, "dt": REF_CUDA_DT, "ms_per_step": round(t, 3),
+            "value": round(sc.n / (t / 1e3), 1), "unit": UNIT,
+            "iters_per_step": iters.tolist()}
 
 
 # ---- batched workload ----------------------------------------------------------

@@ -62,22 +62,75 @@ def _dw(kind: int, q):
     return -4.0 * np.pi * torch.sin(s) - 2.0 * np.pi * torch.sin(2.0 * s)
 
 
+def _pairs_host(a, b, hbar: float, same: bool):
+    """(i, j) with |a_i - b_j| <= hbar from scipy's k-d tree on the host."""
+    import torch
+    an = a.cpu().numpy()
+    ta = cKDTree(an)
+    tb = ta if same else cKDTree(b.cpu().numpy())
+    sp = ta.sparse_distance_matrix(tb, hbar, output_type="ndarray")
+    # for a tree against itself the pairs include i == j (distance 0)
+    i = torch.from_numpy(sp["i"].astype(np.int64)).to(a.device)
+    j = torch.from_numpy(sp["j"].astype(np.int64)).to(a.device)
+    return i, j
+
+
+def _pairs_cells(a, b, hbar: float, chunk: int = 1 << 18):
+    """(i, j) with |a_i - b_j| <= hbar by bucketing b into cubes of side hbar
+    (torch, on the tensors' device): every a_i is tested against the points
+    of the 27 cubes around its own, in FP64, a chunk of a at a time. Used for
+    scenes too large for the host k-d tree; the pair set is the same."""
+    import torch
+    dev = a.device
+    lo = torch.minimum(a.min(0).values, b.min(0).values) - hbar
+    n3 = ((torch.maximum(a.max(0).values, b.max(0).values) + hbar - lo) / hbar).floor().long() + 2
+    nx, ny = int(n3[0]), int(n3[1])
+    cb = ((b - lo) / hbar).floor().long()
+    kb = (cb[:, 2] * ny + cb[:, 1]) * nx + cb[:, 0]
+    kb_sorted, order = torch.sort(kb)
+    offs = torch.tensor([(dz * ny + dy) * nx + dx for dz in (-1, 0, 1) for dy in (-1, 0, 1)
+                         for dx in (-1, 0, 1)], device=dev, dtype=torch.long)
+    ii, jj = [], []
+    h2 = hbar * hbar
+    for c0 in range(0, a.shape[0], chunk):
+        ac = a[c0:c0 + chunk]
+        ca = ((ac - lo) / hbar).floor().long()
+        ka = (ca[:, 2] * ny + ca[:, 1]) * nx + ca[:, 0]
+        keys = (ka[:, None] + offs[None, :]).reshape(-1)
+        st = torch.searchsorted(kb_sorted, keys)
+        en = torch.searchsorted(kb_sorted, keys, right=True)
+        cnt = en - st
+        total = int(cnt.sum())
+        if total == 0:
+            continue
+        seg = torch.repeat_interleave(torch.arange(keys.numel(), device=dev), cnt)
+        first = torch.cumsum(cnt, 0) - cnt
+        pos = torch.arange(total, device=dev) - first[seg] + st[seg]
+        i = seg // offs.numel() + c0
+        j = order[pos]
+        d = a[i] - b[j]
+        keep = (d * d).sum(1) <= h2
+        ii.append(i[keep])
+        jj.append(j[keep])
+        del seg, first, pos, i, j, d, keep
+    if not ii:
+        z = torch.zeros(0, dtype=torch.long, device=dev)
+        return z, z
+    return torch.cat(ii), torch.cat(jj)
+
+
 class _Pairs:
     """All pairs (i, j) with |x_i - x_j| < r, i from `a`, j from `b`, with the
     kernel value and the gradient factor: grad W_ij = gf * x_ij. a, b: (N, 3)
-    float64 tensors; the pairs are found on the host."""
+    float64 tensors; the pairs are found on the host (k-d tree) or, for
+    tensors on a GPU with many points, by cube bucketing on the GPU."""
 
     def __init__(self, kind: int, hbar: float, a, b, same: bool):
         import torch
-        an = a.cpu().numpy()
-        ta = cKDTree(an)
-        tb = ta if same else cKDTree(b.cpu().numpy())
-        sp = ta.sparse_distance_matrix(tb, hbar, output_type="ndarray")
-        # for a tree against itself the pairs include i == j (distance 0)
-        dev = a.device
-        i = torch.from_numpy(sp["i"].astype(np.int64)).to(dev)
-        j = torch.from_numpy(sp["j"].astype(np.int64)).to(dev)
-        del sp
+        if a.device.type == "cuda" and a.shape[0] > 1_000_000:
+            i, j = _pairs_cells(a, b, hbar)
+        else:
+            i, j = _pairs_host(a, b, hbar, same)
         x = a[i] - b[j]
         r = torch.sqrt((x * x).sum(1))
         q = torch.clamp_max(r / hbar, 1.0)

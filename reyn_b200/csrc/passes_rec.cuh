@@ -55,7 +55,8 @@ __device__ __forceinline__ float rec_m0(const Fluid& f)
 // viscosity term (10 nu m_j v_ij.x_ij g / (rho_j (|x_ij|^2 + eps))) x_ij
 // becomes (10 nu m_j v_ij.d g' / (rho_j (unit |d|^2 + eps / unit))) d.
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_np_rec(uint32_t n, Fluid f, RecConst rc,
+__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+k_np_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ vel, const float4* __restrict__ bterm,
     const float* __restrict__ p_old, float nu10, float eps, float3 grav, float dt,
     const uint4* __restrict__ rec_in, uint4* __restrict__ rec_out,
@@ -91,8 +92,7 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_np_rec
     ay += grav.y;
     az += grav.z;
     const float4 bt = bterm[i];
-    gq[i] = make_float4(Gx + bt.x, Gy + bt.y, Gz + bt.z,
-        gsq);
+    gq[i] = make_float4(Gx + bt.x, Gy + bt.y, Gz + bt.z, gsq);
     const float4 vs = make_float4(vi.x + dt * ax, vi.y + dt * ay, vi.z + dt * az, vi.w);
     vel_out[i] = vs;
     const float mr = rec_m16(ri);
@@ -102,12 +102,13 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_np_rec
 // _compute_diagonal_elem_and_source_term (IISPH.cu:11-66) fused with the
 // warm start and the first sweep's pressure accelerations (IISPH.cu:68-98,
 // 193-209) over DG records: a_ii needs no neighbour loop (G and gsq come
-// from the density pass); the loop sums the divergence
+// from the non-pressure pass); the loop sums the divergence
 // sum_j (m_j v*_j).grad W_ij (compensated) and sum_j (m_j p'_j) grad W_ij with
 // the warm-started p' = p_old / 2. Writes a_ii (also into gq.w), s_i, p'
 // (p_new) and the Y record.
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_diag_pacc_rec(uint32_t n, Fluid f, RecConst rc,
+__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+k_diag_pacc_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ vel, float4* __restrict__ gq, float rho0, float dt, float r0i,
     const float* __restrict__ p_old, float* __restrict__ aii, float* __restrict__ sii,
     float* __restrict__ p_new, const uint4* __restrict__ rec_in, uint4* __restrict__ rec_out)
@@ -124,7 +125,8 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_diag_p
     const float pi = p_old[i] * 0.5f;
     Kahan vk;
     float sx = 0.f, sy = 0.f, sz = 0.f;
-    for_each_rec<KIND, R, BATCH>(f, rc.kc, rec_in, i, ri, [&](uint32_t, const uint4& rj, float3 d, float g) {
+    for_each_rec<KIND, R, BATCH>(f, rc.kc, rec_in, i, ri,
+        [&](uint32_t, const uint4& rj, float3 d, float g) {
         const float3 mv = rec_dg_vec(rj);
         vk.add(g * fmaf(mv.x, d.x, fmaf(mv.y, d.y, mv.z * d.z)));
         const float sp = g * rec_dg_mp(rj);
@@ -133,9 +135,8 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_diag_p
         sz += sp * d.z;
     });
     // the neighbours' pressures are half their carried ones
-    const float hs = 0.5f;
-    const float ax = -r0i * fmaf(pi, gt.x, hs * sx), ay = -r0i * fmaf(pi, gt.y, hs * sy),
-                az = -r0i * fmaf(pi, gt.z, hs * sz);
+    const float ax = -r0i * fmaf(pi, gt.x, 0.5f * sx), ay = -r0i * fmaf(pi, gt.y, 0.5f * sy),
+                az = -r0i * fmaf(pi, gt.z, 0.5f * sz);
     const float gss = fmaf(gt.x, gt.x, fmaf(gt.y, gt.y, gt.z * gt.z));
     const float a = -dt * (gss + mi * gt.w) / (rho0 * rho0);
     aii[i] = a;
@@ -151,7 +152,8 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_diag_p
 // from the Jacobi update of zero; writes the X record for the pressure
 // accelerations that follow
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_diag_rec(uint32_t n, Fluid f, RecConst rc,
+__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+k_diag_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ vel, float4* __restrict__ gq, float rho0, float dt,
     float omega, float tiny, float* __restrict__ aii, float* __restrict__ sii,
     float* __restrict__ p, const uint4* __restrict__ rec_in, uint4* __restrict__ rec_out)
@@ -165,7 +167,8 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_diag_r
     const float4 gt = gq[i];
     const uint4 ri = rec_in[i];
     Kahan vk;
-    for_each_rec<KIND, R, BATCH>(f, rc.kc, rec_in, i, ri, [&](uint32_t, const uint4& rj, float3 d, float g) {
+    for_each_rec<KIND, R, BATCH>(f, rc.kc, rec_in, i, ri,
+        [&](uint32_t, const uint4& rj, float3 d, float g) {
         const float3 mv = rec_dg_vec(rj);
         vk.add(g * fmaf(mv.x, d.x, fmaf(mv.y, d.y, mv.z * d.z)));
     });
@@ -186,7 +189,8 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_diag_r
 // particle's own X record; writes the Y record with m a. `gate`: a captured
 // step's loop body skips the first sweep's pass.
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_pacc_rec(uint32_t n, Fluid f, RecConst rc,
+__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+k_pacc_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ gq, float r0i, const uint4* __restrict__ rec_in,
     uint4* __restrict__ rec_out, const uint32_t* __restrict__ gate)
 {
@@ -202,16 +206,16 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_pacc_r
     const uint4 ri = rec_in[i];
     const float pi = rec_x_p(ri);
     float sx = 0.f, sy = 0.f, sz = 0.f;
-    for_each_rec<KIND, R, BATCH>(f, rc.kc, rec_in, i, ri, [&](uint32_t, const uint4& rj, float3 d, float g) {
+    for_each_rec<KIND, R, BATCH>(f, rc.kc, rec_in, i, ri,
+        [&](uint32_t, const uint4& rj, float3 d, float g) {
         const float sp = g * (rec_m16(rj) * rec_x_p(rj));
         sx += sp * d.x;
         sy += sp * d.y;
         sz += sp * d.z;
     });
     const float ma = rec_m16(ri) * ACC_SCALE * -r0i;
-    const float mu = m0;
-    rec_out[i] = rec_y(ri.x, ri.y, ma * fmaf(pi, gt.x, mu * sx), ma * fmaf(pi, gt.y, mu * sy),
-        ma * fmaf(pi, gt.z, mu * sz));
+    rec_out[i] = rec_y(ri.x, ri.y, ma * fmaf(pi, gt.x, m0 * sx), ma * fmaf(pi, gt.y, m0 * sy),
+        ma * fmaf(pi, gt.z, m0 * sz));
 }
 
 // _jacobi_update_pressures (IISPH.cu:108-162) over Y records:
@@ -219,7 +223,8 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_pacc_r
 // own Y record; p += max(0, omega (s - Ap) / a_ii); writes p and the X record;
 // the convergence sums as the FP32 sweep's.
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_jacobi_rec(uint32_t n, Fluid f, RecConst rc,
+__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+k_jacobi_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ gq, const float* __restrict__ sii, float* __restrict__ p,
     float dt, float omega, float tiny, float thr, SweepStats* stats,
     const uint4* __restrict__ rec_in, uint4* __restrict__ rec_out)
@@ -270,7 +275,8 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_jacobi
 // records; writes a and the SoA state (bounds and the max |v| reduction of a
 // bounded step included)
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_final_rec(uint32_t n, Fluid f, RecConst rc,
+__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+k_final_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ gq, float r0i, const float4* __restrict__ vel, float dt,
     float4* __restrict__ acc, const uint4* __restrict__ rec_in, float* __restrict__ x,
     float* __restrict__ y, float* __restrict__ z, float* __restrict__ vx,
@@ -292,9 +298,8 @@ __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>)) k_final_
                 sy += sp * d.y;
                 sz += sp * d.z;
             });
-        const float mu = m0;
-        const float ax = -r0i * fmaf(pi, gt.x, mu * sx), ay = -r0i * fmaf(pi, gt.y, mu * sy),
-                    az = -r0i * fmaf(pi, gt.z, mu * sz);
+            const float ax = -r0i * fmaf(pi, gt.x, m0 * sx), ay = -r0i * fmaf(pi, gt.y, m0 * sy),
+                    az = -r0i * fmaf(pi, gt.z, m0 * sz);
         acc[i] = make_float4(ax, ay, az, 0.f);
         const float4 v = vel[i];
         const float nvx = v.x + dt * ax, nvy = v.y + dt * ay, nvz = v.z + dt * az;
