@@ -1,0 +1,196 @@
+"""Parity with the oracle on the benchmark workloads themselves, by particle
+ID: the 4,194,304-particle IISPH dam break of bench.py (2 main-loop steps in
+FP32 and in the mixed_pos16 headline mode), one in eight scenes of the
+256-scene batched PCISPH workload stepped as a batch, and captured (CUDA
+graph) IISPH and PCISPH steps. The oracle is the C++/OpenMP restatement of
+the reference's step (oracle/oracle.cpp)."""
+import numpy as np
+import pytest
+
+import oracle
+from reyn_b200 import scenes
+from tests.helpers import STEP_TOL, compare_steps, run_engine, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _bench_params(rb, sc, precision):
+    import bench
+    prm = bench.EngineRun.params(rb, sc, precision)
+    return prm
+
+
+@pytest.mark.parametrize("precision,scale", [("fp32", 1), ("mixed_pos16", 20)])
+def test_iisph_4m_steps_vs_oracle(cuda, precision, scale):
+    """The benchmark scene (host generator, bit-identical to the device one),
+    2 steps at dt 2e-4 with the benchmark's solver settings (average density
+    error <= 0.1 %, FP64 reduction). FP32 at the step tolerances; the mixed
+    mode at `scale` times them (its FP16 records); equal sweep counts."""
+    import bench
+    import reyn_b200 as rb
+
+    sc = bench.scene_for(0, 1)
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    bdy = dict(sc.bdy, m=bm)
+    steps, dt = 2, 2e-4
+    prm = _bench_params(rb, sc, precision)
+    got = run_engine(2, rb.C2, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, bench.NU,
+                     dt, steps, params=prm)
+    want = run_oracle(2, 0, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, bench.NU, dt,
+                      steps, params=bench.oracle_params(sc.h, sc.rho0))
+    assert got["iters"] == want["iters"]
+    tol = {k: (r * steps * scale, a * steps * scale) for k, (r, a) in STEP_TOL.items()}
+    compare_steps(got, want, 2, tol, f"iisph_4m/{precision}")
+
+
+def test_batched_pcisph_workload_scenes_vs_oracle(cuda):
+    """The batched PCISPH workload (256 cubes of log-uniform 2,000-200,000
+    particles, cubic B-spline, 1 % average density tolerance, dt 2e-4)
+    stepped as one batch for 3 steps; every eighth scene against the oracle
+    stepped alone in its own box, with equal sweep counts."""
+    import torch
+
+    import reyn_b200 as rb
+
+    b = scenes.batched_pcisph(n_scenes=256, seed=4)
+    n = int(b.first[-1])
+    steps, dt = 3, 2e-4
+
+    def params():
+        prm = rb.reference_params(rb.PCISPH, rb.B3, b.h, b.rho0, 0.01)
+        prm.eta = 0.01
+        prm.max_iter = 100
+        return prm
+
+    dev = torch.device("cuda")
+    st = rb.Particles(n, b.rho0)
+    st.upload(b.fluid)
+    ids = torch.tensor(b.fluid["id"], device=dev)
+    bd = rb.Boundary(*(torch.tensor(b.bdy[k], device=dev) for k in ("x", "y", "z")), None,
+                     h=b.h, rho0=b.rho0, scene_first=b.bfirst)
+    grid = rb.Grid(b.frame_min, b.frame_max, 2 * b.h, 0.5, 0, scene_first=b.first,
+                   scene_min=b.box_min, scene_max=b.box_max)
+    sv = rb.Solver(rb.PCISPH, params(), n)
+    its = []
+    for _ in range(steps):
+        grid.construct_and_reorder(st, [ids])
+        its.append(sv.step_batched(st, grid, bd, dt))
+    out = st.download()
+    out["id"] = ids.cpu().numpy()
+    buf = sv.buffers()
+    for k in ("rho", "p", "aii", "sii", "ax", "ay", "az"):
+        out[k] = rb.device_to_numpy(getattr(buf, k), n)
+    for o in (sv, grid, bd, st):
+        o.close()
+    its = np.array(its)
+    ids_all = out["id"].astype(np.int64)
+    tol = {k: (r * steps * 10, a * steps * 10) for k, (r, a) in STEP_TOL.items()}
+    oprm = oracle.reference_params(1, 1, b.h, b.rho0, 0.01)
+    oprm.eta = 0.01
+    oprm.max_iter = 100
+    for s in range(0, 256, 8):
+        a0, a1 = int(b.first[s]), int(b.first[s + 1])
+        c0, c1 = int(b.bfirst[s]), int(b.bfirst[s + 1])
+        fl = {k: v[a0:a1] for k, v in b.fluid.items()}
+        wall = {k: b.bdy[k][c0:c1] for k in ("x", "y", "z")}
+        wall["m"] = oracle.boundary_masses(wall["x"], wall["y"], wall["z"], b.h, b.rho0, 5)
+        want = run_oracle(1, 1, fl, wall, b.box_min[s], b.box_max[s], b.h, b.rho0, 0.01, dt,
+                          steps, params=oprm)
+        sel = (ids_all >= int(fl["id"].min())) & (ids_all <= int(fl["id"].max()))
+        got = {k: v[sel] for k, v in out.items()}
+        assert sel.sum() == a1 - a0
+        assert list(its[:, s]) == list(want["iters"]), (s, its[:, s], want["iters"])
+        compare_steps(got, want, 1, tol, f"batched_pcisph scene {s}")
+
+
+@pytest.mark.parametrize("scheme,kind,precision", [("IISPH", "C2", "FP32"),
+                                                   ("IISPH", "C2", "MIXED_POS16"),
+                                                   ("PCISPH", "B3", "FP32")])
+def test_captured_steps_vs_oracle(cuda, scheme, kind, precision):
+    """Steps replayed from a captured step graph (grid build + reorder +
+    bounded solver step at a fixed dt, the pressure loop decided on the
+    device) against the oracle; particles are matched by position (the
+    graph carries no ID array), which the step tolerances leave unambiguous
+    at this spacing."""
+    import torch
+    from scipy.spatial import cKDTree
+
+    import reyn_b200 as rb
+
+    sch, knd = getattr(rb, scheme), getattr(rb, kind)
+    sc = scenes.dam_break((16, 14, 12), 0.02, (0.5, 0.5, 0.5), velocity_noise=0.05, seed=8)
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    bdy = dict(sc.bdy, m=bm)
+    steps, dt = 3, 1e-3
+    st = rb.Particles(sc.n, sc.rho0)
+    st.upload(sc.fluid)
+    bd = rb.Boundary(*(torch.tensor(sc.bdy[k], device="cuda") for k in ("x", "y", "z")),
+                     torch.tensor(bm, device="cuda"), h=sc.h, rho0=sc.rho0)
+    grid = rb.Grid(sc.box_min, sc.box_max, 2 * sc.h)
+    prm = rb.reference_params(sch, knd, sc.h, sc.rho0, 0.01)
+    prm.precision = getattr(rb, "PRECISION_" + precision)
+    sv = rb.Solver(sch, prm, sc.n)
+    g = rb.StepGraph(sv, st, grid, bd, dt, bounds=(sc.box_min, sc.box_max))
+    iters = []
+    for _ in range(steps):
+        g.launch()
+        iters.append(g.stats().iters)
+    got = st.download()
+    g.close()
+    for o in (sv, grid, bd, st):
+        o.close()
+    want = run_oracle(sch, 0 if kind == "C2" else 1, sc.fluid, bdy, sc.box_min, sc.box_max,
+                      sc.h, sc.rho0, 0.01, dt, steps)
+    assert iters == [int(x) for x in want["iters"]]
+    gp = np.stack([got[k] for k in ("x", "y", "z")], 1).astype(np.float64)
+    wp = np.stack([want[k] for k in ("x", "y", "z")], 1).astype(np.float64)
+    d, idx = cKDTree(wp).query(gp)
+    assert d.max() < 1e-3 * sc.h
+    assert np.unique(idx).size == sc.n
+    scale = 20 if precision != "FP32" else 1
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        rtol, af = STEP_TOL[k]
+        w = np.asarray(want[k])[idx]
+        err = np.abs(got[k] - w)
+        lim = steps * scale * (af * np.abs(w).max() + rtol * np.abs(w))
+        assert np.all(err <= lim), (k, float(err.max()))
+
+
+def test_sesph_config_gravity_z_vs_oracle(cuda):
+    """The SESPH dam break as its configuration states it: 32^3 particles at
+    spacing 0.02, cubic B-spline, stiffness 1000, viscosity 0.01, gravity
+    -9.81 along z, dt 5e-4. Five steps by particle ID at the step
+    tolerances, then 200 steps in aggregate (per-particle paths diverge
+    chaotically over long runs): centre of mass, mean density, kinetic
+    energy."""
+    import reyn_b200 as rb
+
+    sc = scenes.sesph_small()
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    bdy = dict(sc.bdy, m=bm)
+    prm = rb.reference_params(rb.SESPH, rb.B3, sc.h, sc.rho0, 0.01)
+    prm.k_sesph = 1000.0
+    prm.g[0], prm.g[1], prm.g[2] = 0.0, 0.0, -9.81
+    oprm = oracle.reference_params(0, 1, sc.h, sc.rho0, 0.01)
+    oprm.k_sesph = 1000.0
+    oprm.g[0], oprm.g[1], oprm.g[2] = 0.0, 0.0, -9.81
+    dt = 5e-4
+    got = run_engine(0, 1, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, 0.01, dt, 5,
+                     params=prm)
+    want = run_oracle(0, 1, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, 0.01, dt, 5,
+                      params=oprm)
+    tol = {k: (r * 5, a * 5) for k, (r, a) in STEP_TOL.items()}
+    compare_steps(got, want, 0, tol, "sesph_32k/gravity_z")
+    got = run_engine(0, 1, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, 0.01, dt, 200,
+                     params=prm)
+    want = run_oracle(0, 1, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, 0.01, dt,
+                      200, params=oprm)
+    print({k: (float(got[k].mean()), float(want[k].mean())) for k in ("x", "y", "z", "rho")})
+    # the block has fallen along z: its centre moved down by about two spacings
+    assert want["z"].mean() < sc.fluid["z"].mean() - 0.02
+    for k in ("x", "y", "z"):
+        assert abs(got[k].mean() - want[k].mean()) < 2e-4, k
+    assert abs(got["rho"].mean() - want["rho"].mean()) < 1e-3 * sc.rho0
+    ke_g = float((got["vx"] ** 2 + got["vy"] ** 2 + got["vz"] ** 2).sum())
+    ke_w = float((want["vx"] ** 2 + want["vy"] ** 2 + want["vz"] ** 2).sum())
+    assert abs(ke_g - ke_w) < 0.02 * ke_w
