@@ -189,7 +189,7 @@ int reyn_grid_create(const float bound_min[3], const float bound_max[3], float s
         g->counts.resize(C);
         REYN_CUDA(cudaMemset(g->counts.get(), 0, C * sizeof(uint32_t)));
         g->prefix.resize(C + 1);
-        g->status.resize(1);
+        g->status.resize(3);
         *out = g.release();
     });
 }
@@ -226,7 +226,7 @@ int reyn_grid_create_batched(float search_radius, float cell_ratio, reyn_cell_or
         g->counts.resize(C);
         REYN_CUDA(cudaMemset(g->counts.get(), 0, C * sizeof(uint32_t)));
         g->prefix.resize(C + 1);
-        g->status.resize(1);
+        g->status.resize(3);
         *out = g.release();
     });
 }
@@ -265,7 +265,8 @@ int reyn_grid_construct_and_reorder(reyn_grid* g, float search_radius, reyn_part
         check_radius(g, search_radius);
         require(n_extra == 0 || extra != nullptr, "null extra array list");
         const cudaStream_t s = as_stream(stream);
-        g->build(state->cur[FX].get(), state->cur[FY].get(), state->cur[FZ].get(), state->n, s);
+        g->build(state->cur[FX].get(), state->cur[FY].get(), state->cur[FZ].get(), state->n, s,
+            state);
         reorder_state(*state, *g, extra, n_extra, s);
         g->check_status(s, "construct_and_reorder");
     });

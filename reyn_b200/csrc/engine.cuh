@@ -79,8 +79,9 @@ struct Grid {
     DevArray<uint32_t> keys;   // n
     DevArray<uint32_t> slots;  // n, unordered counting-sort output
     DevArray<uint32_t> sorted; // n, canonical order (the permutation)
+    DevArray<uint32_t> split;  // n, particles of cells split across warps
     DevArray<uint32_t> scan_part;
-    DevArray<uint32_t> status; // 1 word of StatusBits
+    DevArray<uint32_t> status; // StatusBits, the split-cell particle count, pre-key StatusBits
     DevArray<float> extra_tmp; // reorder staging of caller arrays
     mutable DevArray<float4> pts_tmp; // packed positions for statistics
     uint32_t n = 0;
@@ -104,12 +105,25 @@ struct Grid {
     const reyn_particles* reordered_state = nullptr;
     uint64_t reorder_epoch = 0; // state epoch produced by that reorder
     const float* built_pos[3] = { nullptr, nullptr, nullptr }; // positions of the last build
+    // Keys and histogram of the next build, computed by the integrating
+    // kernel of a solver step on this grid's reordered state (status word 2
+    // holds that kernel's status bits): valid while the state is unchanged
+    // since (same arrays and version).
+    bool prekey_pending = false;
+    const reyn_particles* prekey_state = nullptr;
+    uint64_t prekey_version = 0;
+    const float* prekey_x = nullptr;
+    uint32_t prekey_n = 0;
 
     GridView view(float search_radius) const;
     // counting-sort build over positions: keys, counts, prefix, canonical
-    // `sorted`; flags particles outside the grid in `status`
+    // `sorted`; flags particles outside the grid in `status`. With `st` (the
+    // state whose current positions x, y, z are) a pending pre-keyed
+    // histogram of that state is used instead of computing the keys.
     void build(const float* x, const float* y, const float* z, uint32_t n,
-        cudaStream_t s);
+        cudaStream_t s, const reyn_particles* st = nullptr);
+    // drops a pending pre-keyed histogram (its counts are cleared)
+    void drop_prekey(cudaStream_t s);
     // host check of the status word (synchronises)
     void check_status(cudaStream_t s, const char* what);
 };
@@ -205,7 +219,7 @@ void launch_gather(uint32_t n, const uint32_t* perm, const GatherArgs& a,
 // exclusive prefix sum of C counts into out[0..C] (out[C] = total); `part`
 // holds the per-tile partials
 void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& part, uint32_t* out,
-    cudaStream_t s);
+    cudaStream_t s, uint32_t* fold_status = nullptr);
 
 // packs the particle arrays into pm/vel (after a direct SoA write)
 void pack_state(reyn_particles& st, cudaStream_t s);

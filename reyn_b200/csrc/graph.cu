@@ -138,6 +138,10 @@ void capture(reyn_step_graph& gr, int k)
     gr.ctx.top_names.clear();
     gr.ctx.body_names.clear();
     const cudaStream_t s = gr.cap;
+    // the captured build computes its own keys: a histogram pre-keyed by
+    // the last plain step is cleared before the capture starts
+    g.drop_prekey(s);
+    REYN_CUDA(cudaStreamSynchronize(s));
     REYN_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
     sv.graph = &gr.ctx;
     profile_record(&gr.ctx.top_names);
@@ -281,6 +285,7 @@ extern "C" int reyn_step_graph_launch(reyn_step_graph* gr, void* stream)
             require(sv.p_state == &st && sv.p_epoch == st.epoch,
                 "the solver's pressure does not follow this state (create a new graph)");
         const cudaStream_t s = as_stream(stream);
+        g.drop_prekey(s); // the replayed build computes its own keys
         REYN_CUDA(cudaGraphLaunch(gr->exec[k], s));
         // the host side of the replayed step: the reorder's swap and epochs,
         // the grid's ordering, the solver's pressure and max |v|

@@ -151,6 +151,81 @@ __global__ void k_canonical(uint32_t n, const uint32_t* __restrict__ slots,
     sorted[st + rank] = p;
 }
 
+// counting-sort scatter straight into the canonical order (uniformgrid.cu:
+// 40-63, with the order inside a cell made deterministic: ascending index).
+// A warp's lanes hold consecutive indices, so a cell whose particles all lie
+// in one warp (its count, prefix[key + 1] - prefix[key], equals the number of
+// lanes holding its key) is placed by lane rank; the leader returns the
+// cell's counter to zero. A cell split across warps takes counting-sort
+// slots (atomicSub, which also returns its counter to zero) into `slots`,
+// and its particles are listed in `split` (count in *nsplit) for
+// k_rank_split. In a state reordered by the previous step's grid nearly
+// every cell is whole.
+__global__ void k_scatter_stable(uint32_t n, const uint32_t* __restrict__ keys,
+    const uint32_t* __restrict__ prefix, uint32_t* __restrict__ counts,
+    uint32_t* __restrict__ slots, uint32_t* __restrict__ sorted, uint32_t* __restrict__ split,
+    uint32_t* __restrict__ nsplit)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t key = valid ? keys[i] : 0xffffffffu;
+    const unsigned group = __match_any_sync(0xffffffffu, key);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(group) - 1;
+    const uint32_t g = __popc(group);
+    const uint32_t rank = __popc(group & ((1u << lane) - 1u));
+    uint32_t st = 0, tot = 0;
+    if (valid) {
+        st = prefix[key];
+        tot = prefix[key + 1] - st;
+    }
+    const bool whole = valid && g == tot;
+    uint32_t top = 0;
+    if (valid && lane == leader) {
+        if (whole)
+            counts[key] = 0u;
+        else
+            top = atomicSub(counts + key, g);
+    }
+    top = __shfl_sync(0xffffffffu, top, leader);
+    if (valid) {
+        if (whole)
+            sorted[st + rank] = i;
+        else
+            slots[st + top - g + rank] = i;
+    }
+    const unsigned sm = __ballot_sync(0xffffffffu, valid && !whole);
+    if (sm) {
+        const int first = __ffs(sm) - 1;
+        uint32_t base = 0;
+        if (lane == first)
+            base = atomicAdd(nsplit, uint32_t(__popc(sm)));
+        base = __shfl_sync(0xffffffffu, base, first);
+        if (valid && !whole)
+            split[base + __popc(sm & ((1u << lane) - 1u))] = i;
+    }
+}
+
+// the canonical place of each particle of a split cell: its cell's start plus
+// the number of smaller indices among the cell's slots (grid-stride over the
+// split list, whose length is known on the device only)
+__global__ void k_rank_split(const uint32_t* __restrict__ nsplit,
+    const uint32_t* __restrict__ split, const uint32_t* __restrict__ slots,
+    const uint32_t* __restrict__ keys, const uint32_t* __restrict__ prefix,
+    uint32_t* __restrict__ sorted)
+{
+    const uint32_t m = *nsplit;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < m; t += gridDim.x * blockDim.x) {
+        const uint32_t p = split[t];
+        const uint32_t key = keys[p];
+        const uint32_t st = prefix[key], en = prefix[key + 1];
+        uint32_t rank = 0;
+        for (uint32_t q = st; q < en; ++q)
+            rank += (slots[q] < p) ? 1u : 0u;
+        sorted[st + rank] = p;
+    }
+}
+
 // ---- exclusive scan over all cells ----------------------------------------
 // Three passes over tiles of SCAN_TILE counts: tile sums, a single-block scan
 // of the tile sums, and the tile scans with their offsets. The last entry
@@ -214,8 +289,14 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
 }
 
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(
-    const uint32_t* __restrict__ in, int64_t C, uint32_t* __restrict__ part)
+    const uint32_t* __restrict__ in, int64_t C, uint32_t* __restrict__ part,
+    uint32_t* __restrict__ fold_status)
 {
+    // a pre-keyed build: the keys' status bits (word 2) become the build's
+    if (fold_status && blockIdx.x == 0 && threadIdx.x == 0) {
+        fold_status[0] = fold_status[2];
+        fold_status[2] = 0u;
+    }
     const int64_t base = int64_t(blockIdx.x) * SCAN_TILE + int64_t(threadIdx.x) * SCAN_PER_THREAD;
     uint32_t v[SCAN_PER_THREAD];
     load_tile_chunk(in, C, base, v);
@@ -283,23 +364,37 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(
 }
 
 void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& part,
-    uint32_t* out, cudaStream_t s)
+    uint32_t* out, cudaStream_t s, uint32_t* fold_status)
 {
     const uint32_t nparts = (uint32_t)((C + SCAN_TILE - 1) / SCAN_TILE);
     part.resize(size_t(nparts) + 1);
     REYN_KERNEL("k_scan_tiles", s,
-        k_scan_tiles<<<nparts, SCAN_THREADS, 0, s>>>(in, C, part.get()));
+        k_scan_tiles<<<nparts, SCAN_THREADS, 0, s>>>(in, C, part.get(), fold_status));
     REYN_KERNEL("k_scan_parts", s,
         k_scan_parts<<<1, SCAN_THREADS, 0, s>>>(part.get(), nparts));
     REYN_KERNEL("k_scan_apply", s,
         k_scan_apply<<<nparts, SCAN_THREADS, 0, s>>>(in, C, part.get(), nparts, out));
 }
 
+void Grid::drop_prekey(cudaStream_t s)
+{
+    if (prekey_pending) {
+        counts.zero(s);
+        prekey_pending = false;
+    }
+}
+
 void Grid::build(const float* x, const float* y, const float* z, uint32_t np,
-    cudaStream_t s)
+    cudaStream_t s, const reyn_particles* st)
 {
     const int64_t C = total_keys();
     require(!n_scenes || np == first[n_scenes], "particle count differs from the scenes' total");
+    const bool prekeyed = prekey_pending && st && st == prekey_state
+        && st->version == prekey_version && x == prekey_x && np == prekey_n
+        && counts.size() == size_t(C) && !counts_dirty;
+    if (!prekeyed)
+        drop_prekey(s);
+    prekey_pending = false;
     if (counts.size() != size_t(C) || counts_dirty) {
         // the scatter returns every count to zero; only a fresh array or an
         // interrupted build needs clearing
@@ -308,13 +403,16 @@ void Grid::build(const float* x, const float* y, const float* z, uint32_t np,
         prefix.resize(size_t(C) + 1);
         counts_dirty = false;
     }
-    if (status.size() == 0)
-        status.resize(1);
-    status.zero(s);
+    if (status.size() < 3)
+        status.resize(3);
+    // the status bits and the split-cell count (a pre-keyed build keeps word
+    // 2, the keys' status, which the scan folds into word 0)
+    REYN_CUDA(cudaMemsetAsync(status.get(), 0, (prekeyed ? 2 : 3) * sizeof(uint32_t), s));
     n = np;
     keys.resize(np);
     slots.resize(np);
     sorted.resize(np);
+    split.resize(np);
     reordered = false;
     reordered_state = nullptr;
     built_pos[0] = x;
@@ -322,19 +420,23 @@ void Grid::build(const float* x, const float* y, const float* z, uint32_t np,
     built_pos[2] = z;
     const GridView g = view(geom.r);
     counts_dirty = true;
-    if (np) {
+    if (np && !prekeyed) {
         REYN_KERNEL("k_keys_count", s,
             k_keys_count<<<blocks_for(np, THREADS), THREADS, 0, s>>>(
             np, x, y, z, g, keys.get(), counts.get(), status.get()));
     }
-    exclusive_scan(counts.get(), C, scan_part, prefix.get(), s);
+    exclusive_scan(counts.get(), C, scan_part, prefix.get(), s,
+        prekeyed ? status.get() : nullptr);
     if (np) {
         REYN_KERNEL("k_scatter", s,
-            k_scatter<<<blocks_for(np, THREADS), THREADS, 0, s>>>(
-            np, keys.get(), prefix.get(), counts.get(), slots.get()));
-        REYN_KERNEL("k_canonical", s,
-            k_canonical<<<blocks_for(np, THREADS), THREADS, 0, s>>>(
-            np, slots.get(), keys.get(), prefix.get(), sorted.get()));
+            k_scatter_stable<<<blocks_for(np, THREADS), THREADS, 0, s>>>(np, keys.get(),
+            prefix.get(), counts.get(), slots.get(), sorted.get(), split.get(),
+            status.get() + 1));
+        // split cells are rare: a small fixed grid walks their list
+        REYN_KERNEL("k_rank_split", s,
+            k_rank_split<<<std::min<unsigned>(blocks_for(np, THREADS), 2 * 148), THREADS, 0,
+            s>>>(status.get() + 1, split.get(), slots.get(), keys.get(), prefix.get(),
+            sorted.get()));
     }
     counts_dirty = false;
 }

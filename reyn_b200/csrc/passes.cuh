@@ -715,7 +715,34 @@ struct Tail {
     const uint16_t* sid;
     const float* lo_s;
     const float* hi_s;
+    // the next build of the step's grid, pre-keyed (keys != nullptr): each
+    // stored position's cell key and the per-cell histogram, as that build's
+    // k_keys_count would compute them (uniformgrid.cu:20-34), status bits to
+    // kstatus
+    GridView kg;
+    uint32_t* keys;
+    uint32_t* counts;
+    uint32_t* kstatus;
 };
+
+// the cell key of a stored position and its histogram count (k_keys_count's
+// arithmetic: IEEE division, clamping and status of points outside the grid)
+__device__ __forceinline__ void prekey(const Tail& t, uint32_t i, float px, float py, float pz)
+{
+    int3 c = cell_of(t.kg, px, py, pz);
+    const bool finite = isfinite(px) && isfinite(py) && isfinite(pz);
+    const bool inside = finite && c.x >= 0 && c.y >= 0 && c.z >= 0 && c.x < t.kg.nx
+        && c.y < t.kg.ny && c.z < t.kg.nz;
+    if (!inside) {
+        atomicOr(t.kstatus, finite ? STATUS_OUT_OF_GRID : STATUS_NONFINITE);
+        c = finite ? make_int3(min(max(c.x, 0), t.kg.nx - 1), min(max(c.y, 0), t.kg.ny - 1),
+                         min(max(c.z, 0), t.kg.nz - 1))
+                   : make_int3(0, 0, 0);
+    }
+    const uint32_t key = cell_key(t.kg, c.x, c.y, c.z);
+    t.keys[i] = key;
+    atomicAdd(t.counts + key, 1u);
+}
 
 // stores the new state of particle i (bounds applied when tail.vmax is set)
 // and returns |v| of what was stored
@@ -751,6 +778,8 @@ __device__ __forceinline__ float store_state(const Tail& t, uint32_t i, float px
     x[i] = px;
     y[i] = py;
     z[i] = pz;
+    if (!BATCH && t.keys)
+        prekey(t, i, px, py, pz);
     return t.vmax ? norm3df(nvx, nvy, nvz) : 0.f; // cfl.cu:13-18
 }
 
@@ -1486,6 +1515,17 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             tail.hi_s = grid.scene_hi.get();
         }
     }
+    // a bounded step on the grid's own reordered state (not captured, not a
+    // batch) computes the keys and histogram of that grid's next build
+    const bool prekeyed = tail.vmax && !gx && !ns && !shadow && grid.n == n
+        && grid.reordered_state == &st && !grid.counts_dirty && !grid.prekey_pending
+        && grid.counts.size() == size_t(grid.total_keys()) && grid.status.size() >= 3;
+    if (prekeyed) {
+        tail.kg = grid.view(grid.geom.r);
+        tail.keys = grid.keys.get();
+        tail.counts = grid.counts.get();
+        tail.kstatus = grid.status.get() + 2;
+    }
     const unsigned bs = P.block_size ? P.block_size : NBR_THREADS;
     const unsigned nb = blocks_for(n, bs);
     const float rho0 = P.rho0;
@@ -1862,6 +1902,14 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         sv.ay.get(), sv.az.get()));
     st.packed_valid = false; // positions moved: the packed copy is stale
     st.version += 1;
+    if (prekeyed) {
+        Grid& gm = const_cast<Grid&>(grid);
+        gm.prekey_pending = true;
+        gm.prekey_state = &st;
+        gm.prekey_version = st.version;
+        gm.prekey_x = st.cur[FX].get();
+        gm.prekey_n = n;
+    }
     if (tail.vmax) {
         if (!gx) { // a captured step records these after each launch
             REYN_CUDA(cudaMemcpyAsync(sv.vmax_host->get(), tail.vmax, sizeof(float),
