@@ -465,7 +465,7 @@ __device__ __forceinline__ void for_each_rec(const Fluid& f, const KernelConst& 
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const float3 d = delta16(o, r[u]);
-                fn(j[u], r[u], d, pair_g<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
+                fn(j[u], r[u], d, pair_g_vec<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
             }
         }
 #pragma unroll
@@ -473,7 +473,7 @@ __device__ __forceinline__ void for_each_rec(const Fluid& f, const KernelConst& 
             if (k + u < cnt) {
                 const uint4 r = __ldg(rec + jn[u]);
                 const float3 d = delta16(o, r);
-                fn(jn[u], r, d, pair_g<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
+                fn(jn[u], r, d, pair_g_vec<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
             }
         }
     } else {
@@ -802,6 +802,57 @@ __device__ __forceinline__ void tail_reduce(const Tail& t, float v)
     }
 }
 
+// ---- batched scenes: persistent launches over the active tiles --------------
+// The sweeps of a batch's pressure loop (PCISPH prediction and pressure,
+// IISPH pressure accelerations and Jacobi) run as persistent launches: a
+// fixed grid of blocks walks the tiles (blockDim.x consecutive particles) in
+// order, block b taking tiles b, b + gridDim.x, ..., and skips a tile whose
+// scenes have all converged, so converged scenes cost a few loads per tile
+// and the equal-sized tiles spread the remaining work evenly over the SMs
+// whatever the scenes' sizes. Tiles are walked in index order (neighbouring
+// blocks work on neighbouring tiles, which share neighbour data in the L2).
+struct Tiles {
+    const uint16_t* sid;   // scene of each particle
+    const uint8_t* active; // per scene: still iterating
+    uint32_t n;            // particles
+    uint32_t count;        // tiles: ceil(n / blockDim.x)
+};
+
+// whether tile t holds a particle of a scene still iterating (the same value
+// in every thread of the block)
+__device__ __forceinline__ bool tile_active(const Tiles& tl, uint32_t t)
+{
+    const uint32_t first = t * blockDim.x;
+    const uint32_t last = min(first + blockDim.x, tl.n) - 1u;
+    for (uint32_t s = __ldg(tl.sid + first), e = __ldg(tl.sid + last); s <= e; ++s)
+        if (__ldg(tl.active + s))
+            return true;
+    return false;
+}
+
+// blocks of a persistent launch of `kern`: as many as the SMs hold at once
+// (its occupancy at bs threads), at most one per tile
+template <class Kern>
+unsigned persistent_grid(Kern kern, unsigned bs, unsigned tiles)
+{
+    int dev = 0, sms = 0, per_sm = 0;
+    REYN_CUDA(cudaGetDevice(&dev));
+    REYN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    REYN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, int(bs), 0));
+    return std::max(1u, std::min(tiles, unsigned(sms) * unsigned(std::max(per_sm, 1))));
+}
+
+// the persistent loop of a tile kernel: `body` runs for particle i of every
+// active tile assigned to this block (all threads of a block take the same
+// iterations, so bodies may synchronise the block)
+#define REYN_TILE_LOOP(tl, body)                                                \
+    for (uint32_t t_ = blockIdx.x; t_ < (tl).count; t_ += gridDim.x) {           \
+        if (!tile_active(tl, t_))                                              \
+            continue;                                                          \
+        const uint32_t i = t_ * blockDim.x + threadIdx.x;                       \
+        body;                                                                  \
+    }
+
 // ---- passes ----------------------------------------------------------------
 
 // compute_densities (solver.cuh:18-38) + cached boundary sums + the step's
@@ -948,12 +999,14 @@ __global__ void __launch_bounds__(MB) k_sesph(uint32_t n, Fluid f,
 
 // predict_rho (solver.cuh:71-105); the boundary part uses the cached sums:
 // sum_b m_b (W + dt grad W . v_i) = rho_b + dt g_b . v_i
-template <int KIND, int R, bool BATCH = false, int MB = NBR_THREADS>
-__global__ void __launch_bounds__(MB) k_pcisph_predict(uint32_t n, Fluid f,
-    const float4* __restrict__ vel, const float4* __restrict__ bterm, float dt,
-    float* __restrict__ rho, float k, float rho0, float* __restrict__ pr, SweepStats* stats)
+#define REYN_PCISPH_PREDICT_ARGS uint32_t n, Fluid f, const float4* __restrict__ vel, \
+    const float4* __restrict__ bterm, float dt, float* __restrict__ rho, float k, float rho0, \
+    float* __restrict__ pr, SweepStats* stats
+#define REYN_PCISPH_PREDICT_PASS n, f, vel, bterm, dt, rho, k, rho0, pr, stats
+
+template <int KIND, int R, bool BATCH>
+__device__ __forceinline__ void pcisph_predict(uint32_t i, REYN_PCISPH_PREDICT_ARGS)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 0.0;
     constexpr bool batched = BATCH;
     uint32_t sc = 0;
@@ -991,14 +1044,28 @@ __global__ void __launch_bounds__(MB) k_pcisph_predict(uint32_t n, Fluid f,
         block_accumulate(stats, 0u, 0.0, contrib, 0.f);
 }
 
-// _write_pcisph_prs_acc (PCISPH.cu:21-56) + v += dt a in place
 template <int KIND, int R, bool BATCH = false, int MB = NBR_THREADS>
-__global__ void __launch_bounds__(MB) k_pcisph_pressure(uint32_t n, Fluid f,
-    const float* __restrict__ rho, const float* __restrict__ pr,
-    const float4* __restrict__ bterm, float k, float rho0,
-    float r0i, float dt, float4* __restrict__ acc, float4* __restrict__ vel)
+__global__ void __launch_bounds__(MB) k_pcisph_predict(REYN_PCISPH_PREDICT_ARGS)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    pcisph_predict<KIND, R, BATCH>(blockIdx.x * blockDim.x + threadIdx.x,
+        REYN_PCISPH_PREDICT_PASS);
+}
+
+template <int KIND, int R, int MB>
+__global__ void __launch_bounds__(MB) k_pcisph_predict_tiles(REYN_PCISPH_PREDICT_ARGS, Tiles tl)
+{
+    REYN_TILE_LOOP(tl, (pcisph_predict<KIND, R, true>(i, REYN_PCISPH_PREDICT_PASS)));
+}
+
+// _write_pcisph_prs_acc (PCISPH.cu:21-56) + v += dt a in place
+#define REYN_PCISPH_PRESSURE_ARGS uint32_t n, Fluid f, const float* __restrict__ rho, \
+    const float* __restrict__ pr, const float4* __restrict__ bterm, float k, float rho0, \
+    float r0i, float dt, float4* __restrict__ acc, float4* __restrict__ vel
+#define REYN_PCISPH_PRESSURE_PASS n, f, rho, pr, bterm, k, rho0, r0i, dt, acc, vel
+
+template <int KIND, int R, bool BATCH>
+__device__ __forceinline__ void pcisph_pressure(uint32_t i, REYN_PCISPH_PRESSURE_ARGS)
+{
     if (i >= n)
         return;
     if constexpr (BATCH) {
@@ -1028,6 +1095,19 @@ __global__ void __launch_bounds__(MB) k_pcisph_pressure(uint32_t n, Fluid f,
     v.y += dt * ay;
     v.z += dt * az;
     vel[i] = v;
+}
+
+template <int KIND, int R, bool BATCH = false, int MB = NBR_THREADS>
+__global__ void __launch_bounds__(MB) k_pcisph_pressure(REYN_PCISPH_PRESSURE_ARGS)
+{
+    pcisph_pressure<KIND, R, BATCH>(blockIdx.x * blockDim.x + threadIdx.x,
+        REYN_PCISPH_PRESSURE_PASS);
+}
+
+template <int KIND, int R, int MB>
+__global__ void __launch_bounds__(MB) k_pcisph_pressure_tiles(REYN_PCISPH_PRESSURE_ARGS, Tiles tl)
+{
+    REYN_TILE_LOOP(tl, (pcisph_pressure<KIND, R, true>(i, REYN_PCISPH_PRESSURE_PASS)));
 }
 
 // the final position update of integrate (solver.cu:15-32) when v already
@@ -1155,11 +1235,10 @@ __global__ void __launch_bounds__(MB) k_iisph_diag_pacc(uint32_t n, Fluid f,
 
 // _set_pressure_accelerations (IISPH.cu:68-98)
 template <int KIND, int R, int MIX, bool BATCH>
-__device__ __forceinline__ void iisph_pacc(uint32_t n, const Fluid& f,
+__device__ __forceinline__ void iisph_pacc(uint32_t i, uint32_t n, const Fluid& f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     float4* __restrict__ acc, uint2* __restrict__ acch_out, const uint32_t* __restrict__ gate)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     // a captured step's loop body: the first sweep uses the accelerations of
     // the pass before the loop
     if (i >= n || (gate && !*gate))
@@ -1190,12 +1269,11 @@ __device__ __forceinline__ void iisph_pacc(uint32_t n, const Fluid& f,
 // reference becomes a count of particles above the threshold, reduced per
 // block together with the FP64 sum of max(0, error)
 template <int KIND, int R, int MIX, bool BATCH>
-__device__ __forceinline__ void iisph_jacobi(uint32_t n, const Fluid& f,
+__device__ __forceinline__ void iisph_jacobi(uint32_t i, uint32_t n, const Fluid& f,
     const float4* __restrict__ acc, const float4* __restrict__ bterm,
     const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
     float dt, float omega, float tiny, float thr, SweepStats* stats)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned over = 0;
     double epos = 0.0;
     float emax = 0.f;
@@ -1250,7 +1328,8 @@ __global__ void __launch_bounds__(MB) k_iisph_pacc(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     float4* __restrict__ acc, uint2* __restrict__ acch_out, const uint32_t* __restrict__ gate)
 {
-    iisph_pacc<KIND, R, MIX, BATCH>(n, f, p, bterm, r0i, acc, acch_out, gate);
+    iisph_pacc<KIND, R, MIX, BATCH>(blockIdx.x * blockDim.x + threadIdx.x, n, f, p, bterm, r0i,
+        acc, acch_out, gate);
 }
 
 template <int KIND, int R, int MIX = 0, bool BATCH = false, int MB = NBR_THREADS>
@@ -1259,7 +1338,28 @@ __global__ void __launch_bounds__(MB) k_iisph_jacobi(uint32_t n, Fluid f,
     const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
     float dt, float omega, float tiny, float thr, SweepStats* stats)
 {
-    iisph_jacobi<KIND, R, MIX, BATCH>(n, f, acc, bterm, aii, sii, p, dt, omega, tiny, thr, stats);
+    iisph_jacobi<KIND, R, MIX, BATCH>(blockIdx.x * blockDim.x + threadIdx.x, n, f, acc, bterm,
+        aii, sii, p, dt, omega, tiny, thr, stats);
+}
+
+template <int KIND, int R, int MIX, int MB>
+__global__ void __launch_bounds__(MB) k_iisph_pacc_tiles(uint32_t n, Fluid f,
+    const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
+    float4* __restrict__ acc, uint2* __restrict__ acch_out, const uint32_t* __restrict__ gate,
+    Tiles tl)
+{
+    REYN_TILE_LOOP(tl, (iisph_pacc<KIND, R, MIX, true>(i, n, f, p, bterm, r0i, acc, acch_out,
+        gate)));
+}
+
+template <int KIND, int R, int MIX, int MB>
+__global__ void __launch_bounds__(MB) k_iisph_jacobi_tiles(uint32_t n, Fluid f,
+    const float4* __restrict__ acc, const float4* __restrict__ bterm,
+    const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
+    float dt, float omega, float tiny, float thr, SweepStats* stats, Tiles tl)
+{
+    REYN_TILE_LOOP(tl, (iisph_jacobi<KIND, R, MIX, true>(i, n, f, acc, bterm, aii, sii, p, dt,
+        omega, tiny, thr, stats)));
 }
 
 // The mixed modes' sweep kernels for one scene and the polynomial kernels,
@@ -1276,7 +1376,8 @@ __global__ void __launch_bounds__(MB, (65536 / 40) / MB) k_iisph_pacc_occ(uint32
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
     float4* __restrict__ acc, uint2* __restrict__ acch_out, const uint32_t* __restrict__ gate)
 {
-    iisph_pacc<KIND, R, MIX, false>(n, f, p, bterm, r0i, acc, acch_out, gate);
+    iisph_pacc<KIND, R, MIX, false>(blockIdx.x * blockDim.x + threadIdx.x, n, f, p, bterm, r0i,
+        acc, acch_out, gate);
 }
 
 template <int KIND, int R, int MIX, int MB>
@@ -1285,25 +1386,43 @@ __global__ void __launch_bounds__(MB, (65536 / 40) / MB) k_iisph_jacobi_occ(uint
     const float* __restrict__ aii, const float* __restrict__ sii, float* __restrict__ p,
     float dt, float omega, float tiny, float thr, SweepStats* stats)
 {
-    iisph_jacobi<KIND, R, MIX, false>(n, f, acc, bterm, aii, sii, p, dt, omega, tiny, thr, stats);
+    iisph_jacobi<KIND, R, MIX, false>(blockIdx.x * blockDim.x + threadIdx.x, n, f, acc, bterm,
+        aii, sii, p, dt, omega, tiny, thr, stats);
 }
 
+// a batch's sweeps: persistent launches over the active tiles (tl)
 template <int KIND, int R, int MIX, bool BATCH, int MB, class... A>
-void launch_iisph_pacc(unsigned nb, unsigned bs, cudaStream_t q, A... a)
+void launch_iisph_pacc(unsigned nb, unsigned bs, cudaStream_t q, Tiles tl, bool persist,
+    A... a)
 {
-    if constexpr (!BATCH && occupancy_variant<KIND, MIX>)
+    if constexpr (BATCH) {
+        if (persist)
+            k_iisph_pacc_tiles<KIND, R, MIX, MB><<<persistent_grid(
+                k_iisph_pacc_tiles<KIND, R, MIX, MB>, bs, nb), bs, 0, q>>>(a..., tl);
+        else
+            k_iisph_pacc<KIND, R, MIX, BATCH, MB><<<nb, bs, 0, q>>>(a...);
+    } else if constexpr (occupancy_variant<KIND, MIX>) {
         k_iisph_pacc_occ<KIND, R, MIX, MB><<<nb, bs, 0, q>>>(a...);
-    else
+    } else {
         k_iisph_pacc<KIND, R, MIX, BATCH, MB><<<nb, bs, 0, q>>>(a...);
+    }
 }
 
 template <int KIND, int R, int MIX, bool BATCH, int MB, class... A>
-void launch_iisph_jacobi(unsigned nb, unsigned bs, cudaStream_t q, A... a)
+void launch_iisph_jacobi(unsigned nb, unsigned bs, cudaStream_t q, Tiles tl, bool persist,
+    A... a)
 {
-    if constexpr (!BATCH && occupancy_variant<KIND, MIX>)
+    if constexpr (BATCH) {
+        if (persist)
+            k_iisph_jacobi_tiles<KIND, R, MIX, MB><<<persistent_grid(
+                k_iisph_jacobi_tiles<KIND, R, MIX, MB>, bs, nb), bs, 0, q>>>(a..., tl);
+        else
+            k_iisph_jacobi<KIND, R, MIX, BATCH, MB><<<nb, bs, 0, q>>>(a...);
+    } else if constexpr (occupancy_variant<KIND, MIX>) {
         k_iisph_jacobi_occ<KIND, R, MIX, MB><<<nb, bs, 0, q>>>(a...);
-    else
+    } else {
         k_iisph_jacobi<KIND, R, MIX, BATCH, MB><<<nb, bs, 0, q>>>(a...);
+    }
 }
 
 #define REYN_NONPRESSURE_ARGS uint32_t n, Fluid f, const float4* __restrict__ vel, \
@@ -1550,6 +1669,11 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
     // batched scenes: per-scene sums of the current sweep, then the per-scene
     // convergence kernel; returns whether any scene iterates on
     SweepStats* scene_slot = reinterpret_cast<SweepStats*>(sv.scene_stats.get());
+    // a batch whose scenes no longer all iterate runs its sweeps as
+    // persistent launches over the active tiles (plain steps; a captured step
+    // keeps the full launches, whose threads of converged scenes return at
+    // once). While every scene iterates the full launches are faster.
+    bool persist = false;
     auto scenes_go_on = [&](int mode) {
         REYN_CUDA(cudaMemsetAsync(sv.n_active.get(), 0, sizeof(uint32_t), s));
         REYN_KERNEL("k_scene_converge", s,
@@ -1560,6 +1684,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         REYN_CUDA(cudaMemcpyAsync(sv.n_active_host->get(), sv.n_active.get(), sizeof(uint32_t),
             cudaMemcpyDeviceToHost, s));
         REYN_CUDA(cudaStreamSynchronize(s));
+        persist = *sv.n_active_host->get() < ns;
         return *sv.n_active_host->get() > 0;
     };
     // a captured step's sweep loop: a while node after the work captured so
@@ -1607,6 +1732,11 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             &gx->stats->iters, P.min_iter, max_it));
     };
 
+    // batched scenes: the pressure loop's sweeps run as persistent launches
+    // over the tiles of the scenes still iterating
+    Tiles tl {};
+    if (ns)
+        tl = Tiles { grid.sid.get(), sv.scene_active.get(), n, nb };
     const bool mixed = P.precision == REYN_PRECISION_MIXED;
     const bool rec16 = P.precision == REYN_PRECISION_MIXED_POS16;
     uint2* ACH = mixed ? sv.acch.get() : nullptr;
@@ -1645,16 +1775,32 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 (const uint2*)nullptr, nu10, eps, grav, dt, sv.acc.get(), sv.vel2.get(),
                 (uint2*)nullptr));
             float4* v = sv.vel2.get();
+            // one PCISPH iteration: prediction and pressure (a batch: over
+            // the tiles of the scenes still iterating)
+            auto sweep = [&](cudaStream_t q, SweepStats* slot) {
+                if (B && persist) {
+                    REYN_KERNEL("k_pcisph_predict", q,
+                        k_pcisph_predict_tiles<K, R, MB><<<persistent_grid(
+                        k_pcisph_predict_tiles<K, R, MB>, bs, nb), bs, 0, q>>>(n, f, v,
+                        sv.bterm.get(), dt, sv.rho.get(), kp, rho0, sv.p.get(), slot, tl));
+                    REYN_KERNEL("k_pcisph_pressure", q,
+                        k_pcisph_pressure_tiles<K, R, MB><<<persistent_grid(
+                        k_pcisph_pressure_tiles<K, R, MB>, bs, nb), bs, 0, q>>>(n, f, sv.rho.get(),
+                        sv.p.get(), sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v, tl));
+                } else {
+                    REYN_KERNEL("k_pcisph_predict", q,
+                        k_pcisph_predict<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, v, sv.bterm.get(),
+                        dt, sv.rho.get(), kp, rho0, sv.p.get(), slot));
+                    REYN_KERNEL("k_pcisph_pressure", q,
+                        k_pcisph_pressure<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, sv.rho.get(),
+                        sv.p.get(), sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
+                }
+            };
             if (gx) {
                 graph_loop([&](cudaStream_t q, cudaGraphConditionalHandle h) {
                     SweepStats* slot = ns ? scene_slot : slots;
                     REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), q));
-                    REYN_KERNEL("k_pcisph_predict", q,
-                        k_pcisph_predict<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, v, sv.bterm.get(), dt,
-                        sv.rho.get(), kp, rho0, sv.p.get(), slot));
-                    REYN_KERNEL("k_pcisph_pressure", q,
-                        k_pcisph_pressure<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, sv.rho.get(),
-                        sv.p.get(), sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
+                    sweep(q, slot);
                     if (ns)
                         scene_converge_dev(q, 0);
                     decide(q, h, slot);
@@ -1663,12 +1809,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             for (; !gx;) {
                 SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
-                REYN_KERNEL("k_pcisph_predict", s,
-                    k_pcisph_predict<K, R, B, MB><<<nb, bs, 0, s>>>(n, f, v, sv.bterm.get(), dt,
-                    sv.rho.get(), kp, rho0, sv.p.get(), slot));
-                REYN_KERNEL("k_pcisph_pressure", s,
-                    k_pcisph_pressure<K, R, B, MB><<<nb, bs, 0, s>>>(n, f, sv.rho.get(),
-                    sv.p.get(), sv.bterm.get(), kp, rho0, r0i, dt, sv.acc.get(), v));
+                sweep(s, slot);
                 iters += 1;
                 if (ns) {
                     const bool last = max_it && iters >= max_it;
@@ -1716,15 +1857,28 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             uint4* RX = REC1;
             uint4* RY = REC0;
             auto pacc = [&](cudaStream_t q, const uint32_t* gate) {
-                REYN_KERNEL("k_pacc_rec", q,
-                    k_pacc_rec<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, rc,
-                    (const float4*)sv.gq.get(), r0i, RX, RY, gate));
+                if (B && persist)
+                    REYN_KERNEL("k_pacc_rec", q,
+                        k_pacc_rec_tiles<K, R, MB><<<persistent_grid(
+                        k_pacc_rec_tiles<K, R, MB>, bs, nb), bs, 0, q>>>(n, f, rc,
+                        (const float4*)sv.gq.get(), r0i, RX, RY, gate, tl));
+                else
+                    REYN_KERNEL("k_pacc_rec", q,
+                        k_pacc_rec<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, rc,
+                        (const float4*)sv.gq.get(), r0i, RX, RY, gate));
             };
             auto jacobi = [&](cudaStream_t q, SweepStats* slot) {
-                REYN_KERNEL("k_jacobi_rec", q,
-                    k_jacobi_rec<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, rc,
-                    (const float4*)sv.gq.get(), (const float*)sv.sii.get(), sv.p.get(), dt,
-                    P.omega, tiny, thr, slot, RY, RX));
+                if (B && persist)
+                    REYN_KERNEL("k_jacobi_rec", q,
+                        k_jacobi_rec_tiles<K, R, MB><<<persistent_grid(
+                        k_jacobi_rec_tiles<K, R, MB>, bs, nb), bs, 0, q>>>(n, f, rc,
+                        (const float4*)sv.gq.get(), (const float*)sv.sii.get(), sv.p.get(), dt,
+                        P.omega, tiny, thr, slot, RY, RX, tl));
+                else
+                    REYN_KERNEL("k_jacobi_rec", q,
+                        k_jacobi_rec<K, R, B, MB><<<nb, bs, 0, q>>>(n, f, rc,
+                        (const float4*)sv.gq.get(), (const float*)sv.sii.get(), sv.p.get(), dt,
+                        P.omega, tiny, thr, slot, RY, RX));
             };
             if (P.warmstart) {
                 REYN_KERNEL("k_diag_pacc_rec", s,
@@ -1798,7 +1952,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             const float tiny = tiny_threshold();
             auto pacc = [&] {
                 REYN_KERNEL("k_iisph_pacc", s,
-                    launch_iisph_pacc<K, R, MIX, B, MB>(nb, bs, s, n, f, sv.p.get(),
+                    launch_iisph_pacc<K, R, MIX, B, MB>(nb, bs, s, tl, persist, n, f, sv.p.get(),
                     sv.bterm.get(), r0i, sv.acc.get(), ACH, (const uint32_t*)nullptr));
             };
             if (P.warmstart) {
@@ -1822,11 +1976,11 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 graph_loop([&](cudaStream_t q, cudaGraphConditionalHandle h) {
                     SweepStats* slot = ns ? scene_slot : slots;
                     REYN_KERNEL("k_iisph_pacc", q,
-                        launch_iisph_pacc<K, R, MIX, B, MB>(nb, bs, q, n, f, sv.p.get(),
+                        launch_iisph_pacc<K, R, MIX, B, MB>(nb, bs, q, tl, persist, n, f, sv.p.get(),
                         sv.bterm.get(), r0i, sv.acc.get(), ACH, (const uint32_t*)gx->gate));
                     REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), q));
                     REYN_KERNEL("k_iisph_jacobi", q,
-                        launch_iisph_jacobi<K, R, MIX, B, MB>(nb, bs, q, n, f,
+                        launch_iisph_jacobi<K, R, MIX, B, MB>(nb, bs, q, tl, persist, n, f,
                         (const float4*)sv.acc.get(), (const float4*)sv.bterm.get(),
                         (const float*)sv.aii.get(), (const float*)sv.sii.get(), sv.p.get(), dt,
                         P.omega, tiny, thr, slot));
@@ -1841,7 +1995,7 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
                 SweepStats* slot = ns ? scene_slot : slots + (iters % 64);
                 REYN_CUDA(cudaMemsetAsync(slot, 0, sizeof(SweepStats) * (ns ? ns : 1), s));
                 REYN_KERNEL("k_iisph_jacobi", s,
-                    launch_iisph_jacobi<K, R, MIX, B, MB>(nb, bs, s, n, f,
+                    launch_iisph_jacobi<K, R, MIX, B, MB>(nb, bs, s, tl, persist, n, f,
                     (const float4*)sv.acc.get(), (const float4*)sv.bterm.get(),
                     (const float*)sv.aii.get(), (const float*)sv.sii.get(), sv.p.get(), dt,
                     P.omega, tiny, thr, slot));

@@ -188,13 +188,14 @@ k_diag_rec(uint32_t n, Fluid f, RecConst rc,
 // a_i = -(p_i G_i + sum_j (m_j p_j) grad W_ij) / rho0^2, with p_i from the
 // particle's own X record; writes the Y record with m a. `gate`: a captured
 // step's loop body skips the first sweep's pass.
-template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
-k_pacc_rec(uint32_t n, Fluid f, RecConst rc,
-    const float4* __restrict__ gq, float r0i, const uint4* __restrict__ rec_in,
-    uint4* __restrict__ rec_out, const uint32_t* __restrict__ gate)
+#define REYN_PACC_REC_ARGS uint32_t n, Fluid f, RecConst rc, const float4* __restrict__ gq, \
+    float r0i, const uint4* __restrict__ rec_in, uint4* __restrict__ rec_out, \
+    const uint32_t* __restrict__ gate
+#define REYN_PACC_REC_PASS n, f, rc, gq, r0i, rec_in, rec_out, gate
+
+template <int KIND, int R, bool BATCH>
+__device__ __forceinline__ void pacc_rec(uint32_t i, REYN_PACC_REC_ARGS)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || (gate && !*gate))
         return;
     if constexpr (BATCH) {
@@ -218,18 +219,31 @@ k_pacc_rec(uint32_t n, Fluid f, RecConst rc,
         ma * fmaf(pi, gt.z, m0 * sz));
 }
 
+template <int KIND, int R, bool BATCH, int MB>
+__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+k_pacc_rec(REYN_PACC_REC_ARGS)
+{
+    pacc_rec<KIND, R, BATCH>(blockIdx.x * blockDim.x + threadIdx.x, REYN_PACC_REC_PASS);
+}
+
+template <int KIND, int R, int MB>
+__global__ void __launch_bounds__(MB) k_pacc_rec_tiles(REYN_PACC_REC_ARGS, Tiles tl)
+{
+    REYN_TILE_LOOP(tl, (pacc_rec<KIND, R, true>(i, REYN_PACC_REC_PASS)));
+}
+
 // _jacobi_update_pressures (IISPH.cu:108-162) over Y records:
 // Ap = dt (a_i.G_i - sum_j (m_j a_j).grad W_ij) with a_i from the particle's
 // own Y record; p += max(0, omega (s - Ap) / a_ii); writes p and the X record;
 // the convergence sums as the FP32 sweep's.
-template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
-k_jacobi_rec(uint32_t n, Fluid f, RecConst rc,
-    const float4* __restrict__ gq, const float* __restrict__ sii, float* __restrict__ p,
-    float dt, float omega, float tiny, float thr, SweepStats* stats,
-    const uint4* __restrict__ rec_in, uint4* __restrict__ rec_out)
+#define REYN_JACOBI_REC_ARGS uint32_t n, Fluid f, RecConst rc, const float4* __restrict__ gq, \
+    const float* __restrict__ sii, float* __restrict__ p, float dt, float omega, float tiny, \
+    float thr, SweepStats* stats, const uint4* __restrict__ rec_in, uint4* __restrict__ rec_out
+#define REYN_JACOBI_REC_PASS n, f, rc, gq, sii, p, dt, omega, tiny, thr, stats, rec_in, rec_out
+
+template <int KIND, int R, bool BATCH>
+__device__ __forceinline__ void jacobi_rec(uint32_t i, REYN_JACOBI_REC_ARGS)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned over = 0;
     double epos = 0.0;
     float emax = 0.f;
@@ -269,6 +283,19 @@ k_jacobi_rec(uint32_t n, Fluid f, RecConst rc,
         scene_accumulate(stats, sc, live, over, epos, 0.0, emax);
     else
         block_accumulate(stats, over, epos, 0.0, emax);
+}
+
+template <int KIND, int R, bool BATCH, int MB>
+__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+k_jacobi_rec(REYN_JACOBI_REC_ARGS)
+{
+    jacobi_rec<KIND, R, BATCH>(blockIdx.x * blockDim.x + threadIdx.x, REYN_JACOBI_REC_PASS);
+}
+
+template <int KIND, int R, int MB>
+__global__ void __launch_bounds__(MB) k_jacobi_rec_tiles(REYN_JACOBI_REC_ARGS, Tiles tl)
+{
+    REYN_TILE_LOOP(tl, (jacobi_rec<KIND, R, true>(i, REYN_JACOBI_REC_PASS)));
 }
 
 // the last _set_pressure_accelerations + integrate (IISPH.cu:248-257) over X
