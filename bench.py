@@ -432,10 +432,13 @@ def developed_leg(a, world, rank, dev, stream, names, config):
         ratio, block, _, every = config[name]
         r = EngineRun(rank, a.scale, dev, name, a.order, ratio, block, every)
         r.restore(ck)
-        _, _, ms_max, _, clk, log = timed_steps(r, a, world, stream, dev)
+        _, _, ms_max, prof, clk, log = timed_steps(r, a, world, stream, dev)
         leg = leg_summary(r, a, world, ms_max, log)
         leg["dt_per_step"] = [float(f"{x[2]:.4e}") for x in log]
         leg["clocks"] = clk
+        leg["kernels_ms_per_step"] = {
+            k: round(v[1] / a.steps, 3)
+            for k, v in sorted(prof.items(), key=lambda kv: -kv[1][1])[:8]}
         out[name] = leg
         r.close()
     mixed = [k for k in ("mixed", "mixed_pos16") if k in out]
