@@ -155,7 +155,8 @@ __device__ __forceinline__ uint2 record_position(const GridView& g, int3 c, floa
 //      w3 = m p_old (FP32)
 //   Y (pressure accelerations -> Jacobi): w1 hi m/m_0, w2, w3 lo =
 //      m a ACC_SCALE / m_0 (3 x FP16)
-//   X (Jacobi -> pressure accelerations): w1 hi m/m_0, w2 = p (FP32)
+//   X (Jacobi -> pressure accelerations): w1 hi m/m_0, w2 = p (FP32),
+//      w3 = (m/m_0) p (FP32)
 __device__ __forceinline__ uint32_t half_bits(float a)
 {
     return __half_as_ushort(__float2half_rn(a));
@@ -207,10 +208,14 @@ __device__ __forceinline__ float3 rec_y_vec(const uint4& r)
 
 __device__ __forceinline__ uint4 rec_x(uint32_t w0, uint32_t w1, float p)
 {
-    return make_uint4(w0, w1, __float_as_uint(p), 0u);
+    return make_uint4(w0, w1, __float_as_uint(p), __float_as_uint(upper_half(w1) * p));
 }
 
 __device__ __forceinline__ float rec_x_p(const uint4& r) { return __uint_as_float(r.z); }
+
+// (m/m_0) p of an X record: the product a neighbour's pressure enters the
+// pressure accelerations with, rounded as the reader would round it
+__device__ __forceinline__ float rec_x_mp(const uint4& r) { return __uint_as_float(r.w); }
 
 // the mass ratio m/m_0 of a NP, Y or X record
 __device__ __forceinline__ float rec_m16(const uint4& r) { return upper_half(r.y); }
@@ -859,9 +864,13 @@ unsigned persistent_grid(Kern kern, unsigned bs, unsigned tiles)
 // neighbour list, written entry by entry (a block's rows form one 32 KB
 // region, so the L2 merges the scattered 4-byte stores into full lines).
 // MIXED: the particle's FP16 velocity/density record is written for later
-// passes; MIXED_POS16: its 16-byte record for the non-pressure pass.
+// passes; MIXED_POS16: its 16-byte record for the non-pressure pass. The
+// one-scene MIXED_POS16 form is held to 40 registers (12 blocks of 128 per
+// SM, 16 bytes spilled) like the other modes' forms: on the 4M dam break
+// 753 us per launch against 771 us at the compiler's 47 registers.
 template <int KIND, int R, int MIX = 0, bool BATCH = false, int MB = NBR_THREADS>
-__global__ void __launch_bounds__(MB) k_density(uint32_t n, Fluid f, Bdy b,
+__global__ void __launch_bounds__(MB, ((MIX == MIX_POS16 && !BATCH) ? 65536 / 40 / MB : 0))
+k_density(uint32_t n, Fluid f, Bdy b,
     float* __restrict__ rho, float4* __restrict__ vel, float4* __restrict__ bterm,
     uint4* __restrict__ rec_out, uint2* __restrict__ velh_out)
 {

@@ -53,7 +53,11 @@ __device__ __forceinline__ float rec_m0(const Fluid& f)
 // G = sum_j m_j grad W_ij + g_b and gsq = sum_j m_j |grad W_ij|^2, and the DG
 // record with m v* and m p_old for the diagonal pass. In record units the
 // viscosity term (10 nu m_j v_ij.x_ij g / (rho_j (|x_ij|^2 + eps))) x_ij
-// becomes (10 nu m_j v_ij.d g' / (rho_j (unit |d|^2 + eps / unit))) d.
+// becomes (10 nu m_j v_ij.d g' / (rho_j (unit |d|^2 + eps / unit))) d. The
+// quotient is the fast division (2 ulp; its divisor stays far inside
+// [2^-126, 2^126] here: rho_j times a distance term between eps / unit and
+// 4 cells^2 / unit) where FP32 uses the IEEE one, since rho_j and v_j come
+// from FP16 already.
 template <int KIND, int R, bool BATCH, int MB>
 __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
 k_np_rec(uint32_t n, Fluid f, RecConst rc,
@@ -78,7 +82,7 @@ k_np_rec(uint32_t n, Fluid f, RecConst rc,
             const float mj = m0 * rec_m16(rj);
             const float vdx =
                 fmaf(vi.x - vxy.x, d.x, fmaf(vi.y - vxy.y, d.y, (vi.z - vzr.x) * d.z));
-            const float s = (nu10 * mj * vdx * g) / (vzr.y * fmaf(rc.unit, l2, eps_u));
+            const float s = __fdividef(nu10 * mj * vdx * g, vzr.y * fmaf(rc.unit, l2, eps_u));
             ax += s * d.x;
             ay += s * d.y;
             az += s * d.z;
@@ -209,7 +213,7 @@ __device__ __forceinline__ void pacc_rec(uint32_t i, REYN_PACC_REC_ARGS)
     float sx = 0.f, sy = 0.f, sz = 0.f;
     for_each_rec<KIND, R, BATCH>(f, rc.kc, rec_in, i, ri,
         [&](uint32_t, const uint4& rj, float3 d, float g) {
-        const float sp = g * (rec_m16(rj) * rec_x_p(rj));
+        const float sp = g * rec_x_mp(rj);
         sx += sp * d.x;
         sy += sp * d.y;
         sz += sp * d.z;
@@ -320,7 +324,7 @@ k_final_rec(uint32_t n, Fluid f, RecConst rc,
         float sx = 0.f, sy = 0.f, sz = 0.f;
         for_each_rec<KIND, R, BATCH>(f, rc.kc, rec_in, i, ri,
             [&](uint32_t, const uint4& rj, float3 d, float g) {
-                const float sp = g * (rec_m16(rj) * rec_x_p(rj));
+                const float sp = g * rec_x_mp(rj);
                 sx += sp * d.x;
                 sy += sp * d.y;
                 sz += sp * d.z;
