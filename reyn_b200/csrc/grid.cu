@@ -160,8 +160,9 @@ __global__ void k_canonical(uint32_t n, const uint32_t* __restrict__ slots,
 // slots (atomicSub, which also returns its counter to zero) into `slots`,
 // and its particles are listed in `split` (count in *nsplit) for
 // k_rank_split. In a state reordered by the previous step's grid nearly
-// every cell is whole.
-__global__ void k_scatter_stable(uint32_t n, const uint32_t* __restrict__ keys,
+// every cell is whole. Blocks of THREADS threads.
+__global__ void __launch_bounds__(THREADS) k_scatter_stable(uint32_t n,
+    const uint32_t* __restrict__ keys,
     const uint32_t* __restrict__ prefix, uint32_t* __restrict__ counts,
     uint32_t* __restrict__ slots, uint32_t* __restrict__ sorted, uint32_t* __restrict__ split,
     uint32_t* __restrict__ nsplit)
@@ -194,16 +195,31 @@ __global__ void k_scatter_stable(uint32_t n, const uint32_t* __restrict__ keys,
         else
             slots[st + top - g + rank] = i;
     }
+    // the split list: one atomic per block that has split cells (after a
+    // developed flow's step a few percent of the particles land in cells
+    // whose other particles sit in another warp; an atomic per warp then
+    // serialises on the one counter)
+    if (!__syncthreads_or(valid && !whole))
+        return; // the block holds no particle of a split cell
     const unsigned sm = __ballot_sync(0xffffffffu, valid && !whole);
-    if (sm) {
-        const int first = __ffs(sm) - 1;
-        uint32_t base = 0;
-        if (lane == first)
-            base = atomicAdd(nsplit, uint32_t(__popc(sm)));
-        base = __shfl_sync(0xffffffffu, base, first);
-        if (valid && !whole)
-            split[base + __popc(sm & ((1u << lane) - 1u))] = i;
+    __shared__ uint32_t warp_base[THREADS / 32];
+    __shared__ uint32_t block_base;
+    const int w = threadIdx.x >> 5;
+    if (lane == 0)
+        warp_base[w] = __popc(sm);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int k = 0; k < int(blockDim.x >> 5); ++k) {
+            const uint32_t c = warp_base[k];
+            warp_base[k] = tot;
+            tot += c;
+        }
+        block_base = atomicAdd(nsplit, tot);
     }
+    __syncthreads();
+    if (valid && !whole)
+        split[block_base + warp_base[w] + __popc(sm & ((1u << lane) - 1u))] = i;
 }
 
 // the canonical place of each particle of a split cell: its cell's start plus
@@ -227,9 +243,8 @@ __global__ void k_rank_split(const uint32_t* __restrict__ nsplit,
 }
 
 // ---- exclusive scan over all cells ----------------------------------------
-// Three passes over tiles of SCAN_TILE counts: tile sums, a single-block scan
-// of the tile sums, and the tile scans with their offsets. The last entry
-// prefix[C] receives the total.
+// Two passes over tiles of SCAN_TILE counts: the tile sums, then the tile
+// scans with their offsets. The last entry prefix[C] receives the total.
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_PER_THREAD = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_PER_THREAD;
@@ -310,29 +325,16 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(
         part[blockIdx.x] = total;
 }
 
-// exclusive scan of the tile sums in place, one block; part[nparts] = total
-__global__ void __launch_bounds__(SCAN_THREADS) k_scan_parts(uint32_t* part, uint32_t nparts)
-{
-    const uint32_t per = (nparts + SCAN_THREADS - 1) / SCAN_THREADS;
-    const uint32_t b = threadIdx.x * per;
-    uint32_t s = 0;
-    for (uint32_t k = 0; k < per && b + k < nparts; ++k)
-        s += part[b + k];
-    __shared__ uint32_t total;
-    uint32_t run = block_exclusive_scan(s, &total);
-    for (uint32_t k = 0; k < per && b + k < nparts; ++k) {
-        const uint32_t t = part[b + k];
-        part[b + k] = run;
-        run += t;
-    }
-    if (threadIdx.x == 0)
-        part[nparts] = total;
-}
-
+// the tiles' exclusive scans: each tile's offset is the sum of the tile sums
+// before it, which the tile's block adds up itself (at most a few thousand
+// values, from the L2); the last tile writes the total to out[C]
 __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(
     const uint32_t* __restrict__ in, int64_t C, const uint32_t* __restrict__ part,
-    uint32_t nparts, uint32_t* __restrict__ out)
+    uint32_t* __restrict__ out)
 {
+    uint32_t pre = 0;
+    for (uint32_t t = threadIdx.x; t < blockIdx.x; t += SCAN_THREADS)
+        pre += part[t];
     const int64_t base = int64_t(blockIdx.x) * SCAN_TILE + int64_t(threadIdx.x) * SCAN_PER_THREAD;
     uint32_t v[SCAN_PER_THREAD];
     load_tile_chunk(in, C, base, v);
@@ -340,8 +342,9 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(
 #pragma unroll
     for (int k = 0; k < SCAN_PER_THREAD; ++k)
         s += v[k];
-    __shared__ uint32_t total;
-    uint32_t run = block_exclusive_scan(s, &total) + part[blockIdx.x];
+    __shared__ uint32_t offset, total;
+    block_exclusive_scan(pre, &offset);
+    uint32_t run = block_exclusive_scan(s, &total) + offset;
 #pragma unroll
     for (int k = 0; k < SCAN_PER_THREAD; ++k) {
         const uint32_t t = v[k];
@@ -359,8 +362,8 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_scan_apply(
             if (base + k < C)
                 out[base + k] = v[k];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        out[C] = part[nparts];
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0)
+        out[C] = offset + total;
 }
 
 void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& part,
@@ -370,10 +373,8 @@ void exclusive_scan(const uint32_t* in, int64_t C, DevArray<uint32_t>& part,
     part.resize(size_t(nparts) + 1);
     REYN_KERNEL("k_scan_tiles", s,
         k_scan_tiles<<<nparts, SCAN_THREADS, 0, s>>>(in, C, part.get(), fold_status));
-    REYN_KERNEL("k_scan_parts", s,
-        k_scan_parts<<<1, SCAN_THREADS, 0, s>>>(part.get(), nparts));
     REYN_KERNEL("k_scan_apply", s,
-        k_scan_apply<<<nparts, SCAN_THREADS, 0, s>>>(in, C, part.get(), nparts, out));
+        k_scan_apply<<<nparts, SCAN_THREADS, 0, s>>>(in, C, part.get(), out));
 }
 
 void Grid::drop_prekey(cudaStream_t s)

@@ -45,9 +45,8 @@ __global__ void k_canonical(uint32_t n, const uint32_t* __restrict__ slots,
 __global__ void __launch_bounds__(256) k_scan_tiles(
     const uint32_t* __restrict__ in, int64_t C, uint32_t* __restrict__ part,
     uint32_t* __restrict__ fold_status);
-__global__ void __launch_bounds__(256) k_scan_parts(uint32_t* part, uint32_t nparts);
 __global__ void __launch_bounds__(256) k_scan_apply(const uint32_t* __restrict__ in, int64_t C,
-    const uint32_t* __restrict__ part, uint32_t nparts, uint32_t* __restrict__ out);
+    const uint32_t* __restrict__ part, uint32_t* __restrict__ out);
 
 namespace {
 
@@ -138,9 +137,8 @@ extern "C" int reyn_grid_construct_noalloc(const float bound_min[3], const float
         }
         REYN_KERNEL("k_scan_tiles", s,
             k_scan_tiles<<<nparts, 256, 0, s>>>(counts, C, parts, nullptr));
-        REYN_KERNEL("k_scan_parts", s, k_scan_parts<<<1, 256, 0, s>>>(parts, nparts));
         REYN_KERNEL("k_scan_apply", s,
-            k_scan_apply<<<nparts, 256, 0, s>>>(counts, C, parts, nparts, prefix));
+            k_scan_apply<<<nparts, 256, 0, s>>>(counts, C, parts, prefix));
         if (n) {
             REYN_KERNEL("k_scatter", s,
                 k_scatter<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, keys, prefix, counts,
