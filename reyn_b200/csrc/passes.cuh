@@ -705,6 +705,13 @@ __global__ void k_graph_single_pass(GraphStats* gs, uint32_t* __restrict__ scene
         scene_iters[s] = 1;
 }
 
+// three SoA float arrays (an acceleration's components)
+struct Soa3 {
+    float* __restrict__ x;
+    float* __restrict__ y;
+    float* __restrict__ z;
+};
+
 // ---- step tail ---------------------------------------------------------------
 // The reference's main loop follows every step with hard_enforce_bounds
 // (scene.cu:466-483) and starts the next with simple_dt_controller, whose CFL
@@ -1469,11 +1476,12 @@ void launch_nonpressure(unsigned nb, unsigned bs, cudaStream_t q, A... a)
         k_nonpressure<KIND, R, MIX, BATCH, MB><<<nb, bs, 0, q>>>(a...);
 }
 
-// final _set_pressure_accelerations + integrate (IISPH.cu:248-257)
+// final _set_pressure_accelerations + integrate (IISPH.cu:248-257); the
+// accelerations go straight to the solver's SoA arrays
 template <int KIND, int R, int MIX = 0, bool BATCH = false, int MB = NBR_THREADS>
 __global__ void __launch_bounds__(MB) k_iisph_final(uint32_t n, Fluid f,
     const float* __restrict__ p, const float4* __restrict__ bterm, float r0i,
-    const float4* __restrict__ vel, float dt, float4* __restrict__ acc,
+    const float4* __restrict__ vel, float dt, Soa3 acc,
     float* __restrict__ x, float* __restrict__ y, float* __restrict__ z,
     float* __restrict__ vx, float* __restrict__ vy, float* __restrict__ vz, Tail tail)
 {
@@ -1494,7 +1502,9 @@ __global__ void __launch_bounds__(MB) k_iisph_final(uint32_t n, Fluid f,
     ax = -r0i * (ax + pi * bt.x);
     ay = -r0i * (ay + pi * bt.y);
     az = -r0i * (az + pi * bt.z);
-    acc[i] = make_float4(ax, ay, az, 0.f);
+    acc.x[i] = ax;
+    acc.y[i] = ay;
+    acc.z[i] = az;
     const float4 v = vel[i];
     const float nvx = v.x + dt * ax, nvy = v.y + dt * ay, nvz = v.z + dt * az;
     vn = store_state<BATCH>(tail, i, me.x + dt * nvx, me.y + dt * nvy, me.z + dt * nvz, nvx, nvy, nvz,
@@ -1503,6 +1513,7 @@ __global__ void __launch_bounds__(MB) k_iisph_final(uint32_t n, Fluid f,
     tail_reduce(tail, vn);
 }
 
+// SESPH and PCISPH: the packed accelerations to the solver's SoA arrays
 __global__ void k_unpack_acc(uint32_t n, const float4* __restrict__ acc, float* __restrict__ ax,
     float* __restrict__ ay, float* __restrict__ az)
 {
@@ -1952,8 +1963,8 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             }
             REYN_KERNEL("k_final_rec", s,
                 k_final_rec<K, R, B, MB><<<nb, bs, 0, s>>>(n, f, rc,
-                (const float4*)sv.gq.get(), r0i, sv.vel2.get(), dt, sv.acc.get(), RX, X, Y, Z,
-                VX, VY, VZ, tail));
+                (const float4*)sv.gq.get(), r0i, sv.vel2.get(), dt,
+                Soa3 { sv.ax.get(), sv.ay.get(), sv.az.get() }, RX, X, Y, Z, VX, VY, VZ, tail));
         } else { // IISPH
             REYN_KERNEL("k_nonpressure", s,
                 launch_nonpressure<K, R, MIX, B, MB>(nb, bs, s, n, f, (const float4*)st.vel.get(),
@@ -2040,7 +2051,8 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
             }
             REYN_KERNEL("k_iisph_final", s,
                 k_iisph_final<K, R, MIX, B, MB><<<nb, bs, 0, s>>>(n, f, sv.p.get(), sv.bterm.get(),
-                r0i, sv.vel2.get(), dt, sv.acc.get(), X, Y, Z, VX, VY, VZ, tail));
+                r0i, sv.vel2.get(), dt, Soa3 { sv.ax.get(), sv.ay.get(), sv.az.get() }, X, Y, Z,
+                VX, VY, VZ, tail));
         }
     };
     dispatch(P.kernel, grid.geom.range, [&](auto KC, auto RC) {
@@ -2060,9 +2072,11 @@ void solver_step_t(reyn_solver& sv, reyn_particles& st, const Grid& grid,
         else
             body(KC, RC, std::integral_constant<int, 0> {}, std::false_type {});
     });
-    REYN_KERNEL("k_unpack_acc", s,
-        k_unpack_acc<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, sv.acc.get(), sv.ax.get(),
-        sv.ay.get(), sv.az.get()));
+    if (sv.scheme != REYN_IISPH) {
+        REYN_KERNEL("k_unpack_acc", s,
+            k_unpack_acc<<<blocks_for(n, THREADS), THREADS, 0, s>>>(n, sv.acc.get(), sv.ax.get(),
+            sv.ay.get(), sv.az.get()));
+    }
     st.packed_valid = false; // positions moved: the packed copy is stale
     st.version += 1;
     if (prekeyed) {

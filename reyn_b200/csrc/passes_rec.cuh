@@ -303,13 +303,13 @@ __global__ void __launch_bounds__(MB) k_jacobi_rec_tiles(REYN_JACOBI_REC_ARGS, T
 }
 
 // the last _set_pressure_accelerations + integrate (IISPH.cu:248-257) over X
-// records; writes a and the SoA state (bounds and the max |v| reduction of a
-// bounded step included)
+// records; writes a (SoA) and the SoA state (bounds and the max |v|
+// reduction of a bounded step included)
 template <int KIND, int R, bool BATCH, int MB>
 __global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
 k_final_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ gq, float r0i, const float4* __restrict__ vel, float dt,
-    float4* __restrict__ acc, const uint4* __restrict__ rec_in, float* __restrict__ x,
+    Soa3 acc, const uint4* __restrict__ rec_in, float* __restrict__ x,
     float* __restrict__ y, float* __restrict__ z, float* __restrict__ vx,
     float* __restrict__ vy, float* __restrict__ vz, Tail tail)
 {
@@ -331,7 +331,9 @@ k_final_rec(uint32_t n, Fluid f, RecConst rc,
             });
             const float ax = -r0i * fmaf(pi, gt.x, m0 * sx), ay = -r0i * fmaf(pi, gt.y, m0 * sy),
                     az = -r0i * fmaf(pi, gt.z, m0 * sz);
-        acc[i] = make_float4(ax, ay, az, 0.f);
+        acc.x[i] = ax;
+        acc.y[i] = ay;
+        acc.z[i] = az;
         const float4 v = vel[i];
         const float nvx = v.x + dt * ax, nvy = v.y + dt * ay, nvz = v.z + dt * az;
         vn = store_state<BATCH>(tail, i, me.x + dt * nvx, me.y + dt * nvy, me.z + dt * nvz,
