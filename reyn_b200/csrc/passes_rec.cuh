@@ -35,6 +35,8 @@
 // compiler's own choice (71 registers, 237 us per Jacobi sweep) and caps of
 // 48 (214 us) and 40 (217 us, with spills): 209 us.
 template <int MB> constexpr int rec_min_blocks = 65536 / 56 / MB;
+// the batched forms (scene lookups, per-scene sums) are held to 64 registers,
+// 8 blocks of 128 per SM, against the 71 to 92 the compiler takes unbounded
 
 // per-step constants of the record passes
 struct RecConst {
@@ -59,7 +61,7 @@ __device__ __forceinline__ float rec_m0(const Fluid& f)
 // 4 cells^2 / unit) where FP32 uses the IEEE one, since rho_j and v_j come
 // from FP16 already.
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+__global__ void __launch_bounds__(MB, (BATCH ? 65536 / 64 / MB : rec_min_blocks<MB>))
 k_np_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ vel, const float4* __restrict__ bterm,
     const float* __restrict__ p_old, float nu10, float eps, float3 grav, float dt,
@@ -111,7 +113,7 @@ k_np_rec(uint32_t n, Fluid f, RecConst rc,
 // the warm-started p' = p_old / 2. Writes a_ii (also into gq.w), s_i, p'
 // (p_new) and the Y record.
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+__global__ void __launch_bounds__(MB, (BATCH ? 65536 / 64 / MB : rec_min_blocks<MB>))
 k_diag_pacc_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ vel, float4* __restrict__ gq, float rho0, float dt, float r0i,
     const float* __restrict__ p_old, float* __restrict__ aii, float* __restrict__ sii,
@@ -156,7 +158,7 @@ k_diag_pacc_rec(uint32_t n, Fluid f, RecConst rc,
 // from the Jacobi update of zero; writes the X record for the pressure
 // accelerations that follow
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+__global__ void __launch_bounds__(MB, (BATCH ? 65536 / 64 / MB : rec_min_blocks<MB>))
 k_diag_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ vel, float4* __restrict__ gq, float rho0, float dt,
     float omega, float tiny, float* __restrict__ aii, float* __restrict__ sii,
@@ -224,7 +226,7 @@ __device__ __forceinline__ void pacc_rec(uint32_t i, REYN_PACC_REC_ARGS)
 }
 
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+__global__ void __launch_bounds__(MB, (BATCH ? 65536 / 64 / MB : rec_min_blocks<MB>))
 k_pacc_rec(REYN_PACC_REC_ARGS)
 {
     pacc_rec<KIND, R, BATCH>(blockIdx.x * blockDim.x + threadIdx.x, REYN_PACC_REC_PASS);
@@ -290,7 +292,7 @@ __device__ __forceinline__ void jacobi_rec(uint32_t i, REYN_JACOBI_REC_ARGS)
 }
 
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+__global__ void __launch_bounds__(MB, (BATCH ? 65536 / 64 / MB : rec_min_blocks<MB>))
 k_jacobi_rec(REYN_JACOBI_REC_ARGS)
 {
     jacobi_rec<KIND, R, BATCH>(blockIdx.x * blockDim.x + threadIdx.x, REYN_JACOBI_REC_PASS);
@@ -306,7 +308,7 @@ __global__ void __launch_bounds__(MB) k_jacobi_rec_tiles(REYN_JACOBI_REC_ARGS, T
 // records; writes a (SoA) and the SoA state (bounds and the max |v|
 // reduction of a bounded step included)
 template <int KIND, int R, bool BATCH, int MB>
-__global__ void __launch_bounds__(MB, (BATCH ? 1 : rec_min_blocks<MB>))
+__global__ void __launch_bounds__(MB, (BATCH ? 65536 / 64 / MB : rec_min_blocks<MB>))
 k_final_rec(uint32_t n, Fluid f, RecConst rc,
     const float4* __restrict__ gq, float r0i, const float4* __restrict__ vel, float dt,
     Soa3 acc, const uint4* __restrict__ rec_in, float* __restrict__ x,
