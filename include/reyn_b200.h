@@ -78,8 +78,14 @@ typedef struct reyn_soa {
 /* Particles(N, rho0) (particles.cu:22): allocates 7 zeroed device arrays */
 int reyn_particles_create(uint32_t n, float rho0, reyn_particles** out);
 int reyn_particles_destroy(reyn_particles* p);
-/* pointers for direct device access; marks the engine's packed copy stale */
+/* pointers for direct device access. The call counts as a change of the
+ * state: what the engine derived from it (its packed copy, the next grid
+ * build's keys pre-computed by the last step, that step's max |v|) is
+ * recomputed. Fetch the pointers again after every reorder and before
+ * writing through them. */
 int reyn_particles_soa(reyn_particles* p, reyn_soa* out);
+/* the particle count (no change to the state) */
+int reyn_particles_count(const reyn_particles* p, uint32_t* n);
 /* host <-> device copies of the 7 arrays (any host pointer may be NULL) */
 int reyn_particles_upload(reyn_particles* p, const float* xx, const float* xy,
     const float* xz, const float* vx, const float* vy, const float* vz,
@@ -419,7 +425,8 @@ int reyn_dt_controller(reyn_particles* state, uint32_t iter_last,
 /* simple_dt_controller with the max |v| that the solver's last
  * reyn_solver_step_bounded reduced, when `state` has not changed through
  * this library since (otherwise a reduction pass, as reyn_dt_controller).
- * Writes to the state through raw device pointers are not seen: after such
+ * Fetching the state's pointers (reyn_particles_soa) counts as a change;
+ * writes through pointers fetched before the step are not seen: after such
  * writes use reyn_dt_controller. Waits for that step's last kernel. */
 int reyn_solver_next_dt(reyn_solver* s, reyn_particles* state,
     uint32_t iter_last, float dt_last, float lambda, float h, const float g[3],

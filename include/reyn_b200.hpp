@@ -115,9 +115,9 @@ public:
 private:
     uint32_t n() const
     {
-        reyn_soa s {};
-        reyn_particles_soa(h_, &s);
-        return s.n;
+        uint32_t c = 0;
+        reyn_particles_count(h_, &c);
+        return c;
     }
     reyn_particles* h_ = nullptr;
 };

@@ -101,6 +101,7 @@ _SIGNATURES = {
     "reyn_particles_create": [_u32, _f, ctypes.POINTER(_vp)],
     "reyn_particles_destroy": [_vp],
     "reyn_particles_soa": [_vp, ctypes.POINTER(Soa)],
+    "reyn_particles_count": [_vp, ctypes.POINTER(_u32)],
     "reyn_particles_reorder": [_vp, _vp, _vp],
     "reyn_particles_resize": [_vp, _u32, ctypes.c_int, _vp],
     "reyn_boundary_bounds": [_vp, _vp, _vp],

@@ -105,7 +105,20 @@ int reyn_particles_soa(reyn_particles* p, reyn_soa* out)
         out->m = p->cur[FM].get();
         out->n = p->n;
         out->rho0 = p->rho0;
+        // the caller may write through these pointers: what was derived from
+        // the current state (the packed copy, the next build's keys and
+        // histogram pre-computed by the last step, that step's max |v|) is
+        // no longer trusted
         p->packed_valid = false;
+        p->version += 1;
+    });
+}
+
+int reyn_particles_count(const reyn_particles* p, uint32_t* n)
+{
+    return guard([&] {
+        require(p && n, "null argument");
+        *n = p->n;
     });
 }
 

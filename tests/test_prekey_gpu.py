@@ -81,6 +81,39 @@ def test_prekey_dropped_when_state_changes(cuda):
         o.close()
 
 
+def test_prekey_dropped_after_writes_through_raw_pointers(cuda):
+    """A caller that takes the state's device pointers (Particles'
+    DeviceBuffer::ptr()) and moves the particles with its own kernel between
+    a pre-keyed step and the next build must get the build of the new
+    positions."""
+    import torch
+
+    import reyn_b200 as rb
+    sc = scenes.dam_break((14, 12, 10), 0.02, (0.5, 0.5, 0.5), velocity_noise=0.3, seed=34)
+    st, bd, grid, sv = _setup(rb, sc)
+    grid.construct_and_reorder(st)
+    sv.step(st, grid, bd, 1e-3, bounds=(sc.box_min, sc.box_max))
+    moved = st.download()
+    moved["x"] = np.asarray(moved["x"], np.float32)[::-1].copy()
+    v = st.soa()
+
+    class _Dev:  # a device array at a raw pointer
+        def __init__(self, ptr, n):
+            self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4",
+                                             "data": (int(ptr), False), "version": 3}
+
+    xs = torch.as_tensor(_Dev(v.xx, sc.n), device="cuda")
+    xs.copy_(torch.tensor(moved["x"], device="cuda"))
+    torch.cuda.synchronize()
+    grid.construct_and_reorder(st)
+    want_prefix, want_sorted = _fresh_build(rb, sc, moved)
+    prefix, srt = _grid_arrays(rb, grid, sc.n)
+    np.testing.assert_array_equal(prefix, want_prefix)
+    np.testing.assert_array_equal(srt, want_sorted)
+    for o in (sv, grid, bd, st):
+        o.close()
+
+
 def test_prekey_reports_positions_outside_the_grid(cuda):
     import reyn_b200 as rb
     sc = scenes.dam_break((10, 8, 8), 0.02, (0.5, 0.5, 0.5), seed=33)
