@@ -172,23 +172,6 @@ __device__ __forceinline__ float pair_g(const KernelConst& k, float l2)
     }
 }
 
-// pair_g for a factor that only ever multiplies the pair vector itself (or
-// |x|^2): for Wendland C2 at x = 0 the unguarded form returns 0 instead of
-// the finite g(0) (rsqrt(0) = inf, len = NaN, the clamp fmaxf(0, 1 - NaN) =
-// 0, and dw(q)/q = -20 t^3 has no other factor of q), which leaves g x and
-// g^2 |x|^2 unchanged, so the guard is dropped there; the other kernels keep
-// pair_g (W6's dw(q)/q carries a polynomial in q that NaN would reach)
-template <int KIND>
-__device__ __forceinline__ float pair_g_vec(const KernelConst& k, float l2)
-{
-    if constexpr (KIND == K_C2) {
-        const float len = l2 * rsqrtf(l2);
-        return (k.dw_scale * k.h_inv) * Shape<KIND>::dw_over_q(len * k.h_inv);
-    } else {
-        return pair_g<KIND>(k, l2);
-    }
-}
-
 template <int KIND>
 __device__ __forceinline__ void pair_wg(
     const KernelConst& k, float l2, float& w, float& g)

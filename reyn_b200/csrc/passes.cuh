@@ -419,10 +419,36 @@ __device__ __forceinline__ void for_each_listed(const Fluid& f, uint32_t i, cons
     }
 }
 
+// The kernel-gradient factor of a record pair up to a factor that is the
+// same for every pair of a pass: for Wendland C2 the cube of (1 - q), the
+// constant dw(q)/q / (1 - q)^3 = -20 times dw_scale h_inv being applied once
+// to each particle's sums (rec_gscale); for the other kernels pair_g itself.
+// At l2 = 0 (a coincident pair, whose d is 0) the C2 factor is 0.
+template <int KIND>
+__device__ __forceinline__ float rec_g(const KernelConst& k, float l2)
+{
+    if constexpr (KIND == K_C2) {
+        const float t = fmaxf(0.f, fmaf(-k.h_inv, l2 * rsqrtf(l2), 1.f));
+        return t * t * t;
+    } else {
+        return pair_g<KIND>(k, l2);
+    }
+}
+
+template <int KIND>
+__device__ __forceinline__ float rec_gscale(const KernelConst& k)
+{
+    if constexpr (KIND == K_C2)
+        return (k.dw_scale * k.h_inv) * Shape<KIND>::dw_over_q(0.f);
+    else
+        return 1.f;
+}
+
 // MIXED_POS16: the fluid neighbours j != i of particle i with their 16-byte
 // records: fn(j, rec_j, d, g) with d = x_i - x_j in units of 1/FIXQ cell and
-// g the kernel-gradient factor of the pair in those units (grad W_ij = g d;
-// kc holds the kernel constants in record units), in the traversal order of
+// g = rec_g, the kernel-gradient factor of the pair in those units up to the
+// pass-wide rec_gscale (grad W_ij = rec_gscale g d; kc holds the kernel
+// constants in record units), in the traversal order of
 // the cells. ri is the particle's own record in `rec`. A particle whose list
 // overflowed walks the cell traversal over the FP32 positions, its pair
 // vectors converted to the record units.
@@ -470,7 +496,7 @@ __device__ __forceinline__ void for_each_rec(const Fluid& f, const KernelConst& 
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const float3 d = delta16(o, r[u]);
-                fn(j[u], r[u], d, pair_g_vec<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
+                fn(j[u], r[u], d, rec_g<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
             }
         }
 #pragma unroll
@@ -478,7 +504,7 @@ __device__ __forceinline__ void for_each_rec(const Fluid& f, const KernelConst& 
             if (k + u < cnt) {
                 const uint4 r = __ldg(rec + jn[u]);
                 const float3 d = delta16(o, r);
-                fn(jn[u], r, d, pair_g_vec<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
+                fn(jn[u], r, d, rec_g<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
             }
         }
     } else {
@@ -496,7 +522,7 @@ __device__ __forceinline__ void for_each_rec(const Fluid& f, const KernelConst& 
                     return;
                 const float3 d = make_float3(dx * to_units, dy * to_units, dz * to_units);
                 fn(j, __ldg(rec + j), d,
-                    pair_g<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
+                    rec_g<KIND>(kc, fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z))));
             });
     }
 }

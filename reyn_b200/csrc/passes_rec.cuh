@@ -75,30 +75,33 @@ k_np_rec(uint32_t n, Fluid f, RecConst rc,
     const float4 vi = vel[i];
     const uint4 ri = rec_in[i];
     const float eps_u = eps / rc.unit;
+    // the pair sums carry m_j / m_0 and rec_g; m_0 and rec_gscale are
+    // applied once per particle
     float ax = 0.f, ay = 0.f, az = 0.f, Gx = 0.f, Gy = 0.f, Gz = 0.f, gsq = 0.f;
     for_each_rec<KIND, R, BATCH>(f, rc.kc, rec_in, i, ri,
         [&](uint32_t, const uint4& rj, float3 d, float g) {
             const float l2 = fmaf(d.x, d.x, fmaf(d.y, d.y, d.z * d.z));
             const float2 vxy = bits_half2(rj.z);
             const float2 vzr = bits_half2(rj.w);
-            const float mj = m0 * rec_m16(rj);
+            const float mg = rec_m16(rj) * g;
             const float vdx =
                 fmaf(vi.x - vxy.x, d.x, fmaf(vi.y - vxy.y, d.y, (vi.z - vzr.x) * d.z));
-            const float s = __fdividef(nu10 * mj * vdx * g, vzr.y * fmaf(rc.unit, l2, eps_u));
+            const float s = __fdividef(nu10 * mg * vdx, vzr.y * fmaf(rc.unit, l2, eps_u));
             ax += s * d.x;
             ay += s * d.y;
             az += s * d.z;
-            const float mg = mj * g;
             Gx += mg * d.x;
             Gy += mg * d.y;
             Gz += mg * d.z;
             gsq += mg * g * l2;
         });
-    ax += grav.x;
-    ay += grav.y;
-    az += grav.z;
+    const float gs = rec_gscale<KIND>(rc.kc), sm = gs * m0;
+    ax = fmaf(ax, sm, grav.x);
+    ay = fmaf(ay, sm, grav.y);
+    az = fmaf(az, sm, grav.z);
     const float4 bt = bterm[i];
-    gq[i] = make_float4(Gx + bt.x, Gy + bt.y, Gz + bt.z, gsq);
+    gq[i] = make_float4(fmaf(Gx, sm, bt.x), fmaf(Gy, sm, bt.y), fmaf(Gz, sm, bt.z),
+        gsq * (sm * gs));
     const float4 vs = make_float4(vi.x + dt * ax, vi.y + dt * ay, vi.z + dt * az, vi.w);
     vel_out[i] = vs;
     const float mr = rec_m16(ri);
@@ -140,6 +143,11 @@ k_diag_pacc_rec(uint32_t n, Fluid f, RecConst rc,
         sy += sp * d.y;
         sz += sp * d.z;
     });
+    const float gs = rec_gscale<KIND>(rc.kc);
+    sx *= gs;
+    sy *= gs;
+    sz *= gs;
+    vk.sum *= gs;
     // the neighbours' pressures are half their carried ones
     const float ax = -r0i * fmaf(pi, gt.x, 0.5f * sx), ay = -r0i * fmaf(pi, gt.y, 0.5f * sy),
                 az = -r0i * fmaf(pi, gt.z, 0.5f * sz);
@@ -178,6 +186,7 @@ k_diag_rec(uint32_t n, Fluid f, RecConst rc,
         const float3 mv = rec_dg_vec(rj);
         vk.add(g * fmaf(mv.x, d.x, fmaf(mv.y, d.y, mv.z * d.z)));
     });
+    vk.sum *= rec_gscale<KIND>(rc.kc);
     const float gss = fmaf(gt.x, gt.x, fmaf(gt.y, gt.y, gt.z * gt.z));
     const float a = -dt * (gss + mi * gt.w) / (rho0 * rho0);
     const float vdiv = fmaf(vi.x, gt.x, fmaf(vi.y, gt.y, vi.z * gt.z)) - m0 * vk.sum;
@@ -220,9 +229,10 @@ __device__ __forceinline__ void pacc_rec(uint32_t i, REYN_PACC_REC_ARGS)
         sy += sp * d.y;
         sz += sp * d.z;
     });
+    const float sm = m0 * rec_gscale<KIND>(rc.kc);
     const float ma = rec_m16(ri) * ACC_SCALE * -r0i;
-    rec_out[i] = rec_y(ri.x, ri.y, ma * fmaf(pi, gt.x, m0 * sx), ma * fmaf(pi, gt.y, m0 * sy),
-        ma * fmaf(pi, gt.z, m0 * sz));
+    rec_out[i] = rec_y(ri.x, ri.y, ma * fmaf(pi, gt.x, sm * sx), ma * fmaf(pi, gt.y, sm * sy),
+        ma * fmaf(pi, gt.z, sm * sz));
 }
 
 template <int KIND, int R, bool BATCH, int MB>
@@ -233,7 +243,8 @@ k_pacc_rec(REYN_PACC_REC_ARGS)
 }
 
 template <int KIND, int R, int MB>
-__global__ void __launch_bounds__(MB) k_pacc_rec_tiles(REYN_PACC_REC_ARGS, Tiles tl)
+__global__ void __launch_bounds__(MB, 65536 / 64 / MB)
+k_pacc_rec_tiles(REYN_PACC_REC_ARGS, Tiles tl)
 {
     REYN_TILE_LOOP(tl, (pacc_rec<KIND, R, true>(i, REYN_PACC_REC_PASS)));
 }
@@ -271,6 +282,7 @@ __device__ __forceinline__ void jacobi_rec(uint32_t i, REYN_JACOBI_REC_ARGS)
                 const float3 ma = rec_y_vec(rj);
                 sum += g * fmaf(ma.x, d.x, fmaf(ma.y, d.y, ma.z * d.z));
             });
+        sum *= rec_gscale<KIND>(rc.kc);
         // m_i a_i ACC_SCALE / m_0 as stored: a_i.G_i = (that . G_i) / (m16_i ACC_SCALE)
         const float3 mai = rec_y_vec(ri);
         const float Ap = dt * (1.f / ACC_SCALE)
@@ -299,7 +311,8 @@ k_jacobi_rec(REYN_JACOBI_REC_ARGS)
 }
 
 template <int KIND, int R, int MB>
-__global__ void __launch_bounds__(MB) k_jacobi_rec_tiles(REYN_JACOBI_REC_ARGS, Tiles tl)
+__global__ void __launch_bounds__(MB, 65536 / 64 / MB)
+k_jacobi_rec_tiles(REYN_JACOBI_REC_ARGS, Tiles tl)
 {
     REYN_TILE_LOOP(tl, (jacobi_rec<KIND, R, true>(i, REYN_JACOBI_REC_PASS)));
 }
@@ -331,8 +344,9 @@ k_final_rec(uint32_t n, Fluid f, RecConst rc,
                 sy += sp * d.y;
                 sz += sp * d.z;
             });
-            const float ax = -r0i * fmaf(pi, gt.x, m0 * sx), ay = -r0i * fmaf(pi, gt.y, m0 * sy),
-                    az = -r0i * fmaf(pi, gt.z, m0 * sz);
+        const float sm = m0 * rec_gscale<KIND>(rc.kc);
+        const float ax = -r0i * fmaf(pi, gt.x, sm * sx), ay = -r0i * fmaf(pi, gt.y, sm * sy),
+                    az = -r0i * fmaf(pi, gt.z, sm * sz);
         acc.x[i] = ax;
         acc.y[i] = ay;
         acc.z[i] = az;
