@@ -13,6 +13,14 @@ from tests.helpers import STEP_TOL, compare_steps, run_engine, run_oracle
 
 pytestmark = pytest.mark.gpu
 
+# aggregate bounds of the developed collapse, about 5x the MIXED_POS16
+# differences measured on a B200 (FP32: 3e-6 m, 5e-5 rho0, 4e-6, 0 sweeps;
+# MIXED_POS16: 1.1e-5 m, 3.2e-4 rho0, 7.5e-4, 0 sweeps of 1,203)
+DEV_COM_TOL = 5e-5  # metres, per axis
+DEV_RHO_TOL = 1.5e-3  # of rho0, mean density
+DEV_KE_TOL = 4e-3  # relative, kinetic energy
+DEV_ITER_TOL = 0.02  # relative, total sweeps
+
 
 def _bench_params(rb, sc, precision):
     import bench
@@ -194,3 +202,43 @@ def test_sesph_config_gravity_z_vs_oracle(cuda):
     ke_g = float((got["vx"] ** 2 + got["vy"] ** 2 + got["vz"] ** 2).sum())
     ke_w = float((want["vx"] ** 2 + want["vy"] ** 2 + want["vz"] ** 2).sum())
     assert abs(ke_g - ke_w) < 0.02 * ke_w
+
+
+@pytest.mark.parametrize("precision", ["FP32", "MIXED_POS16"])
+def test_developed_collapse_vs_oracle(cuda, precision):
+    """A column collapse run until the flow has developed (400 steps of 1 ms:
+    the front reaches the far wall, cells hold 0 to several particles) with
+    the benchmark's IISPH settings, against the oracle stepped alike.
+    Per-particle paths separate over long runs, so the comparison is in
+    aggregate: centre of mass, mean density, kinetic energy, and the total
+    sweep count."""
+    import bench
+    import reyn_b200 as rb
+
+    sc = scenes.dam_break((12, 20, 10), 0.02, (0.8, 0.5, 0.24), mass_kernel="C2", gap=1.5,
+                          seed=12)
+    bm = oracle.boundary_masses(sc.bdy["x"], sc.bdy["y"], sc.bdy["z"], sc.h, sc.rho0, 5)
+    bdy = dict(sc.bdy, m=bm)
+    steps, dt = 400, 1e-3
+    prm = rb.reference_params(rb.IISPH, rb.C2, sc.h, sc.rho0, bench.NU)
+    prm.convergence = rb.CONV_AVERAGE
+    prm.eta = 0.001
+    prm.max_iter = 1000
+    prm.precision = getattr(rb, "PRECISION_" + precision)
+    got = run_engine(2, rb.C2, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, bench.NU,
+                     dt, steps, params=prm)
+    want = run_oracle(2, 0, sc.fluid, bdy, sc.box_min, sc.box_max, sc.h, sc.rho0, bench.NU, dt,
+                      steps, params=bench.oracle_params(sc.h, sc.rho0))
+    com = {k: (float(got[k].mean()), float(want[k].mean())) for k in ("x", "y", "z")}
+    ke_g = float((got["vx"] ** 2 + got["vy"] ** 2 + got["vz"] ** 2).sum())
+    ke_w = float((want["vx"] ** 2 + want["vy"] ** 2 + want["vz"] ** 2).sum())
+    it_g, it_w = int(np.sum(got["iters"])), int(np.sum(want["iters"]))
+    print(precision, com, float(got["rho"].mean()), float(want["rho"].mean()), ke_g, ke_w,
+          it_g, it_w, float(want["x"].max()))
+    # the front has crossed the box: the flow is developed
+    assert want["x"].max() > 0.6
+    for k, (g, w) in com.items():
+        assert abs(g - w) < DEV_COM_TOL, (k, g, w)
+    assert abs(got["rho"].mean() - want["rho"].mean()) < DEV_RHO_TOL * sc.rho0
+    assert abs(ke_g - ke_w) < DEV_KE_TOL * ke_w
+    assert abs(it_g - it_w) <= DEV_ITER_TOL * it_w
