@@ -303,37 +303,66 @@ __device__ __forceinline__ int3 clamp_cell(const GridView& g, int3 c, int R)
 // approximate square root used for the chord), so exactly the candidates
 // within r are still visited, in the same order; only provably empty cells
 // are skipped.
+
+// the point in cell units relative to its own cell's lower corner, and the
+// squared search radius in cells with the trimming margin
+struct RowFrame {
+    float fx, fy, fz, rr;
+};
+
+__device__ __forceinline__ RowFrame row_frame(const GridView& g, int3 c, float xi, float yi,
+    float zi)
+{
+    constexpr float EPS = 1e-3f;
+    RowFrame fr;
+    fr.fx = (xi - g.lox) * g.inv_cell - (float)c.x;
+    fr.fy = (yi - g.loy) * g.inv_cell - (float)c.y;
+    fr.fz = (zi - g.loz) * g.inv_cell - (float)c.z;
+    fr.rr = g.r2 * g.inv_cell * g.inv_cell * (1.f + EPS) + EPS;
+    return fr;
+}
+
+// squared distance (cells) from the point to the slab of cells at c.z + dz
+__device__ __forceinline__ float slab_gap2(const RowFrame& fr, int dz)
+{
+    const float gz = dz > 0 ? fmaxf((float)dz - fr.fz, 0.f)
+                            : (dz < 0 ? fmaxf(fr.fz - (float)(dz + 1), 0.f) : 0.f);
+    return gz * gz;
+}
+
+// the x-cells [x0, x1] (relative to c.x) of row dy in a slab at squared gap
+// gz2 that the sphere can reach; false when the row is skipped
+template <int R>
+__device__ __forceinline__ bool row_span(const RowFrame& fr, float gz2, int dy, int& x0, int& x1)
+{
+    constexpr float EPS = 1e-3f;
+    const float gy = dy > 0 ? fmaxf((float)dy - fr.fy, 0.f)
+                            : (dy < 0 ? fmaxf(fr.fy - (float)(dy + 1), 0.f) : 0.f);
+    const float d2 = fmaf(gy, gy, gz2);
+    if (d2 > fr.rr)
+        return false;
+    const float t = fr.rr - d2;
+    const float w = (t > 0.f ? t * rsqrtf(t) : 0.f) + EPS; // half chord, cells
+    x0 = max(-R, (int)floorf(fr.fx - w));
+    x1 = min(R, (int)floorf(fr.fx + w));
+    return x0 <= x1; // empty only for points clamped into the grid from outside
+}
+
 template <int R, class Run>
 __device__ __forceinline__ void for_each_row(const GridView& g, int3 c, float xi, float yi,
     float zi, Run&& run)
 {
-    constexpr float EPS = 1e-3f;
-    // the point in cell units, relative to its own cell's lower corner
-    const float fx = (xi - g.lox) * g.inv_cell - (float)c.x;
-    const float fy = (yi - g.loy) * g.inv_cell - (float)c.y;
-    const float fz = (zi - g.loz) * g.inv_cell - (float)c.z;
-    const float rr = g.r2 * g.inv_cell * g.inv_cell * (1.f + EPS) + EPS;
+    const RowFrame fr = row_frame(g, c, xi, yi, zi);
 #pragma unroll 1
     for (int dz = -R; dz <= R; ++dz) {
-        // distance (cells) from the point to the slab of cells at c.z + dz
-        const float gz = dz > 0 ? fmaxf((float)dz - fz, 0.f)
-                                : (dz < 0 ? fmaxf(fz - (float)(dz + 1), 0.f) : 0.f);
-        const float gz2 = gz * gz;
-        if (gz2 > rr)
+        const float gz2 = slab_gap2(fr, dz);
+        if (gz2 > fr.rr)
             continue;
         const int plane = (c.z + dz) * g.nxny;
 #pragma unroll 1
         for (int dy = -R; dy <= R; ++dy) {
-            const float gy = dy > 0 ? fmaxf((float)dy - fy, 0.f)
-                                    : (dy < 0 ? fmaxf(fy - (float)(dy + 1), 0.f) : 0.f);
-            const float d2 = fmaf(gy, gy, gz2);
-            if (d2 > rr)
-                continue;
-            const float t = rr - d2;
-            const float w = (t > 0.f ? t * rsqrtf(t) : 0.f) + EPS; // half chord, cells
-            const int x0 = max(-R, (int)floorf(fx - w));
-            const int x1 = min(R, (int)floorf(fx + w));
-            if (x0 > x1) // only for points clamped into the grid from outside
+            int x0, x1;
+            if (!row_span<R>(fr, gz2, dy, x0, x1))
                 continue;
             // one run per row, two where a Z-order row crosses a brick; one
             // call site, so the caller's candidate loop is inlined once

@@ -542,6 +542,93 @@ __device__ __forceinline__ void for_each_boundary(const Bdy& b, float x, float y
     for_each_neighbour<2>(b.g, c, x, y, z, b.pm, f);
 }
 
+// The density pass's boundary sums (rb = sum_b m_b W_ib and
+// g = sum_b m_b grad W_ib) for every lane of the warp whose cell has samples
+// within reach, computed by the whole warp: for each such lane in turn, lanes
+// 0-24 take one row each of that point's 5x5 rows of boundary cells (the
+// rows and trim of for_each_boundary) and the warp adds the rows up. A lane
+// walking its 25 rows alone holds its warp for all of them; in the batched
+// workloads three warps in four hold a lane near a wall (scene boxes are a
+// few dozen particles wide), so the batched density pass uses this; in one
+// large scene few warps do, and the lanes walk alone there. Every lane of the
+// warp must call this (no lane may have returned); `need_point` says whether
+// the lane's own point is a fluid particle. The sums run over the samples
+// for_each_boundary visits, added in another order. Batched scenes: each
+// point uses its own scene's boundary grid.
+template <int KIND, bool BATCH>
+__device__ __forceinline__ float4 boundary_sums_warp(const Bdy& b0, const KernelConst& kc,
+    bool need_point, uint32_t scene, float x, float y, float z)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    bool need = false;
+    if (need_point && b0.n) {
+        Bdy b = b0;
+        if constexpr (BATCH) {
+            if (b.g.sid) {
+                b.g = at_scene(b.g, scene);
+                b.near += b.g.key_base;
+            }
+        }
+        const int3 c = cell_of(b.g, x, y, z);
+        need = cell_inside(b.g, c, 2)
+            && __ldg(b.near + (c.z * b.g.nxny + c.y * b.g.nx + c.x)) != 0;
+    }
+    unsigned m = __ballot_sync(FULL, need);
+    float4 mine = make_float4(0.f, 0.f, 0.f, 0.f);
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const float px = __shfl_sync(FULL, x, src), py = __shfl_sync(FULL, y, src),
+                    pz = __shfl_sync(FULL, z, src);
+        Bdy b = b0;
+        if constexpr (BATCH) {
+            const uint32_t s = __shfl_sync(FULL, scene, src);
+            if (b.g.sid) {
+                b.g = at_scene(b.g, s);
+                b.near += b.g.key_base;
+            }
+        }
+        float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
+        if (lane < 25) {
+            const int3 c = cell_of(b.g, px, py, pz);
+            const RowFrame fr = row_frame(b.g, c, px, py, pz);
+            const int dz = lane / 5 - 2, dy = lane % 5 - 2;
+            const float gz2 = slab_gap2(fr, dz);
+            int x0, x1;
+            if (gz2 <= fr.rr && row_span<2>(fr, gz2, dy, x0, x1)) {
+                const uint32_t k0 =
+                    uint32_t((c.z + dz) * b.g.nxny + (c.y + dy) * b.g.nx + c.x + x0);
+                const uint32_t e = __ldg(b.g.prefix + k0 + uint32_t(x1 - x0 + 1));
+                for (uint32_t j = __ldg(b.g.prefix + k0); j < e; ++j) {
+                    const float4 q = __ldg(b.pm + j);
+                    const float dx = px - q.x, dyy = py - q.y, dzz = pz - q.z;
+                    const float l2 = fmaf(dx, dx, fmaf(dyy, dyy, dzz * dzz));
+                    if (l2 <= b.g.r2) {
+                        float w, g;
+                        pair_wg<KIND>(kc, l2, w, g);
+                        rb += q.w * w;
+                        const float mg = q.w * g;
+                        gx += mg * dx;
+                        gy += mg * dyy;
+                        gz += mg * dzz;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            rb += __shfl_xor_sync(FULL, rb, o);
+            gx += __shfl_xor_sync(FULL, gx, o);
+            gy += __shfl_xor_sync(FULL, gy, o);
+            gz += __shfl_xor_sync(FULL, gz, o);
+        }
+        if (lane == src)
+            mine = make_float4(gx, gy, gz, rb);
+    }
+    return mine;
+}
+
 // jacobi_update (IISPH.cu:108-117). The reference compares the float a_ii
 // with the double 1e-6; `tiny` is the smallest float above 1e-6, for which
 // a < tiny holds exactly when (double)a < 1e-6 does (tiny_threshold()).
@@ -908,45 +995,62 @@ k_density(uint32_t n, Fluid f, Bdy b,
     uint4* __restrict__ rec_out, uint2* __restrict__ velh_out)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    if constexpr (BATCH)
-        enter_scene(f, b, i);
-    const float4 me = f.pm[i];
-    const int3 c = fluid_cell<R>(f, me);
-    uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
+    // batched scenes: every lane stays until the boundary sums, which its warp
+    // forms together
+    if constexpr (!BATCH) {
+        if (i >= n)
+            return;
+    }
+    const bool valid = i < n;
+    uint32_t scene = 0;
+    if constexpr (BATCH) {
+        if (valid)
+            scene = enter_scene(f, i);
+    }
+    const float4 me = valid ? f.pm[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    int3 c = make_int3(0, 0, 0);
     uint32_t cnt = 0;
     float rf = 0.f;
-    [[maybe_unused]] Kahan rk; // mixed modes: compensated density sum
-    for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
-        [&](uint32_t j, const float4& q, float, float, float, float l2) {
-            if constexpr (MIX)
-                rk.add(q.w * pair_w<KIND>(f.kc, l2));
-            else
-                rf += q.w * pair_w<KIND>(f.kc, l2);
-            if (j != i) {
-                if (cnt < KMAX)
-                    row[size_t(cnt) * 128] = j;
-                ++cnt;
-            }
-        });
-    if constexpr (MIX)
-        rf = rk.sum;
-    float rb = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-    for_each_boundary(b, me.x, me.y, me.z,
-        [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
-            float w, g;
-            pair_wg<KIND>(f.kc, l2, w, g);
-            rb += q.w * w;
-            const float mg = q.w * g;
-            gx += mg * dx;
-            gy += mg * dy;
-            gz += mg * dz;
-        });
-    const float r = rf + rb;
+    if (valid) {
+        c = fluid_cell<R>(f, me);
+        uint32_t* __restrict__ row = f.nbr + list_slot(i, 0);
+        [[maybe_unused]] Kahan rk; // mixed modes: compensated density sum
+        for_each_neighbour<R>(f.g, c, me.x, me.y, me.z, f.pm,
+            [&](uint32_t j, const float4& q, float, float, float, float l2) {
+                if constexpr (MIX)
+                    rk.add(q.w * pair_w<KIND>(f.kc, l2));
+                else
+                    rf += q.w * pair_w<KIND>(f.kc, l2);
+                if (j != i) {
+                    if (cnt < KMAX)
+                        row[size_t(cnt) * 128] = j;
+                    ++cnt;
+                }
+            });
+        if constexpr (MIX)
+            rf = rk.sum;
+    }
+    float4 bs = make_float4(0.f, 0.f, 0.f, 0.f);
+    if constexpr (BATCH) {
+        bs = boundary_sums_warp<KIND, BATCH>(b, f.kc, valid, scene, me.x, me.y, me.z);
+        if (!valid)
+            return;
+    } else {
+        for_each_boundary(b, me.x, me.y, me.z,
+            [&](uint32_t, const float4& q, float dx, float dy, float dz, float l2) {
+                float w, g;
+                pair_wg<KIND>(f.kc, l2, w, g);
+                bs.w += q.w * w;
+                const float mg = q.w * g;
+                bs.x += mg * dx;
+                bs.y += mg * dy;
+                bs.z += mg * dz;
+            });
+    }
+    const float r = rf + bs.w;
     rho[i] = r;
     vel[i].w = r;
-    bterm[i] = make_float4(gx, gy, gz, rb);
+    bterm[i] = bs;
     f.ncount[i] = cnt;
     if constexpr (MIX == MIX_POS16) {
         const float4 v = vel[i];
