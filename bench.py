@@ -638,9 +638,14 @@ def run_engine(a, world, rank, local):
     roofline = {"bound": "hbm", "kernel": dom_name, "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": profile_traffic(dom_name, headline), "peak_source": peak_kind,
-                # the unit these passes are bound by (ncu, committed summary)
+                # what bounds these passes instead (ncu, committed summary):
+                # instruction issue, and the L1 that serves their gathers
+                "issue_active_pct": profile_field(dom_name, headline, "issue_active_pct"),
                 "l1tex_throughput_pct": profile_field(dom_name, headline,
                                                       "l1tex_throughput_pct"),
+                "dram_traffic_over_alg": (round(profile_traffic(dom_name, headline) / alg, 2)
+                                          if alg and profile_traffic(dom_name, headline)
+                                          else None),
                 "alg_bytes_per_launch": alg, "ms_per_launch": round(per_launch_s * 1e3, 4),
                 "share_of_step": round(dom_ms / ms, 4)}
     kernels = {k: {"launches": v[0], "ms": round(v[1], 3)} for k, v in
