@@ -242,3 +242,54 @@ def test_developed_collapse_vs_oracle(cuda, precision):
     assert abs(got["rho"].mean() - want["rho"].mean()) < DEV_RHO_TOL * sc.rho0
     assert abs(ke_g - ke_w) < DEV_KE_TOL * ke_w
     assert abs(it_g - it_w) <= DEV_ITER_TOL * it_w
+
+
+@pytest.mark.parametrize("precision,scale", [("FP32", 1), ("MIXED", 20)])
+def test_column_16m_step_vs_oracle(cuda, precision, scale):
+    """The 16,777,216-particle column collapse of bench.py (--workload
+    column_16m: 256^3 lattice at 0.004 in a 3 x 1.5 x 1.5 box, box walls and a
+    Fibonacci sphere of radius 0.2, fluid culled near the samples, Wendland C6,
+    nu 0.005, 0.1 % average density error) generated on the GPU as the
+    benchmark does; one step at dt 0.08 h^2 / nu by particle ID against the
+    oracle, FP32 at the step tolerances and the benchmark's MIXED mode at
+    `scale` times them, equal sweep counts."""
+    import torch
+
+    import bench
+    import reyn_b200 as rb
+    from reyn_b200 import scenes as sc_mod
+
+    h, rho0, nu = 0.004, 1000.0, 0.005
+    box = np.array([3.0, 1.5, 1.5], np.float32)
+    st = rb.Particles(256 ** 3, rho0)
+    o = np.float32(1.5 * h)
+    rb.scene_fluid_block(st, (256, 256, 256), (o, o, o), h, sc_mod.rest_mass(h, rho0, "W6"),
+                         0.05, 0.0, 5)
+    wx, wy, wz = rb.scene_box_walls((0, 0, 0), box, h)
+    sx, sy, sz = rb.scene_sphere((1.5, 0.2, 0.75), 0.2, h)
+    bx, by, bz = (torch.cat([u, v]) for u, v in ((wx, sx), (wy, sy), (wz, sz)))
+    bd = rb.Boundary(bx, by, bz, None, h=h, rho0=rho0, mass_iters=5)
+    n = rb.scene_cull(st, bd, h)
+    torch.cuda.synchronize()
+    fluid = st.download()
+    fluid["id"] = np.arange(n, dtype=np.float32)
+    (px, py, pz, pm), nb = bd.arrays()
+    bdy = {k: rb.device_to_numpy(p, nb) for k, p in zip(("x", "y", "z", "m"), (px, py, pz, pm))}
+    for o_ in (bd, st):
+        o_.close()
+    del bx, by, bz, wx, wy, wz, sx, sy, sz
+    dt = bench.viscous_dt_limit(h, nu)
+    prm = rb.reference_params(rb.IISPH, rb.W6, h, rho0, nu)
+    prm.convergence = rb.CONV_AVERAGE
+    prm.eta = 0.001
+    prm.max_iter = 1000
+    prm.precision = getattr(rb, "PRECISION_" + precision)
+    got = run_engine(2, rb.W6, fluid, bdy, (0, 0, 0), box, h, rho0, nu, dt, 1, params=prm)
+    oprm = oracle.reference_params(2, 2, h, rho0, nu)
+    oprm.iisph_avg = 1
+    oprm.eta = 0.001
+    oprm.max_iter = 1000
+    want = run_oracle(2, 2, fluid, bdy, (0, 0, 0), box, h, rho0, nu, dt, 1, params=oprm)
+    assert got["iters"] == [int(x) for x in want["iters"]]
+    tol = {k: (r * scale, a * scale) for k, (r, a) in STEP_TOL.items()}
+    compare_steps(got, want, 2, tol, f"column_16m/{precision}")
